@@ -1,0 +1,71 @@
+// Shared helpers for the sm_100a kernels and their host drivers.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+
+#define ATLB_CUDA_CHECK(expr)                                                  \
+  do {                                                                         \
+    cudaError_t e__ = (expr);                                                  \
+    if (e__ != cudaSuccess) {                                                  \
+      fprintf(stderr, "atlas_b200: CUDA error %s at %s:%d: %s\n",             \
+              cudaGetErrorName(e__), __FILE__, __LINE__,                       \
+              cudaGetErrorString(e__));                                        \
+      atlb::set_cuda_error(e__);                                               \
+    }                                                                          \
+  } while (0)
+
+namespace atlb {
+
+// Enum values of the CBLAS interface (include/cblas.h:5-10 of the reference).
+enum { kRowMajor = 101, kColMajor = 102 };
+enum { kNoTrans = 111, kTrans = 112, kConjTrans = 113 };
+enum { kUpper = 121, kLower = 122 };
+enum { kNonUnit = 131, kUnit = 132 };
+enum { kLeft = 141, kRight = 142 };
+
+void set_cuda_error(cudaError_t e);
+cudaStream_t stream();           // the library's stream for the calling thread
+int num_sms();
+
+// Device memory cache: grow-only buffers keyed by slot, reused across calls
+// so the hot path performs no cudaMalloc once warm.
+void *scratch(int slot, size_t bytes);
+void *pinned(int slot, size_t bytes);
+enum ScratchSlot {
+  kSlotA = 0, kSlotB, kSlotC, kSlotIpiv, kSlotTau, kSlotWork, kSlotWork2,
+  kSlotInfo, kSlotMixedA, kSlotMixedR, kSlotMixedX, kSlotMixedD,
+  kSlotOzA, kSlotOzB, kSlotOzScale, kSlotBatch0, kSlotBatch1, kSlotBatch2,
+  kSlotBatch3, kSlotAdj0, kSlotAdj1, kSlotAdj2, kSlotTc0, kSlotTc1,
+  kNumSlots
+};
+
+inline int cdiv(long a, long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace atlb
+
+// ---------------------------------------------------------------------------
+// Device helpers
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool pred) {
+  uint32_t s = smem_u32(smem);
+  int n = pred ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool pred) {
+  uint32_t s = smem_u32(smem);
+  int n = pred ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem, bool pred) {
+  uint32_t s = smem_u32(smem);
+  int n = pred ? 4 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }

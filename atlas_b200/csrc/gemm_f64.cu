@@ -1,0 +1,246 @@
+// FP64 GEMM on the sm_100a FP64 tensor path (DMMA, mma.sync m8n8k4 f64).
+//
+// Replaces the amm micro-kernels + block copies of the reference GEMM driver
+// (src/blas/ammm/ATL_ammm.c:12-364, ATL_iploops.c:19-181): instead of copying
+// A/B into access-major blocks on the host, a 4-stage cp.async pipeline stages
+// 128x16 tiles of op(A) and op(B) in shared memory in the layout their global
+// memory already has (no transposing copy), and each of 8 warps accumulates a
+// 64x32 block of C in registers with DMMA.  The same kernel computes one
+// triangle of C for SYRK (tiles outside the triangle exit at once; elements
+// outside it are not stored).
+#include "common.cuh"
+#include "kernels.h"
+
+namespace atlb {
+namespace {
+
+constexpr int BM = 128, BN = 128, BK = 16, THREADS = 256, STAGES = 4, PAD = 4;
+
+// Shared-memory layout of one operand tile.  "o" is the outer index (m for A,
+// n for B), "k" the reduction index.  KC = the operand is k-contiguous in
+// global memory (A transposed, B not transposed); otherwise o-contiguous.
+template <bool KC> struct Lay;
+template <> struct Lay<false> {
+  static constexpr int LD = BM + PAD;  // 132 doubles: conflict-free fragments
+  static constexpr int SIZE = BK * LD;
+  __device__ static __forceinline__ int at(int o, int k) { return k * LD + o; }
+};
+template <> struct Lay<true> {
+  static constexpr int LD = BK + PAD;  // 20 doubles
+  static constexpr int SIZE = BM * LD;
+  __device__ static __forceinline__ int at(int o, int k) { return o * LD + k; }
+};
+
+// Issue the cp.async copies of one BMxBK tile (o0.., k0..) of an operand.
+template <bool KC, int VEC>
+__device__ __forceinline__ void load_tile(double *s, const double *X, long ld, int o0, int k0,
+                                          int O, int K, int tid) {
+  if (!KC) {
+    if (VEC == 2) {
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        int c = tid + THREADS * i, k = c >> 6, o = (c & 63) * 2;
+        int go = o0 + o, gk = k0 + k;
+        double *d = s + Lay<false>::at(o, k);
+        const double *g = X + go + (long)gk * ld;
+        if (gk < K && go + 1 < O) cp_async16(d, g, true);
+        else {
+          bool p0 = gk < K && go < O;
+          cp_async8(d, p0 ? g : X, p0);
+          cp_async8(d + 1, X, false);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        int c = tid + THREADS * i, k = c >> 7, o = c & 127;
+        int go = o0 + o, gk = k0 + k;
+        bool p = gk < K && go < O;
+        cp_async8(s + Lay<false>::at(o, k), p ? X + go + (long)gk * ld : X, p);
+      }
+    }
+  } else {
+    if (VEC == 2) {
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        int c = tid + THREADS * i, o = c >> 3, k = (c & 7) * 2;
+        int go = o0 + o, gk = k0 + k;
+        double *d = s + Lay<true>::at(o, k);
+        const double *g = X + gk + (long)go * ld;
+        if (go < O && gk + 1 < K) cp_async16(d, g, true);
+        else {
+          bool p0 = go < O && gk < K;
+          cp_async8(d, p0 ? g : X, p0);
+          cp_async8(d + 1, X, false);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        int c = tid + THREADS * i, o = c >> 4, k = c & 15;
+        int go = o0 + o, gk = k0 + k;
+        bool p = go < O && gk < K;
+        cp_async8(s + Lay<true>::at(o, k), p ? X + gk + (long)go * ld : X, p);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
+  asm volatile(
+      "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+      : "+d"(c[0]), "+d"(c[1])
+      : "d"(a), "d"(b));
+}
+
+// C = alpha*op(A)*op(B) + beta*C (column-major).  tri: 0 full, 1 lower
+// (store row >= col), 2 upper (row <= col).
+template <bool TA, bool TB, int VEC>
+__global__ void __launch_bounds__(THREADS, 1)
+dgemm_dmma_kernel(int M, int N, int K, double alpha, const double *__restrict__ A, long lda,
+                  const double *__restrict__ B, long ldb, double beta, double *__restrict__ C,
+                  long ldc, int tri) {
+  extern __shared__ __align__(16) double smem[];
+  using LA = Lay<TA>;   // A k-contiguous when transposed
+  using LB = Lay<!TB>;  // B k-contiguous when not transposed
+  double *sA = smem;
+  double *sB = smem + STAGES * LA::SIZE;
+
+  const int tiles_m = (M + BM - 1) / BM, tiles_n = (N + BN - 1) / BN;
+  // grouped rasterisation: 8 tile-rows share B panels in L2
+  const int bid = blockIdx.x, G = 8;
+  const int per_group = G * tiles_n, group = bid / per_group;
+  const int first_m = group * G, gsz = min(tiles_m - first_m, G);
+  const int tm = first_m + (bid % per_group) % gsz, tn = (bid % per_group) / gsz;
+  const int m0 = tm * BM, n0 = tn * BN;
+  if (tri == 1 && m0 + BM - 1 < n0) return;
+  if (tri == 2 && m0 > n0 + BN - 1) return;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = (warp & 1) * 64, wn = (warp >> 1) * 32;
+
+  double acc[8][4][2];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+  const int KT = (K + BK - 1) / BK;
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; s++) {
+    if (s < KT) {
+      load_tile<TA, VEC>(sA + s * LA::SIZE, A, lda, m0, s * BK, M, K, tid);
+      load_tile<!TB, VEC>(sB + s * LB::SIZE, B, ldb, n0, s * BK, N, K, tid);
+    }
+    cp_async_commit();
+  }
+
+  const int fr = lane >> 2, fk = lane & 3;
+  for (int kt = 0; kt < KT; kt++) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    {
+      int nk = kt + STAGES - 1;
+      if (nk < KT) {
+        int st = nk % STAGES;
+        load_tile<TA, VEC>(sA + st * LA::SIZE, A, lda, m0, nk * BK, M, K, tid);
+        load_tile<!TB, VEC>(sB + st * LB::SIZE, B, ldb, n0, nk * BK, N, K, tid);
+      }
+      cp_async_commit();
+    }
+    const double *a_s = sA + (kt % STAGES) * LA::SIZE;
+    const double *b_s = sB + (kt % STAGES) * LB::SIZE;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 4) {
+      double a[8], b[4];
+#pragma unroll
+      for (int i = 0; i < 8; i++) a[i] = a_s[LA::at(wm + i * 8 + fr, kk + fk)];
+#pragma unroll
+      for (int j = 0; j < 4; j++) b[j] = b_s[LB::at(wn + j * 8 + fr, kk + fk)];
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) dmma(acc[i][j], a[i], b[j]);
+    }
+  }
+  cp_async_wait<0>();
+
+  // epilogue: C fragment row = lane>>2, cols = 2*(lane&3) + {0,1}
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    int r = m0 + wm + i * 8 + fr;
+    if (r >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        int c = n0 + wn + j * 8 + fk * 2 + h;
+        if (c >= N) continue;
+        if (tri == 1 && r < c) continue;
+        if (tri == 2 && r > c) continue;
+        double *p = C + r + (long)c * ldc;
+        double v = alpha * acc[i][j][h];
+        if (beta != 0.0) v = fma(beta, *p, v);
+        *p = v;
+      }
+    }
+  }
+}
+
+__global__ void scale_kernel(int M, int N, double beta, double *C, long ldc, int tri) {
+  long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  long total = (long)M * N;
+  for (; idx < total; idx += (long)gridDim.x * blockDim.x) {
+    int r = (int)(idx % M), c = (int)(idx / M);
+    if (tri == 1 && r < c) continue;
+    if (tri == 2 && r > c) continue;
+    double *p = C + r + (long)c * ldc;
+    *p = (beta == 0.0) ? 0.0 : beta * *p;
+  }
+}
+
+template <bool TA, bool TB, int VEC>
+void launch(int M, int N, int K, double alpha, const double *A, long lda, const double *B,
+            long ldb, double beta, double *C, long ldc, int tri, cudaStream_t st) {
+  constexpr int smem = STAGES * (Lay<TA>::SIZE + Lay<!TB>::SIZE) * (int)sizeof(double);
+  static bool configured = false;
+  if (!configured) {
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(dgemm_dmma_kernel<TA, TB, VEC>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    configured = true;
+  }
+  int tiles = cdiv(M, BM) * cdiv(N, BN);
+  dgemm_dmma_kernel<TA, TB, VEC><<<tiles, THREADS, smem, st>>>(M, N, K, alpha, A, lda, B, ldb,
+                                                              beta, C, ldc, tri);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
+
+inline bool al16(const void *p, long ld) { return ((uintptr_t)p % 16 == 0) && (ld % 2 == 0); }
+
+}  // namespace
+
+void dgemm_dev(int ta, int tb, int M, int N, int K, double alpha, const double *A, long lda,
+               const double *B, long ldb, double beta, double *C, long ldc, cudaStream_t st,
+               int tri) {
+  if (M <= 0 || N <= 0) return;
+  if (K <= 0 || alpha == 0.0) {
+    if (beta == 1.0) return;
+    long total = (long)M * N;
+    int blocks = (int)std::min<long>((total + 255) / 256, 148L * 16);
+    scale_kernel<<<blocks, 256, 0, st>>>(M, N, beta, C, ldc, tri);
+    ATLB_CUDA_CHECK(cudaGetLastError());
+    return;
+  }
+  const bool tA = ta != kNoTrans, tB = tb != kNoTrans;
+  const bool v2 = al16(A, lda) && al16(B, ldb);
+#define ATLB_DG(TA_, TB_)                                                                 \
+  if (v2) launch<TA_, TB_, 2>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, tri, st);    \
+  else launch<TA_, TB_, 1>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, tri, st);
+  if (!tA && !tB) { ATLB_DG(false, false) }
+  else if (!tA && tB) { ATLB_DG(false, true) }
+  else if (tA && !tB) { ATLB_DG(true, false) }
+  else { ATLB_DG(true, true) }
+#undef ATLB_DG
+}
+
+}  // namespace atlb

@@ -1,0 +1,79 @@
+// Device-pointer building blocks shared by the drivers and the C-ABI layer.
+// All routines are column-major, enqueue on `st` and return without waiting.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace atlb {
+
+// C = alpha*op(A)*op(B) + beta*C.  tri: 0 whole C, 1 lower triangle only,
+// 2 upper triangle only (SYRK).
+void dgemm_dev(int ta, int tb, int M, int N, int K, double alpha, const double *A, long lda,
+               const double *B, long ldb, double beta, double *C, long ldc, cudaStream_t st,
+               int tri = 0);
+void sgemm_dev(int ta, int tb, int M, int N, int K, float alpha, const float *A, long lda,
+               const float *B, long ldb, float beta, float *C, long ldc, cudaStream_t st,
+               int tri = 0);
+
+// A FP32 GEMM entry with the sgemm_dev signature; the mixed-precision LU and
+// Cholesky take one of these for their trailing updates.
+typedef void (*SgemmFn)(int ta, int tb, int M, int N, int K, float alpha, const float *A,
+                        long lda, const float *B, long ldb, float beta, float *C, long ldc,
+                        cudaStream_t st, int tri);
+
+// Tensor-core (tcgen05) FP32-in/FP32-out GEMMs: operands rounded to TF32 or
+// BF16 on the fly, FP32 accumulation in tensor memory.
+void sgemm_tf32_dev(int ta, int tb, int M, int N, int K, float alpha, const float *A, long lda,
+                    const float *B, long ldb, float beta, float *C, long ldc, cudaStream_t st,
+                    int tri);
+void sgemm_bf16_dev(int ta, int tb, int M, int N, int K, float alpha, const float *A, long lda,
+                    const float *B, long ldb, float beta, float *C, long ldc, cudaStream_t st,
+                    int tri);
+
+template <typename T>
+void gemm_dev(int ta, int tb, int M, int N, int K, T alpha, const T *A, long lda, const T *B,
+              long ldb, T beta, T *C, long ldc, cudaStream_t st, int tri = 0);
+
+// Triangular solve (BLAS trsm semantics), recursive with GEMM off-diagonal
+// updates; `gemm` is used for the FP32 instantiation (nullptr = sgemm_dev).
+template <typename T>
+void trsm_dev(int side, int uplo, int trans, int diag, int M, int N, T alpha, const T *A, long lda,
+              T *B, long ldb, cudaStream_t st, SgemmFn gemm = nullptr);
+// B = alpha*op(A)*B (Left) or alpha*B*op(A) (Right), A triangular.
+void dtrmm_dev(int side, int uplo, int trans, int diag, int M, int N, double alpha,
+               const double *A, long lda, double *B, long ldb, cudaStream_t st);
+
+// Row interchanges: for k = k1..k2-1 (inc > 0) or k2-1..k1 (inc < 0) swap
+// rows k and ipiv[k] of the ncols columns starting at A (row indices are
+// absolute: row r of the matrix is A[r]).
+template <typename T>
+void laswp_dev(int ncols, T *A, long lda, int k1, int k2, const int *ipiv, int inc,
+               cudaStream_t st);
+
+// LU with partial pivoting, ATLAS's recursive splitting.  ipiv: device,
+// 0-based absolute rows.  dinfo: device int, receives 0 or the first zero
+// pivot (1-based).
+template <typename T>
+void getrf_dev(int M, int N, T *A, long lda, int *ipiv, int *dinfo, cudaStream_t st,
+               SgemmFn gemm = nullptr);
+template <typename T>
+void getrs_dev(int trans, int N, int NRHS, const T *A, long lda, const int *ipiv, T *B, long ldb,
+               cudaStream_t st, SgemmFn gemm = nullptr);
+
+// Cholesky (uplo = kLower: A = L L^T; kUpper: A = U^T U); dinfo as above.
+template <typename T>
+void potrf_dev(int uplo, int N, T *A, long lda, int *dinfo, cudaStream_t st,
+               SgemmFn gemm = nullptr);
+template <typename T>
+void potrs_dev(int uplo, int N, int NRHS, const T *A, long lda, T *B, long ldb, cudaStream_t st,
+               SgemmFn gemm = nullptr);
+
+// Householder QR (ATLAS conventions: tau in [1,2], beta = -sign(alpha)*norm).
+void dgeqrf_dev(int M, int N, double *A, long lda, double *tau, cudaStream_t st);
+
+// Small utilities
+void set_info_kernel_launch(int *dinfo, cudaStream_t st);       // *dinfo = INT_MAX
+void finish_info_kernel_launch(int *dinfo, cudaStream_t st);    // INT_MAX -> 0
+template <typename T>
+void fill_zero_dev(T *A, int M, int N, long lda, cudaStream_t st);
+
+}  // namespace atlb

@@ -1,0 +1,381 @@
+// LU factorization with partial pivoting (clapack_dgetrf / ATL_getrfC) and
+// the solve (ATL_getrs).
+//
+// Driver: the reference's recursive column halving (src/lapack/ATL_getrfC.c:
+// 277-301): factor the left half, swap + TRSM + GEMM-update the right half,
+// factor it, back-apply its swaps to the left half.  The recursion stops at a
+// panel of NB <= 32 columns, which ONE kernel factors: a thread-block cluster
+// of up to 16 CTAs x 512 threads holds the panel's rows in registers (one
+// row, or a few, per thread), and each column costs one cluster barrier:
+// every CTA publishes its local pivot candidate (|value|, row position, and
+// the candidate row itself) in shared memory, all CTAs read all candidates
+// over distributed shared memory, pick the same winner (largest |value|,
+// lowest row index on ties = cblas_idamax's first maximum, ATL_getf2.c:33),
+// and update their own rows with it.  Row swaps are not performed during the
+// panel: each row carries its current position and the final permutation is
+// applied when the rows are written back.
+#include <algorithm>
+#include <cfloat>
+#include <climits>
+#include <cooperative_groups.h>
+#include "common.cuh"
+#include "kernels.h"
+
+namespace cg = cooperative_groups;
+
+namespace atlb {
+namespace {
+
+constexpr int PT = 512;  // threads per CTA of the panel kernel
+
+template <typename T> __device__ __forceinline__ T safmin();
+template <> __device__ __forceinline__ double safmin<double>() { return DBL_MIN; }
+template <> __device__ __forceinline__ float safmin<float>() { return FLT_MIN; }
+
+template <typename T, int NB>
+struct PanelPub {  // one CTA's published candidate for one column
+  T row[NB];
+  T val;
+  int pos;
+};
+
+// Factor the M x ncols panel at A (ncols <= NB, M >= ncols).  Writes
+// ipiv[j] = roff + (pivot row within the panel) and atomically lowers
+// *dinfo to roff + j + 1 for a zero pivot in column j.
+template <typename T, int NB, int RPT>
+__global__ void __launch_bounds__(PT, 1)
+getf2_cluster_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restrict__ ipiv,
+                     int roff, int *__restrict__ dinfo) {
+  cg::cluster_group cl = cg::this_cluster();
+  const int C = (int)cl.num_blocks(), crank = (int)cl.block_rank();
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int TOT = C * PT;
+  const int MN = min(M, ncols);
+
+  __shared__ PanelPub<T, NB> pub[2];
+  __shared__ T grow[16][NB];
+  __shared__ T gval[16];
+  __shared__ int gpos[16];
+  __shared__ T wval[PT / 32];
+  __shared__ int wpos[PT / 32];
+
+  T a[RPT][NB];
+  int pos[RPT];
+  bool act[RPT];
+#pragma unroll
+  for (int q = 0; q < RPT; q++) {
+    int r = crank * PT + tid + q * TOT;
+    act[q] = r < M;
+    pos[q] = act[q] ? r : INT_MAX;
+#pragma unroll
+    for (int k = 0; k < NB; k++) a[q][k] = (act[q] && k < ncols) ? A[r + (long)k * lda] : T(0);
+  }
+
+  // publish this CTA's candidate for column c into pub[c & 1]
+  auto publish = [&](int c) {
+    T v = T(-1);
+    int vp = INT_MAX;
+#pragma unroll
+    for (int q = 0; q < RPT; q++) {
+      if (act[q]) {
+        T t = T(0);
+#pragma unroll
+        for (int k = 0; k < NB; k++)
+          if (k == c) t = fabs(a[q][k]);
+        if (t > v || (t == v && pos[q] < vp)) { v = t; vp = pos[q]; }
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      T ov = __shfl_xor_sync(0xffffffffu, v, o);
+      int op = __shfl_xor_sync(0xffffffffu, vp, o);
+      if (ov > v || (ov == v && op < vp)) { v = ov; vp = op; }
+    }
+    if (lane == 0) { wval[warp] = v; wpos[warp] = vp; }
+    __syncthreads();
+    if (warp == 0) {
+      v = lane < PT / 32 ? wval[lane] : T(-1);
+      vp = lane < PT / 32 ? wpos[lane] : INT_MAX;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        T ov = __shfl_xor_sync(0xffffffffu, v, o);
+        int op = __shfl_xor_sync(0xffffffffu, vp, o);
+        if (ov > v || (ov == v && op < vp)) { v = ov; vp = op; }
+      }
+      if (lane == 0) { pub[c & 1].val = v; pub[c & 1].pos = vp; }
+    }
+    __syncthreads();
+    const int wp = pub[c & 1].pos;
+#pragma unroll
+    for (int q = 0; q < RPT; q++)
+      if (act[q] && pos[q] == wp) {
+#pragma unroll
+        for (int k = 0; k < NB; k++) pub[c & 1].row[k] = a[q][k];
+      }
+    cl.sync();
+  };
+
+  if (MN > 0) publish(0);
+
+#pragma unroll
+  for (int j = 0; j < NB; j++) {
+    if (j >= MN) break;
+    const int b = j & 1;
+    // gather every CTA's candidate (one distributed-shared-memory round trip)
+    for (int idx = tid; idx < C * (NB + 2); idx += PT) {
+      int r = idx / (NB + 2), e = idx % (NB + 2);
+      PanelPub<T, NB> *rp = cl.map_shared_rank(&pub[b], r);
+      if (e < NB) grow[r][e] = rp->row[e];
+      else if (e == NB) gval[r] = rp->val;
+      else gpos[r] = rp->pos;
+    }
+    __syncthreads();
+    T best = T(-1);
+    int p = INT_MAX, w = 0;
+    for (int r = 0; r < C; r++) {
+      T v = gval[r];
+      int vp = gpos[r];
+      if (v > best || (v == best && vp < p)) { best = v; p = vp; w = r; }
+    }
+    const T piv = grow[w][j];
+    if (crank == 0 && tid == 0) {
+      ipiv[j] = roff + p;
+      if (piv == T(0)) atomicMin(dinfo, roff + j + 1);
+    }
+    const bool use_rcp = fabs(piv) >= safmin<T>();
+    const T rcp = T(1) / piv;
+#pragma unroll
+    for (int q = 0; q < RPT; q++) {
+      if (!act[q]) continue;
+      if (pos[q] == p) {  // the pivot row becomes row j of U
+        act[q] = false;
+        pos[q] = j;
+        continue;
+      }
+      if (pos[q] == j) pos[q] = p;  // the row displaced by the swap
+      if (piv != T(0)) {
+        T l = use_rcp ? a[q][j] * rcp : a[q][j] / piv;
+        a[q][j] = l;
+#pragma unroll
+        for (int k = j + 1; k < NB; k++) a[q][k] = fma(-l, grow[w][k], a[q][k]);
+      }
+    }
+    if (j + 1 < MN) publish(j + 1);
+  }
+
+  // write rows back at their final positions (the permutation is applied here)
+#pragma unroll
+  for (int q = 0; q < RPT; q++) {
+    int r = crank * PT + tid + q * TOT;
+    if (r < M) {
+#pragma unroll
+      for (int k = 0; k < NB; k++)
+        if (k < ncols) A[pos[q] + (long)k * lda] = a[q][k];
+    }
+  }
+  cl.sync();  // keep this CTA's shared memory alive until every peer is done
+}
+
+// Fallback for panels taller than a cluster can hold: one CTA, global memory.
+template <typename T>
+__global__ void __launch_bounds__(1024)
+getf2_global_kernel(int M, int ncols, T *A, long lda, int *ipiv, int roff, int *dinfo) {
+  __shared__ T sv[32];
+  __shared__ int sp[32];
+  __shared__ int piv_row;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int MN = min(M, ncols);
+  for (int j = 0; j < MN; j++) {
+    T v = T(-1);
+    int vp = INT_MAX;
+    for (int i = j + tid; i < M; i += blockDim.x) {
+      T t = fabs(A[i + (long)j * lda]);
+      if (t > v) { v = t; vp = i; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      T ov = __shfl_xor_sync(0xffffffffu, v, o);
+      int op = __shfl_xor_sync(0xffffffffu, vp, o);
+      if (ov > v || (ov == v && op < vp)) { v = ov; vp = op; }
+    }
+    if (lane == 0) { sv[warp] = v; sp[warp] = vp; }
+    __syncthreads();
+    if (warp == 0) {
+      v = lane < (int)(blockDim.x / 32) ? sv[lane] : T(-1);
+      vp = lane < (int)(blockDim.x / 32) ? sp[lane] : INT_MAX;
+      for (int o = 16; o > 0; o >>= 1) {
+        T ov = __shfl_xor_sync(0xffffffffu, v, o);
+        int op = __shfl_xor_sync(0xffffffffu, vp, o);
+        if (ov > v || (ov == v && op < vp)) { v = ov; vp = op; }
+      }
+      if (lane == 0) {
+        if (v <= T(0)) vp = j;
+        piv_row = vp;
+        ipiv[j] = roff + vp;
+        if (v == T(0)) atomicMin(dinfo, roff + j + 1);
+      }
+    }
+    __syncthreads();
+    const int p = piv_row;
+    if (p != j)
+      for (int k = tid; k < ncols; k += blockDim.x) {
+        T t = A[j + (long)k * lda];
+        A[j + (long)k * lda] = A[p + (long)k * lda];
+        A[p + (long)k * lda] = t;
+      }
+    __syncthreads();
+    const T piv = A[j + (long)j * lda];
+    if (piv != T(0)) {
+      const bool use_rcp = fabs(piv) >= safmin<T>();
+      const T rcp = T(1) / piv;
+      for (int i = j + 1 + tid; i < M; i += blockDim.x) {
+        T l = use_rcp ? A[i + (long)j * lda] * rcp : A[i + (long)j * lda] / piv;
+        A[i + (long)j * lda] = l;
+        for (int k = j + 1; k < ncols; k++) A[i + (long)k * lda] -= l * A[j + (long)k * lda];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+int g_max_cluster = 0;
+
+template <typename T, int NB, int RPT>
+bool launch_cluster_panel(int M, int ncols, T *A, long lda, int *ipiv, int roff, int *dinfo,
+                          cudaStream_t st) {
+  int C = cdiv(M, PT * RPT);
+  if (C > g_max_cluster) return false;
+  auto kern = getf2_cluster_kernel<T, NB, RPT>;
+  static bool configured = false;
+  if (!configured) {
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    configured = true;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(C, 1, 1);
+  cfg.blockDim = dim3(PT, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  ATLB_CUDA_CHECK(cudaLaunchKernelEx(&cfg, kern, M, ncols, A, lda, ipiv, roff, dinfo));
+  return true;
+}
+
+void init_max_cluster() {
+  if (g_max_cluster) return;
+  // largest cluster of PT-thread CTAs the device can co-schedule (16 needs
+  // the non-portable opt-in; fall back to the portable 8)
+  auto kern = getf2_cluster_kernel<double, 32, 1>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(16, 1, 1);
+  cfg.blockDim = dim3(PT, 1, 1);
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 16;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  cudaError_t e = cudaOccupancyMaxActiveClusters(&n, kern, &cfg);
+  if (e != cudaSuccess) { cudaGetLastError(); n = 0; }
+  g_max_cluster = n > 0 ? 16 : 8;
+}
+
+// Panel width the cluster kernel supports for M rows.
+int panel_nb(int M) {
+  init_max_cluster();
+  if (M <= g_max_cluster * PT) return 32;
+  if (M <= g_max_cluster * PT * 2) return 16;
+  if (M <= g_max_cluster * PT * 4) return 8;
+  return 8;
+}
+
+template <typename T>
+void panel(int M, int ncols, T *A, long lda, int *ipiv, int roff, int *dinfo, cudaStream_t st) {
+  bool ok = false;
+  if (ncols <= 32 && M <= g_max_cluster * PT) ok = launch_cluster_panel<T, 32, 1>(M, ncols, A, lda, ipiv, roff, dinfo, st);
+  else if (ncols <= 16 && M <= g_max_cluster * PT * 2) ok = launch_cluster_panel<T, 16, 2>(M, ncols, A, lda, ipiv, roff, dinfo, st);
+  else if (ncols <= 8 && M <= g_max_cluster * PT * 4) ok = launch_cluster_panel<T, 8, 4>(M, ncols, A, lda, ipiv, roff, dinfo, st);
+  if (!ok) {
+    getf2_global_kernel<T><<<1, 1024, 0, st>>>(M, ncols, A, lda, ipiv, roff, dinfo);
+    ATLB_CUDA_CHECK(cudaGetLastError());
+  }
+}
+
+// trailing update A22 -= A21 * A12 (FP64 DMMA, or the FP32 GEMM supplied)
+void update_gemm(SgemmFn, int M, int N, int K, const double *A21, const double *A12, double *A22,
+                 long lda, cudaStream_t st) {
+  dgemm_dev(kNoTrans, kNoTrans, M, N, K, -1.0, A21, lda, A12, lda, 1.0, A22, lda, st);
+}
+void update_gemm(SgemmFn fn, int M, int N, int K, const float *A21, const float *A12, float *A22,
+                 long lda, cudaStream_t st) {
+  (fn ? fn : sgemm_dev)(kNoTrans, kNoTrans, M, N, K, -1.f, A21, lda, A12, lda, 1.f, A22, lda, st, 0);
+}
+
+template <typename T>
+void getrf_rec(int off, int M, int N, T *A, long lda, int *ipiv, int *dinfo, cudaStream_t st,
+               SgemmFn gemm) {
+  const int MN = std::min(M, N);
+  if (MN <= 0) return;
+  T *Ad = A + off + (long)off * lda;  // diagonal block start
+  const int nb = panel_nb(M);
+  if (MN <= nb) {
+    panel<T>(M, MN, Ad, lda, ipiv + off, off, dinfo, st);
+    if (N > MN) {
+      laswp_dev<T>(N - MN, A + (long)(off + MN) * lda, lda, off, off + MN, ipiv, 1, st);
+      trsm_dev<T>(kLeft, kLower, kNoTrans, kUnit, MN, N - MN, T(1), Ad, lda,
+                  Ad + (long)MN * lda, lda, st, gemm);
+    }
+    return;
+  }
+  const int Nl = std::max(nb, (MN / 2) / nb * nb), Nr = N - Nl;
+  getrf_rec<T>(off, M, Nl, A, lda, ipiv, dinfo, st, gemm);
+  laswp_dev<T>(Nr, A + (long)(off + Nl) * lda, lda, off, off + Nl, ipiv, 1, st);
+  T *A12 = Ad + (long)Nl * lda;
+  trsm_dev<T>(kLeft, kLower, kNoTrans, kUnit, Nl, Nr, T(1), Ad, lda, A12, lda, st, gemm);
+  T *A21 = Ad + Nl, *A22 = A12 + Nl;
+  update_gemm(gemm, M - Nl, Nr, Nl, A21, A12, A22, lda, st);
+  getrf_rec<T>(off + Nl, M - Nl, Nr, A, lda, ipiv, dinfo, st, gemm);
+  laswp_dev<T>(Nl, A + (long)off * lda, lda, off + Nl, off + MN, ipiv, 1, st);
+}
+
+}  // namespace
+
+template <typename T>
+void getrf_dev(int M, int N, T *A, long lda, int *ipiv, int *dinfo, cudaStream_t st,
+               SgemmFn gemm) {
+  set_info_kernel_launch(dinfo, st);
+  getrf_rec<T>(0, M, N, A, lda, ipiv, dinfo, st, gemm);
+  finish_info_kernel_launch(dinfo, st);
+}
+template void getrf_dev<double>(int, int, double *, long, int *, int *, cudaStream_t, SgemmFn);
+template void getrf_dev<float>(int, int, float *, long, int *, int *, cudaStream_t, SgemmFn);
+
+template <typename T>
+void getrs_dev(int trans, int N, int NRHS, const T *A, long lda, const int *ipiv, T *B, long ldb,
+               cudaStream_t st, SgemmFn gemm) {
+  // ATL_getrs column-major (src/lapack/ATL_getrs.c:34-50)
+  if (N <= 0 || NRHS <= 0) return;
+  if (trans == kNoTrans) {
+    laswp_dev<T>(NRHS, B, ldb, 0, N, ipiv, 1, st);
+    trsm_dev<T>(kLeft, kLower, kNoTrans, kUnit, N, NRHS, T(1), A, lda, B, ldb, st, gemm);
+    trsm_dev<T>(kLeft, kUpper, kNoTrans, kNonUnit, N, NRHS, T(1), A, lda, B, ldb, st, gemm);
+  } else {
+    trsm_dev<T>(kLeft, kUpper, kTrans, kNonUnit, N, NRHS, T(1), A, lda, B, ldb, st, gemm);
+    trsm_dev<T>(kLeft, kLower, kTrans, kUnit, N, NRHS, T(1), A, lda, B, ldb, st, gemm);
+    laswp_dev<T>(NRHS, B, ldb, 0, N, ipiv, -1, st);
+  }
+}
+template void getrs_dev<double>(int, int, int, const double *, long, const int *, double *, long,
+                                cudaStream_t, SgemmFn);
+template void getrs_dev<float>(int, int, int, const float *, long, const int *, float *, long,
+                               cudaStream_t, SgemmFn);
+
+}  // namespace atlb

@@ -1,0 +1,309 @@
+// Triangular solve, triangular multiply and row interchanges.
+//
+// TRSM follows the reference's recursive method (src/blas/ulevel3/ATL_trsm.c:
+// 13-228: halve the triangle, solve one half, GEMM-update the other, solve
+// it), down to 64x64 leaves that one CTA solves in shared memory / registers.
+// Every side/uplo/trans case is reduced to an "effective" forward or backward
+// solve T*X = B with T and B addressed through (row, column) strides, so one
+// leaf kernel serves all eight cases.
+#include <algorithm>
+#include "common.cuh"
+#include "kernels.h"
+
+namespace atlb {
+
+template <>
+void gemm_dev<double>(int ta, int tb, int M, int N, int K, double alpha, const double *A, long lda,
+                      const double *B, long ldb, double beta, double *C, long ldc,
+                      cudaStream_t st, int tri) {
+  dgemm_dev(ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, st, tri);
+}
+template <>
+void gemm_dev<float>(int ta, int tb, int M, int N, int K, float alpha, const float *A, long lda,
+                     const float *B, long ldb, float beta, float *C, long ldc, cudaStream_t st,
+                     int tri) {
+  sgemm_dev(ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, st, tri);
+}
+
+namespace {
+
+constexpr int LEAF = 64;
+
+// Solve T*X = B in place for one 64-column block of B.  T(i,k) =
+// Tp[i*tr + k*tc] (n x n, n <= 64), B(i,j) = Bp[i*br + j*bc].  lower: forward
+// substitution, else backward.  One thread per right-hand side, its column
+// held in registers; T broadcast from shared memory.
+template <typename T>
+__global__ void __launch_bounds__(LEAF)
+trsm_leaf_kernel(int n, int m, const T *__restrict__ Tp, long tr, long tc, T *__restrict__ Bp,
+                 long br, long bc, int lower, int unit) {
+  extern __shared__ __align__(16) unsigned char trsm_smem[];
+  T(*sT)[LEAF + 1] = reinterpret_cast<T(*)[LEAF + 1]>(trsm_smem);
+  T(*sB)[LEAF + 1] = sT + LEAF;
+  const int j0 = blockIdx.x * LEAF, tid = threadIdx.x;
+  for (int idx = tid; idx < n * n; idx += LEAF) {
+    int i, k;
+    if (tr == 1) { i = idx % n; k = idx / n; } else { k = idx % n; i = idx / n; }
+    sT[i][k] = Tp[i * tr + k * tc];
+  }
+  const int mcols = min(LEAF, m - j0);
+  for (int idx = tid; idx < n * mcols; idx += LEAF) {
+    int i, j;
+    if (br == 1) { i = idx % n; j = idx / n; } else { j = idx % mcols; i = idx / mcols; }
+    sB[i][j] = Bp[i * br + (long)(j0 + j) * bc];
+  }
+  __syncthreads();
+  if (tid < mcols) {
+    T x[LEAF];
+#pragma unroll
+    for (int i = 0; i < LEAF; i++) x[i] = (i < n) ? sB[i][tid] : T(0);
+    if (lower) {
+#pragma unroll
+      for (int k = 0; k < LEAF; k++) {
+        if (k < n) {
+          T xk = unit ? x[k] : x[k] / sT[k][k];
+          x[k] = xk;
+#pragma unroll
+          for (int i = k + 1; i < LEAF; i++)
+            if (i < n) x[i] -= sT[i][k] * xk;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k = LEAF - 1; k >= 0; k--) {
+        if (k < n) {
+          T xk = unit ? x[k] : x[k] / sT[k][k];
+          x[k] = xk;
+#pragma unroll
+          for (int i = 0; i < k; i++) x[i] -= sT[i][k] * xk;
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < LEAF; i++)
+      if (i < n) sB[i][tid] = x[i];
+  }
+  __syncthreads();
+  for (int idx = tid; idx < n * mcols; idx += LEAF) {
+    int i, j;
+    if (br == 1) { i = idx % n; j = idx / n; } else { j = idx % mcols; i = idx / mcols; }
+    Bp[i * br + (long)(j0 + j) * bc] = sB[i][j];
+  }
+}
+
+template <typename T>
+__global__ void scale_strided_kernel(int n, int m, T alpha, T *B, long br, long bc) {
+  long total = (long)n * m;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    int i, j;
+    if (br == 1) { i = (int)(idx % n); j = (int)(idx / n); } else { j = (int)(idx % m); i = (int)(idx / m); }
+    B[i * br + (long)j * bc] *= alpha;
+  }
+}
+
+template <typename T>
+struct Eff {  // effective problem T*X = B
+  const T *Tp; long tr, tc;
+  T *Bp; long br, bc;
+  int lower, unit;
+};
+
+template <typename T>
+void gemm_call(SgemmFn fn, int ta, int tb, int M, int N, int K, T alpha, const T *A, long lda,
+               const T *B, long ldb, T beta, T *C, long ldc, cudaStream_t st);
+template <>
+void gemm_call<double>(SgemmFn, int ta, int tb, int M, int N, int K, double alpha,
+                       const double *A, long lda, const double *B, long ldb, double beta,
+                       double *C, long ldc, cudaStream_t st) {
+  dgemm_dev(ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, st, 0);
+}
+template <>
+void gemm_call<float>(SgemmFn fn, int ta, int tb, int M, int N, int K, float alpha,
+                      const float *A, long lda, const float *B, long ldb, float beta, float *C,
+                      long ldc, cudaStream_t st) {
+  (fn ? fn : sgemm_dev)(ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, st, 0);
+}
+
+// B2 (n2 x m) -= T21 (n2 x n1) * X1 (n1 x m), everything in effective strides.
+template <typename T>
+void eff_update(const Eff<T> &e, int r2, int n2, int r1, int n1, int m, SgemmFn fn,
+                cudaStream_t st) {
+  const T *T21 = e.Tp + r2 * e.tr + r1 * e.tc;
+  T *B2 = e.Bp + r2 * e.br;
+  const T *X1 = e.Bp + r1 * e.br;
+  if (e.br == 1) {  // B column-major (ld = bc)
+    int ta = (e.tr == 1) ? kNoTrans : kTrans;
+    long ldt = (e.tr == 1) ? e.tc : e.tr;
+    gemm_call<T>(fn, ta, kNoTrans, n2, m, n1, T(-1), T21, ldt, X1, e.bc, T(1), B2, e.bc, st);
+  } else {  // B^T column-major (m x n) with ld = br: B2^T -= X1^T * T21^T
+    int tb = (e.tc == 1) ? kNoTrans : kTrans;
+    long ldt = (e.tc == 1) ? e.tr : e.tc;
+    gemm_call<T>(fn, kNoTrans, tb, m, n2, n1, T(-1), X1, e.br, T21, ldt, T(1), B2, e.br, st);
+  }
+}
+
+template <typename T>
+void eff_solve(const Eff<T> &e, int r0, int n, int m, SgemmFn fn, cudaStream_t st) {
+  if (n <= 0 || m <= 0) return;
+  if (n <= LEAF) {
+    constexpr int smem = 2 * LEAF * (LEAF + 1) * (int)sizeof(T);
+    static bool configured = false;
+    if (!configured) {
+      ATLB_CUDA_CHECK(cudaFuncSetAttribute(trsm_leaf_kernel<T>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      configured = true;
+    }
+    trsm_leaf_kernel<T><<<cdiv(m, LEAF), LEAF, smem, st>>>(
+        n, m, e.Tp + r0 * e.tr + r0 * e.tc, e.tr, e.tc, e.Bp + r0 * e.br, e.br, e.bc, e.lower,
+        e.unit);
+    ATLB_CUDA_CHECK(cudaGetLastError());
+    return;
+  }
+  int n1 = std::max(LEAF, (n / 2) / LEAF * LEAF), n2 = n - n1;
+  if (e.lower) {
+    eff_solve(e, r0, n1, m, fn, st);
+    eff_update(e, r0 + n1, n2, r0, n1, m, fn, st);
+    eff_solve(e, r0 + n1, n2, m, fn, st);
+  } else {
+    eff_solve(e, r0 + n1, n2, m, fn, st);
+    eff_update(e, r0, n1, r0 + n1, n2, m, fn, st);
+    eff_solve(e, r0, n1, m, fn, st);
+  }
+}
+
+template <typename T>
+__global__ void laswp_kernel(int ncols, T *A, long lda, int k1, int k2, const int *__restrict__ ipiv,
+                             int inc) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncols) return;
+  T *col = A + (long)c * lda;
+  if (inc > 0) {
+    for (int k = k1; k < k2; k++) {
+      int p = ipiv[k];
+      if (p != k) { T t = col[k]; col[k] = col[p]; col[p] = t; }
+    }
+  } else {
+    for (int k = k2 - 1; k >= k1; k--) {
+      int p = ipiv[k];
+      if (p != k) { T t = col[k]; col[k] = col[p]; col[p] = t; }
+    }
+  }
+}
+
+// dense copy of op-free triangle: D = tri(A) with unit/zero handling
+__global__ void tri_to_dense_kernel(int n, const double *A, long lda, double *D, int uplo, int unit) {
+  long total = (long)n * n;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    int i = (int)(idx % n), j = (int)(idx / n);
+    double v;
+    if (i == j) v = unit ? 1.0 : A[i + (long)j * lda];
+    else if ((uplo == kLower) == (i > j)) v = A[i + (long)j * lda];
+    else v = 0.0;
+    D[idx] = v;
+  }
+}
+
+template <typename T>
+__global__ void copy2d_kernel(int M, int N, const T *S, long lds, T *D, long ldd) {
+  long total = (long)M * N;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    int i = (int)(idx % M), j = (int)(idx / M);
+    D[i + (long)j * ldd] = S[i + (long)j * lds];
+  }
+}
+
+template <typename T>
+__global__ void fill_zero_kernel(T *A, int M, int N, long lda) {
+  long total = (long)M * N;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x)
+    A[(idx % M) + (idx / M) * lda] = T(0);
+}
+
+__global__ void set_info_kernel(int *d) { *d = 0x7fffffff; }
+__global__ void finish_info_kernel(int *d) { if (*d == 0x7fffffff) *d = 0; }
+
+}  // namespace
+
+template <typename T>
+void trsm_dev(int side, int uplo, int trans, int diag, int M, int N, T alpha, const T *A, long lda,
+              T *B, long ldb, cudaStream_t st, SgemmFn gemm) {
+  if (M <= 0 || N <= 0) return;
+  const bool tr = trans != kNoTrans;
+  Eff<T> e;
+  e.Tp = A;
+  e.unit = diag == kUnit;
+  int n, m;
+  const bool opLower = (uplo == kLower) != tr;  // op(A) lower triangular?
+  if (side == kLeft) {  // op(A) X = B
+    e.tr = tr ? lda : 1; e.tc = tr ? 1 : lda;
+    e.Bp = B; e.br = 1; e.bc = ldb;
+    e.lower = opLower;
+    n = M; m = N;
+  } else {  // X op(A) = B  <=>  op(A)^T X^T = B^T
+    e.tr = tr ? 1 : lda; e.tc = tr ? lda : 1;
+    e.Bp = B; e.br = ldb; e.bc = 1;
+    e.lower = !opLower;
+    n = N; m = M;
+  }
+  if (alpha == T(0)) { fill_zero_dev<T>(B, M, N, ldb, st); return; }
+  if (alpha != T(1)) {
+    long total = (long)n * m;
+    scale_strided_kernel<T><<<(int)std::min<long>((total + 255) / 256, 4096), 256, 0, st>>>(
+        n, m, alpha, e.Bp, e.br, e.bc);
+    ATLB_CUDA_CHECK(cudaGetLastError());
+  }
+  eff_solve(e, 0, n, m, gemm, st);
+}
+
+template void trsm_dev<double>(int, int, int, int, int, int, double, const double *, long,
+                               double *, long, cudaStream_t, SgemmFn);
+template void trsm_dev<float>(int, int, int, int, int, int, float, const float *, long, float *,
+                              long, cudaStream_t, SgemmFn);
+
+void dtrmm_dev(int side, int uplo, int trans, int diag, int M, int N, double alpha,
+               const double *A, long lda, double *B, long ldb, cudaStream_t st) {
+  if (M <= 0 || N <= 0) return;
+  int n = side == kLeft ? M : N;
+  double *D = (double *)scratch(kSlotWork2, sizeof(double) * ((size_t)n * n + (size_t)M * N));
+  double *W = D + (size_t)n * n;
+  long tot = (long)n * n;
+  tri_to_dense_kernel<<<(int)std::min<long>((tot + 255) / 256, 4096), 256, 0, st>>>(
+      n, A, lda, D, uplo, diag == kUnit);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+  if (side == kLeft)
+    dgemm_dev(trans, kNoTrans, M, N, M, alpha, D, n, B, ldb, 0.0, W, M, st);
+  else
+    dgemm_dev(kNoTrans, trans, M, N, N, alpha, B, ldb, D, n, 0.0, W, M, st);
+  long tot2 = (long)M * N;
+  copy2d_kernel<double><<<(int)std::min<long>((tot2 + 255) / 256, 4096), 256, 0, st>>>(M, N, W, M, B, ldb);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
+
+template <typename T>
+void laswp_dev(int ncols, T *A, long lda, int k1, int k2, const int *ipiv, int inc,
+               cudaStream_t st) {
+  if (ncols <= 0 || k2 <= k1) return;
+  laswp_kernel<T><<<cdiv(ncols, 128), 128, 0, st>>>(ncols, A, lda, k1, k2, ipiv, inc);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
+template void laswp_dev<double>(int, double *, long, int, int, const int *, int, cudaStream_t);
+template void laswp_dev<float>(int, float *, long, int, int, const int *, int, cudaStream_t);
+
+template <typename T>
+void fill_zero_dev(T *A, int M, int N, long lda, cudaStream_t st) {
+  if (M <= 0 || N <= 0) return;
+  long total = (long)M * N;
+  fill_zero_kernel<T><<<(int)std::min<long>((total + 255) / 256, 4096), 256, 0, st>>>(A, M, N, lda);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
+template void fill_zero_dev<double>(double *, int, int, long, cudaStream_t);
+template void fill_zero_dev<float>(float *, int, int, long, cudaStream_t);
+
+void set_info_kernel_launch(int *d, cudaStream_t st) { set_info_kernel<<<1, 1, 0, st>>>(d); }
+void finish_info_kernel_launch(int *d, cudaStream_t st) { finish_info_kernel<<<1, 1, 0, st>>>(d); }
+
+}  // namespace atlb

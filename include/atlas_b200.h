@@ -1,0 +1,131 @@
+/*
+ * atlas_b200.h -- C ABI of libatlas_b200.so, a B200 (sm_100a) implementation
+ * of ATLAS's dense level-3 BLAS / LAPACK hot path.
+ *
+ * Part 1 declares the drop-in entry points with the reference's exact
+ * prototypes (each comment names the reference declaration it replaces).
+ * They take host pointers (device pointers are also accepted and used in
+ * place), compute on the GPU and return when the result is in the caller's
+ * buffers, like the CPU library.  Argument errors follow cblas_xerbla: a
+ * message on stderr and exit(-1), unless atlb_set_error_mode(1) (or the
+ * environment variable ATLAS_B200_XERBLA=return) makes them return instead.
+ *
+ * Part 2 declares extensions with no counterpart in the reference:
+ * device-pointer variants (asynchronous on the library's stream), the
+ * mixed-precision solvers, the split-integer (Ozaki) DGEMM, batched
+ * factorizations and the adjoints of potrf/potrs and getrf/getrs.
+ */
+#ifndef ATLAS_B200_H
+#define ATLAS_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#ifndef CBLAS_ENUM_DEFINED_H
+#define CBLAS_ENUM_DEFINED_H
+/* include/cblas.h:5-10 of the reference */
+enum CBLAS_ORDER { CblasRowMajor = 101, CblasColMajor = 102 };
+enum CBLAS_TRANSPOSE { CblasNoTrans = 111, CblasTrans = 112, CblasConjTrans = 113, AtlasConj = 114 };
+enum CBLAS_UPLO { CblasUpper = 121, CblasLower = 122 };
+enum CBLAS_DIAG { CblasNonUnit = 131, CblasUnit = 132 };
+enum CBLAS_SIDE { CblasLeft = 141, CblasRight = 142 };
+#endif
+
+/* ---------------------------------------------------------------- Part 1 */
+
+/* cblas_dgemm: include/cblas.h:471, interfaces/blas/C/src/cblas_dgemm.c:16-134 */
+void cblas_dgemm(const enum CBLAS_ORDER Order, const enum CBLAS_TRANSPOSE TransA,
+                 const enum CBLAS_TRANSPOSE TransB, const int M, const int N, const int K,
+                 const double alpha, const double *A, const int lda, const double *B,
+                 const int ldb, const double beta, double *C, const int ldc);
+/* cblas_sgemm: include/cblas.h:441, interfaces/blas/C/src/cblas_sgemm.c:131-133 */
+void cblas_sgemm(const enum CBLAS_ORDER Order, const enum CBLAS_TRANSPOSE TransA,
+                 const enum CBLAS_TRANSPOSE TransB, const int M, const int N, const int K,
+                 const float alpha, const float *A, const int lda, const float *B,
+                 const int ldb, const float beta, float *C, const int ldc);
+/* cblas_dtrsm: include/cblas.h:495, interfaces/blas/C/src/cblas_dtrsm.c:14-105 */
+void cblas_dtrsm(const enum CBLAS_ORDER Order, const enum CBLAS_SIDE Side,
+                 const enum CBLAS_UPLO Uplo, const enum CBLAS_TRANSPOSE TransA,
+                 const enum CBLAS_DIAG Diag, const int M, const int N, const double alpha,
+                 const double *A, const int lda, double *B, const int ldb);
+/* cblas_dtrmm: include/cblas.h:490, interfaces/blas/C/src/cblas_dtrmm.c:14 (used by larfb) */
+void cblas_dtrmm(const enum CBLAS_ORDER Order, const enum CBLAS_SIDE Side,
+                 const enum CBLAS_UPLO Uplo, const enum CBLAS_TRANSPOSE TransA,
+                 const enum CBLAS_DIAG Diag, const int M, const int N, const double alpha,
+                 const double *A, const int lda, double *B, const int ldb);
+/* cblas_dsyrk: include/cblas.h:481, interfaces/blas/C/src/cblas_dsyrk.c:14-90 */
+void cblas_dsyrk(const enum CBLAS_ORDER Order, const enum CBLAS_UPLO Uplo,
+                 const enum CBLAS_TRANSPOSE Trans, const int N, const int K, const double alpha,
+                 const double *A, const int lda, const double beta, double *C, const int ldc);
+
+/* clapack_dgetrf: include/clapack.h:63, interfaces/lapack/C/src/clapack_dgetrf.c:13-88 */
+int clapack_dgetrf(const enum CBLAS_ORDER Order, const int M, const int N, double *A,
+                   const int lda, int *ipiv);
+/* clapack_dgetrs: include/clapack.h:65, interfaces/lapack/C/src/clapack_dgetrs.c:57 */
+int clapack_dgetrs(const enum CBLAS_ORDER Order, const enum CBLAS_TRANSPOSE Trans, const int N,
+                   const int NRHS, const double *A, const int lda, const int *ipiv, double *B,
+                   const int ldb);
+/* clapack_dgesv: include/clapack.h:60, interfaces/lapack/C/src/clapack_dgesv.c:61-62 */
+int clapack_dgesv(const enum CBLAS_ORDER Order, const int N, const int NRHS, double *A,
+                  const int lda, int *ipiv, double *B, const int ldb);
+/* clapack_dpotrf: include/clapack.h:74, interfaces/lapack/C/src/clapack_dpotrf.c:43 */
+int clapack_dpotrf(const enum CBLAS_ORDER Order, const enum CBLAS_UPLO Uplo, const int N,
+                   double *A, const int lda);
+/* clapack_dpotrs: include/clapack.h:76, interfaces/lapack/C/src/clapack_dpotrs.c:56 */
+int clapack_dpotrs(const enum CBLAS_ORDER Order, const enum CBLAS_UPLO Uplo, const int N,
+                   const int NRHS, const double *A, const int lda, double *B, const int ldb);
+/* clapack_dposv: include/clapack.h:71, interfaces/lapack/C/src/clapack_dposv.c:57-58 */
+int clapack_dposv(const enum CBLAS_ORDER Order, const enum CBLAS_UPLO Uplo, const int N,
+                  const int NRHS, double *A, const int lda, double *B, const int ldb);
+/* clapack_dgeqrf: include/clapack.h:96, interfaces/lapack/C/src/clapack_dgeqrf.c:14-61 */
+int clapack_dgeqrf(const enum CBLAS_ORDER Order, const int M, const int N, double *A,
+                   const int lda, double *TAU);
+/* ATL_dgeqrf: src/lapack/ATL_geqrf.c:29-196 (LWORK < 0: workspace query) */
+int ATL_dgeqrf(const int M, const int N, double *A, const int lda, double *TAU, double *WORK,
+               const int LWORK);
+
+/* cblas_xerbla / cblas_errprn: interfaces/blas/C/src/cblas_xerbla.c:13-28,
+ * cblas_errprn.c (error reporting of the drop-in entry points) */
+void cblas_xerbla(int p, const char *rout, const char *form, ...);
+int cblas_errprn(int ierr, int info, char *form, ...);
+
+/* ---------------------------------------------------------------- Part 2 */
+
+/* Library control.  atlb_init(dev) selects the GPU (-1: keep the default,
+ * device 0 or $ATLAS_B200_DEVICE) and returns the device in use.  Error mode
+ * 0 = exit(-1) on a bad argument (the reference's behaviour), 1 = return the
+ * negative argument position.  Each host thread gets its own stream;
+ * atlb_set_stream() substitutes a caller's cudaStream_t (NULL: restore). */
+int atlb_init(int device);
+void atlb_set_error_mode(int mode);
+int atlb_get_error_mode(void);
+int atlb_last_error(void);
+int atlb_last_cuda_error(void);
+void *atlb_get_stream(void);
+void atlb_set_stream(void *stream);
+int atlb_sync(void);
+
+/* Device-pointer variants: column-major, all pointers in device memory,
+ * enqueued on the library stream and NOT synchronised.  Integer arguments
+ * use the CBLAS enum values.  Return 0, or -(position) of a bad argument.
+ * *dinfo (device) receives the LAPACK info value. */
+int atlb_dgemm_dev(int TransA, int TransB, int M, int N, int K, double alpha, const double *A,
+                   int lda, const double *B, int ldb, double beta, double *C, int ldc);
+int atlb_sgemm_dev(int TransA, int TransB, int M, int N, int K, float alpha, const float *A,
+                   int lda, const float *B, int ldb, float beta, float *C, int ldc);
+int atlb_dtrsm_dev(int Side, int Uplo, int TransA, int Diag, int M, int N, double alpha,
+                   const double *A, int lda, double *B, int ldb);
+int atlb_dsyrk_dev(int Uplo, int Trans, int N, int K, double alpha, const double *A, int lda,
+                   double beta, double *C, int ldc);
+int atlb_dgetrf_dev(int M, int N, double *A, int lda, int *ipiv, int *dinfo);
+int atlb_dgetrs_dev(int Trans, int N, int NRHS, const double *A, int lda, const int *ipiv,
+                    double *B, int ldb);
+int atlb_dpotrf_dev(int Uplo, int N, double *A, int lda, int *dinfo);
+int atlb_dpotrs_dev(int Uplo, int N, int NRHS, const double *A, int lda, double *B, int ldb);
+int atlb_dgeqrf_dev(int M, int N, double *A, int lda, double *tau);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ATLAS_B200_H */
