@@ -57,6 +57,7 @@ _SIGS = {
     "atlb_sync": (_I, []),
     "atlb_dgemm_dev": (_I, [_I, _I, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I]),
     "atlb_sgemm_dev": (_I, [_I, _I, _I, _I, _I, _F, _P, _I, _P, _I, _F, _P, _I]),
+    "atlb_sgemm_tc_dev": (_I, [_I, _I, _I, _I, _I, _I, _F, _P, _I, _P, _I, _F, _P, _I]),
     "atlb_dtrsm_dev": (_I, [_I, _I, _I, _I, _I, _I, _D, _P, _I, _P, _I]),
     "atlb_dsyrk_dev": (_I, [_I, _I, _I, _I, _D, _P, _I, _D, _P, _I]),
     "atlb_dgetrf_dev": (_I, [_I, _I, _P, _I, _P, _P]),
@@ -64,6 +65,8 @@ _SIGS = {
     "atlb_dpotrf_dev": (_I, [_I, _I, _P, _I, _P]),
     "atlb_dpotrs_dev": (_I, [_I, _I, _I, _P, _I, _P, _I]),
     "atlb_dgeqrf_dev": (_I, [_I, _I, _P, _I, _P]),
+    "atlb_dsgesv": (_I, [_I, _I, _P, _I, _P, _P, _I, _P, _I, _I, _P]),
+    "atlb_dsposv": (_I, [_I, _I, _I, _P, _I, _P, _I, _P, _I, _I, _P]),
 }
 
 

@@ -10,62 +10,12 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "../../include/atlas_b200.h"
+#include "staging.h"
 
 namespace atlb {
 void xerbla(int pos, const char *rout);
 
 namespace {
-
-bool is_dev(const void *p) {
-  if (!p) return false;
-  cudaPointerAttributes a;
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
-}
-
-template <typename T>
-struct DMat {
-  T *d;
-  long ld;
-  bool in_place;
-};
-
-// Bring a rows x cols column-major host matrix (leading dimension ld) to the
-// device; device pointers are used where they are.
-template <typename T>
-DMat<T> stage_in(int slot, const T *h, int rows, int cols, long ld, bool copy, cudaStream_t st) {
-  if (is_dev(h)) return {(T *)h, ld, true};
-  long dld = std::max(rows, 1);
-  T *d = (T *)scratch(slot, sizeof(T) * (size_t)dld * std::max(cols, 1));
-  if (copy && rows > 0 && cols > 0)
-    ATLB_CUDA_CHECK(cudaMemcpy2DAsync(d, dld * sizeof(T), h, ld * sizeof(T), rows * sizeof(T),
-                                      cols, cudaMemcpyHostToDevice, st));
-  return {d, dld, false};
-}
-
-template <typename T>
-void stage_out(T *h, long ld, const DMat<T> &m, int rows, int cols, cudaStream_t st) {
-  if (m.in_place || rows <= 0 || cols <= 0) return;
-  ATLB_CUDA_CHECK(cudaMemcpy2DAsync(h, ld * sizeof(T), m.d, m.ld * sizeof(T), rows * sizeof(T),
-                                    cols, cudaMemcpyDeviceToHost, st));
-}
-
-template <typename T>
-T *stage_vec_in(int slot, const T *h, int n, bool copy, cudaStream_t st) {
-  if (is_dev(h)) return (T *)h;
-  T *d = (T *)scratch(slot, sizeof(T) * std::max(n, 1));
-  if (copy && n > 0)
-    ATLB_CUDA_CHECK(cudaMemcpyAsync(d, h, sizeof(T) * n, cudaMemcpyHostToDevice, st));
-  return d;
-}
-template <typename T>
-void stage_vec_out(T *h, const T *d, int n, cudaStream_t st) {
-  if (h == d || n <= 0) return;
-  ATLB_CUDA_CHECK(cudaMemcpyAsync(h, d, sizeof(T) * n, cudaMemcpyDeviceToHost, st));
-}
 
 void sync(cudaStream_t st) { ATLB_CUDA_CHECK(cudaStreamSynchronize(st)); }
 
@@ -559,6 +509,23 @@ int atlb_sgemm_dev(int TA, int TB, int M, int N, int K, float alpha, const float
   if (ldc < std::max(1, M)) return -13;
   sgemm_dev(TA == kNoTrans ? kNoTrans : kTrans, TB == kNoTrans ? kNoTrans : kTrans, M, N, K, alpha,
             A, lda, B, ldb, beta, C, ldc, stream(), 0);
+  return 0;
+}
+
+int atlb_sgemm_tc_dev(int prec, int TA, int TB, int M, int N, int K, float alpha, const float *A,
+                      int lda, const float *B, int ldb, float beta, float *C, int ldc) {
+  if (prec != 1 && prec != 2) return -1;
+  if (bad_trans(TA)) return -2;
+  if (bad_trans(TB)) return -3;
+  if (M < 0) return -4;
+  if (N < 0) return -5;
+  if (K < 0) return -6;
+  if (lda < std::max(1, TA == kNoTrans ? M : K)) return -9;
+  if (ldb < std::max(1, TB == kNoTrans ? K : N)) return -11;
+  if (ldc < std::max(1, M)) return -14;
+  (prec == 1 ? sgemm_tf32_dev : sgemm_bf16_dev)(TA == kNoTrans ? kNoTrans : kTrans,
+                                                TB == kNoTrans ? kNoTrans : kTrans, M, N, K, alpha,
+                                                A, lda, B, ldb, beta, C, ldc, stream(), 0);
   return 0;
 }
 

@@ -1,0 +1,398 @@
+// Mixed-precision solvers: factor in FP32 on the GPU (trailing updates on the
+// tensor cores in TF32 or BF16 with FP32 accumulation, or exact FP32 FMA),
+// recover FP64 accuracy by iterative refinement.  FP64 is used only for the
+// residual r = b - A x, the solution update and the norms that decide
+// convergence.  No counterpart in the reference (ATLAS has no mixed-precision
+// solver); the interface and the fallback rule follow LAPACK's dsgesv /
+// dsposv: A and B are left unchanged when refinement succeeds; if it does
+// not converge (or the FP32 factorization breaks down) the FP64 solver is
+// used and `iter` is returned negative.
+//
+// Stopping rule: every right-hand side reaches a normwise backward error
+// ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= N * 2^-53.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+#include "common.cuh"
+#include "kernels.h"
+#include "mixed.h"
+#include "staging.h"
+#include "../../include/atlas_b200.h"
+
+namespace atlb {
+namespace {
+
+constexpr int ITERMAX = 30;
+
+__global__ void d2s_kernel(int M, int N, const double *__restrict__ A, long lda, float *__restrict__ S,
+                           long lds) {
+  long total = (long)M * N;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    int i = (int)(idx % M), j = (int)(idx / M);
+    S[i + (long)j * lds] = (float)A[i + (long)j * lda];
+  }
+}
+
+__global__ void add_s2d_kernel(int M, int N, const float *__restrict__ S, long lds, double *__restrict__ X,
+                               long ldx) {
+  long total = (long)M * N;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    int i = (int)(idx % M), j = (int)(idx / M);
+    X[i + (long)j * ldx] += (double)S[i + (long)j * lds];
+  }
+}
+
+__global__ void s2d_kernel(int M, int N, const float *__restrict__ S, long lds, double *__restrict__ X,
+                           long ldx) {
+  long total = (long)M * N;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    int i = (int)(idx % M), j = (int)(idx / M);
+    X[i + (long)j * ldx] = (double)S[i + (long)j * lds];
+  }
+}
+
+// partial row sums of |A| over column chunks: part[chunk * N + i]
+constexpr int GV_ROWS = 256, GV_COLS = 256;
+__global__ void __launch_bounds__(GV_ROWS)
+abs_rowsum_partial_kernel(int N, const double *__restrict__ A, long lda, double *__restrict__ part) {
+  const int i = blockIdx.x * GV_ROWS + threadIdx.x, c0 = blockIdx.y * GV_COLS;
+  if (i >= N) return;
+  double s = 0.0;
+  const int c1 = min(N, c0 + GV_COLS);
+  for (int c = c0; c < c1; c++) s += fabs(A[i + (long)c * lda]);
+  part[(long)blockIdx.y * N + i] = s;
+}
+
+// residual partials: part[(chunk * nrhs + r) * N + i] = sum_{c in chunk} A(i,c) X(c,r)
+template <int NR>
+__global__ void __launch_bounds__(GV_ROWS)
+gemv_partial_kernel(int N, int nrhs, const double *__restrict__ A, long lda,
+                    const double *__restrict__ X, long ldx, double *__restrict__ part) {
+  __shared__ double xs[GV_COLS][NR];
+  const int c0 = blockIdx.y * GV_COLS, i = blockIdx.x * GV_ROWS + threadIdx.x;
+  const int c1 = min(N, c0 + GV_COLS);
+  for (int t = threadIdx.x; t < GV_COLS * NR; t += GV_ROWS) {
+    int c = t / NR, r = t % NR;
+    xs[c][r] = (c0 + c < N && r < nrhs) ? X[(c0 + c) + (long)r * ldx] : 0.0;
+  }
+  __syncthreads();
+  if (i >= N) return;
+  double acc[NR];
+#pragma unroll
+  for (int r = 0; r < NR; r++) acc[r] = 0.0;
+  const double *a = A + i + (long)c0 * lda;
+  int c = c0;
+  for (; c + 4 <= c1; c += 4) {
+    double a0 = a[0], a1 = a[lda], a2 = a[2 * lda], a3 = a[3 * lda];
+    const int k = c - c0;
+#pragma unroll
+    for (int r = 0; r < NR; r++)
+      acc[r] = fma(a3, xs[k + 3][r], fma(a2, xs[k + 2][r], fma(a1, xs[k + 1][r], fma(a0, xs[k][r], acc[r]))));
+    a += 4 * lda;
+  }
+  for (; c < c1; c++) {
+    const double av = a[0];
+#pragma unroll
+    for (int r = 0; r < NR; r++) acc[r] = fma(av, xs[c - c0][r], acc[r]);
+    a += lda;
+  }
+#pragma unroll
+  for (int r = 0; r < NR; r++)
+    if (r < nrhs) part[((long)blockIdx.y * nrhs + r) * N + i] = acc[r];
+}
+
+// R = B - sum of partials (fixed order: deterministic); also per-RHS maxima of
+// |R| and |X| and |B| into red[3*r + {0,1,2}] via atomicMax on the bit patterns
+__global__ void resid_finish_kernel(int N, int nrhs, int nchunks, const double *__restrict__ part,
+                                    const double *__restrict__ B, long ldb,
+                                    const double *__restrict__ X, long ldx, double *__restrict__ R,
+                                    long ldr, unsigned long long *__restrict__ red) {
+  const int r = blockIdx.y;
+  double mr = 0.0, mx = 0.0, mb = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int ch = 0; ch < nchunks; ch++) s += part[((long)ch * nrhs + r) * N + i];
+    const double b = B[i + (long)r * ldb];
+    const double v = b - s;
+    R[i + (long)r * ldr] = v;
+    mr = fmax(mr, fabs(v));
+    mx = fmax(mx, fabs(X[i + (long)r * ldx]));
+    mb = fmax(mb, fabs(b));
+  }
+  for (int o = 16; o; o >>= 1) {
+    mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    mb = fmax(mb, __shfl_xor_sync(0xffffffffu, mb, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    // non-negative doubles order like their bit patterns
+    atomicMax(&red[3 * r + 0], (unsigned long long)__double_as_longlong(mr));
+    atomicMax(&red[3 * r + 1], (unsigned long long)__double_as_longlong(mx));
+    atomicMax(&red[3 * r + 2], (unsigned long long)__double_as_longlong(mb));
+  }
+}
+
+__global__ void rowsum_finish_kernel(int N, int nchunks, const double *__restrict__ part,
+                                     unsigned long long *__restrict__ out) {
+  double m = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int ch = 0; ch < nchunks; ch++) s += part[(long)ch * N + i];
+    m = fmax(m, s);
+  }
+  for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+__global__ void symmetrize_kernel(int uplo, int N, const double *__restrict__ A, long lda,
+                                  double *__restrict__ F, long ldf) {
+  long total = (long)N * N;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    int i = (int)(idx % N), j = (int)(idx / N);
+    bool stored = (uplo == kLower) ? (i >= j) : (i <= j);
+    F[i + (long)j * ldf] = stored ? A[i + (long)j * lda] : A[j + (long)i * lda];
+  }
+}
+
+inline int grid_for(long total) { return (int)std::min<long>((total + 255) / 256, 148L * 8); }
+
+}  // namespace
+
+void symmetrize_dev(int uplo, int N, const double *A, long lda, double *F, long ldf, cudaStream_t st) {
+  symmetrize_kernel<<<grid_for((long)N * N), 256, 0, st>>>(uplo, N, A, lda, F, ldf);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
+
+SgemmFn factor_gemm(int prec) {
+  if (prec == kPrecTF32) return sgemm_tf32_dev;
+  if (prec == kPrecBF16) return sgemm_bf16_dev;
+  return sgemm_dev;
+}
+
+// ||A||_inf (FP64) into *out (device, as bits), using part (N * ceil(N/256) doubles)
+void dnorm_inf_dev(int N, const double *A, long lda, double *part, unsigned long long *out,
+                   cudaStream_t st) {
+  const int nch = cdiv(N, GV_COLS);
+  ATLB_CUDA_CHECK(cudaMemsetAsync(out, 0, sizeof(unsigned long long), st));
+  abs_rowsum_partial_kernel<<<dim3(cdiv(N, GV_ROWS), nch), GV_ROWS, 0, st>>>(N, A, lda, part);
+  rowsum_finish_kernel<<<std::min(cdiv(N, 256), 148), 256, 0, st>>>(N, nch, part, out);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
+
+// R = B - A X; red[3r..3r+2] = max|R_r|, max|X_r|, max|B_r| (right-hand
+// sides are processed 8 at a time; part holds ceil(N/256) * 8 * N doubles)
+void dresid_dev(int N, int nrhs, const double *A, long lda, const double *X, long ldx,
+                const double *B, long ldb, double *R, long ldr, double *part,
+                unsigned long long *red, cudaStream_t st) {
+  const int nch = cdiv(N, GV_COLS);
+  ATLB_CUDA_CHECK(cudaMemsetAsync(red, 0, sizeof(unsigned long long) * 3 * nrhs, st));
+  dim3 grid(cdiv(N, GV_ROWS), nch);
+  for (int r0 = 0; r0 < nrhs; r0 += 8) {
+    const int nr = std::min(8, nrhs - r0);
+    const double *Xr = X + (long)r0 * ldx;
+    if (nr <= 1) gemv_partial_kernel<1><<<grid, GV_ROWS, 0, st>>>(N, nr, A, lda, Xr, ldx, part);
+    else if (nr <= 4) gemv_partial_kernel<4><<<grid, GV_ROWS, 0, st>>>(N, nr, A, lda, Xr, ldx, part);
+    else gemv_partial_kernel<8><<<grid, GV_ROWS, 0, st>>>(N, nr, A, lda, Xr, ldx, part);
+    resid_finish_kernel<<<dim3(std::min(cdiv(N, 256), 64), nr), 256, 0, st>>>(
+        N, nr, nch, part, B + (long)r0 * ldb, ldb, Xr, ldx, R + (long)r0 * ldr, ldr, red + 3 * r0);
+  }
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
+
+void d2s_dev(int M, int N, const double *A, long lda, float *S, long lds, cudaStream_t st) {
+  d2s_kernel<<<grid_for((long)M * N), 256, 0, st>>>(M, N, A, lda, S, lds);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
+void s2d_dev(int M, int N, const float *S, long lds, double *X, long ldx, cudaStream_t st) {
+  s2d_kernel<<<grid_for((long)M * N), 256, 0, st>>>(M, N, S, lds, X, ldx);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
+void add_s2d_dev(int M, int N, const float *S, long lds, double *X, long ldx, cudaStream_t st) {
+  add_s2d_kernel<<<grid_for((long)M * N), 256, 0, st>>>(M, N, S, lds, X, ldx);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
+
+// Refinement driver shared by dsgesv and dsposv.  `factor` factors the FP32
+// copy (returns info), `solve` solves in FP32 in place; A, B, X device.
+template <class Factor, class Solve, class Fallback>
+int refine(int N, int nrhs, const double *A, long lda, const double *B, long ldb, double *X,
+           long ldx, int *iter, Factor factor, Solve solve, Fallback fallback, cudaStream_t st,
+           MixedStats *stats) {
+  const int nch = cdiv(N, GV_COLS);
+  const long lds = N;
+  float *S = (float *)scratch(kSlotMixedA, sizeof(float) * (size_t)N * N);
+  float *Rs = (float *)scratch(kSlotMixedX, sizeof(float) * (size_t)N * nrhs);
+  double *R = (double *)scratch(kSlotMixedR, sizeof(double) * (size_t)N * nrhs);
+  double *part = (double *)scratch(kSlotMixedD, sizeof(double) * (size_t)nch * N * 8 + 64);
+  unsigned long long *red = (unsigned long long *)scratch(kSlotWork2, sizeof(unsigned long long) * (3 * nrhs + 8));
+  unsigned long long *hred = (unsigned long long *)pinned(kSlotWork2, sizeof(unsigned long long) * (3 * nrhs + 8));
+
+  dnorm_inf_dev(N, A, lda, part, red + 3 * nrhs, st);
+  d2s_dev(N, N, A, lda, S, lds, st);
+  int finfo = factor(S, lds);
+  double anrm = 0.0;
+  {
+    ATLB_CUDA_CHECK(cudaMemcpyAsync(hred, red + 3 * nrhs, 8, cudaMemcpyDeviceToHost, st));
+    ATLB_CUDA_CHECK(cudaStreamSynchronize(st));
+    anrm = bits_to_double(hred[0]);
+  }
+  const double tol = N * std::ldexp(1.0, -53);
+  if (finfo == 0) {
+    // x0 = solve(b) in FP32
+    d2s_dev(N, nrhs, B, ldb, Rs, N, st);
+    solve(S, lds, Rs, N);
+    s2d_dev(N, nrhs, Rs, N, X, ldx, st);
+    for (int it = 0; it <= ITERMAX; it++) {
+      dresid_dev(N, nrhs, A, lda, X, ldx, B, ldb, R, N, part, red, st);
+      ATLB_CUDA_CHECK(cudaMemcpyAsync(hred, red, sizeof(unsigned long long) * 3 * nrhs,
+                                      cudaMemcpyDeviceToHost, st));
+      ATLB_CUDA_CHECK(cudaStreamSynchronize(st));
+      bool ok = true;
+      double worst = 0.0;
+      for (int r = 0; r < nrhs; r++) {
+        double rn = bits_to_double(hred[3 * r]), xn = bits_to_double(hred[3 * r + 1]),
+               bn = bits_to_double(hred[3 * r + 2]);
+        double den = anrm * xn + bn;
+        double eta = den > 0 ? rn / den : rn;
+        if (!(eta <= tol)) ok = false;
+        worst = std::max(worst, std::isfinite(eta) ? eta : 1e300);
+      }
+      if (stats) { stats->bwd_err = worst; stats->anrm = anrm; }
+      if (ok) {
+        *iter = it;
+        return 0;
+      }
+      if (it == ITERMAX) break;
+      d2s_dev(N, nrhs, R, N, Rs, N, st);
+      solve(S, lds, Rs, N);
+      add_s2d_dev(N, nrhs, Rs, N, X, ldx, st);
+    }
+    *iter = -(ITERMAX + 1);
+  } else {
+    *iter = -3;  // FP32 factorization broke down (LAPACK dsgesv: ITER = -3)
+  }
+  return fallback();
+}
+
+}  // namespace atlb
+
+using namespace atlb;
+
+namespace {
+int read_info(const int *dinfo, cudaStream_t st) {
+  int *h = (int *)pinned(kSlotInfo, 64);
+  ATLB_CUDA_CHECK(cudaMemcpyAsync(h, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st));
+  ATLB_CUDA_CHECK(cudaStreamSynchronize(st));
+  return *h;
+}
+}  // namespace
+
+extern "C" {
+
+int atlb_dsgesv(int N, int NRHS, double *A, int lda, int *ipiv, double *B, int ldb, double *X,
+                int ldx, int prec, int *iter) {
+  if (N < 0) return -1;
+  if (NRHS < 0) return -2;
+  if (lda < std::max(1, N)) return -4;
+  if (ldb < std::max(1, N)) return -7;
+  if (ldx < std::max(1, N)) return -9;
+  if (prec < kPrecFP32 || prec > kPrecBF16) return -10;
+  int it_local = 0;
+  if (!iter) iter = &it_local;
+  *iter = 0;
+  if (N == 0 || NRHS == 0) return 0;
+  cudaStream_t st = stream();
+  DMat<double> dA = stage_in(kSlotA, (const double *)A, N, N, lda, true, st);
+  DMat<double> dB = stage_in(kSlotB, (const double *)B, N, NRHS, ldb, true, st);
+  DMat<double> dX = stage_in(kSlotC, (const double *)X, N, NRHS, ldx, false, st);
+  int *dip = stage_vec_in<int>(kSlotIpiv, ipiv, N, false, st);
+  int *dinfo = (int *)scratch(kSlotInfo, 64);
+  SgemmFn g = factor_gemm(prec);
+  auto factor = [&](float *S, long lds) {
+    getrf_dev<float>(N, N, S, lds, dip, dinfo, st, g);
+    return read_info(dinfo, st);
+  };
+  auto solve = [&](const float *S, long lds, float *R, long ldr) {
+    getrs_dev<float>(kNoTrans, N, NRHS, S, lds, dip, R, ldr, st, g);
+  };
+  bool fell_back = false;
+  auto fallback = [&]() {
+    // FP64 dgesv on A itself (LAPACK dsgesv: A then holds the FP64 factors)
+    fell_back = true;
+    getrf_dev<double>(N, N, dA.d, dA.ld, dip, dinfo, st);
+    int info = read_info(dinfo, st);
+    if (info == 0) {
+      for (int r = 0; r < NRHS; r++)
+        ATLB_CUDA_CHECK(cudaMemcpyAsync(dX.d + (long)r * dX.ld, dB.d + (long)r * dB.ld,
+                                        sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+      getrs_dev<double>(kNoTrans, N, NRHS, dA.d, dA.ld, dip, dX.d, dX.ld, st);
+    }
+    return info;
+  };
+  int info = refine(N, NRHS, dA.d, dA.ld, dB.d, dB.ld, dX.d, dX.ld, iter, factor, solve, fallback, st,
+                    nullptr);
+  stage_out(X, ldx, dX, N, NRHS, st);
+  if (fell_back) {
+    stage_out(A, lda, dA, N, N, st);
+    stage_vec_out<int>(ipiv, dip, N, st);
+  }
+  ATLB_CUDA_CHECK(cudaStreamSynchronize(st));
+  return info;
+}
+
+int atlb_dsposv(int Uplo, int N, int NRHS, double *A, int lda, double *B, int ldb, double *X,
+                int ldx, int prec, int *iter) {
+  if (Uplo != kUpper && Uplo != kLower) return -1;
+  if (N < 0) return -2;
+  if (NRHS < 0) return -3;
+  if (lda < std::max(1, N)) return -5;
+  if (ldb < std::max(1, N)) return -7;
+  if (ldx < std::max(1, N)) return -9;
+  if (prec < kPrecFP32 || prec > kPrecBF16) return -10;
+  int it_local = 0;
+  if (!iter) iter = &it_local;
+  *iter = 0;
+  if (N == 0 || NRHS == 0) return 0;
+  cudaStream_t st = stream();
+  DMat<double> dA = stage_in(kSlotA, (const double *)A, N, N, lda, true, st);
+  DMat<double> dB = stage_in(kSlotB, (const double *)B, N, NRHS, ldb, true, st);
+  DMat<double> dX = stage_in(kSlotC, (const double *)X, N, NRHS, ldx, false, st);
+  int *dinfo = (int *)scratch(kSlotInfo, 64);
+  SgemmFn g = factor_gemm(prec);
+  // The residual needs all of A: the other triangle is taken from the
+  // referenced one by symmetry (a full symmetric copy, FP64).
+  double *Af = (double *)scratch(kSlotWork, sizeof(double) * (size_t)N * N);
+  symmetrize_dev(Uplo, N, dA.d, dA.ld, Af, N, st);
+  auto factor = [&](float *S, long lds) {
+    potrf_dev<float>(Uplo, N, S, lds, dinfo, st, g);
+    return read_info(dinfo, st);
+  };
+  auto solve = [&](const float *S, long lds, float *R, long ldr) {
+    potrs_dev<float>(Uplo, N, NRHS, S, lds, R, ldr, st, g);
+  };
+  bool fell_back = false;
+  auto fallback = [&]() {
+    fell_back = true;
+    potrf_dev<double>(Uplo, N, dA.d, dA.ld, dinfo, st);
+    int info = read_info(dinfo, st);
+    if (info == 0) {
+      for (int r = 0; r < NRHS; r++)
+        ATLB_CUDA_CHECK(cudaMemcpyAsync(dX.d + (long)r * dX.ld, dB.d + (long)r * dB.ld,
+                                        sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+      potrs_dev<double>(Uplo, N, NRHS, dA.d, dA.ld, dX.d, dX.ld, st);
+    }
+    return info;
+  };
+  int info = refine(N, NRHS, Af, N, dB.d, dB.ld, dX.d, dX.ld, iter, factor, solve, fallback, st,
+                    nullptr);
+  stage_out(X, ldx, dX, N, NRHS, st);
+  if (fell_back) stage_out(A, lda, dA, N, N, st);
+  ATLB_CUDA_CHECK(cudaStreamSynchronize(st));
+  return info;
+}
+
+}  // extern "C"

@@ -157,8 +157,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="atlas", choices=["atlas", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--n", type=int, default=N, help="matrix order (default 8192; smaller for profiling)")
+    ap.add_argument("--skip-e2e", action="store_true", help="omit the host-buffer leg (profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    n = args.n
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -179,21 +182,23 @@ def main():
     import atlas_b200 as AB
     AB.lib()
     AB.atlb_init(local)
-    stream = torch.cuda.current_stream()
+    # one non-default stream shared by torch (inputs, events) and the library
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
     AB.atlb_set_stream(stream.cuda_stream)
 
-    acol0, b0 = make_system(torch, N, KAPPA, 1234 + rank, dev)
+    acol0, b0 = make_system(torch, n, KAPPA, 1234 + rank, dev)
     A = torch.empty_like(acol0)
     x = torch.empty_like(b0)
-    ipiv = torch.empty(N, dtype=torch.int32, device=dev)
+    ipiv = torch.empty(n, dtype=torch.int32, device=dev)
     info = torch.zeros(1, dtype=torch.int32, device=dev)
     launches = {"n": 0}
 
     def step():
         A.copy_(acol0)
         x.copy_(b0)
-        AB.atlb_dgetrf_dev(N, N, A, N, ipiv, info)
-        AB.atlb_dgetrs_dev(111, N, 1, A, N, ipiv, x, N)
+        AB.atlb_dgetrf_dev(n, n, A, n, ipiv, info)
+        AB.atlb_dgetrs_dev(111, n, 1, A, n, ipiv, x, n)
 
     for _ in range(args.warmup):
         step()
@@ -248,22 +253,24 @@ def main():
     del ga, gb, gc
 
     # end to end through the drop-in C ABI with pinned host buffers
-    ha = torch.empty(N * N, dtype=torch.float64, pin_memory=True)
-    hb = torch.empty(N, dtype=torch.float64, pin_memory=True)
-    ha_src = acol0.reshape(-1).cpu()
-    hb_src = b0.cpu()
-    hip = np.zeros(N, dtype=np.int32)
-    e2e_t = []
-    for i in range(2 + max(2, args.steps // 3)):
-        ha.copy_(ha_src)
-        hb.copy_(hb_src)
-        t0 = time.perf_counter()
-        r = AB.clapack_dgesv(AB.CblasColMajor, N, 1, ha, N, hip, hb, N)
-        t1 = time.perf_counter()
-        assert r == 0
-        if i >= 2:
-            e2e_t.append(t1 - t0)
-    e2e_val = world / (sum(e2e_t) / len(e2e_t))
+    e2e_val = None
+    if not args.skip_e2e:
+        ha = torch.empty(n * n, dtype=torch.float64, pin_memory=True)
+        hb = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        ha_src = acol0.reshape(-1).cpu()
+        hb_src = b0.cpu()
+        hip = np.zeros(n, dtype=np.int32)
+        e2e_t = []
+        for i in range(2 + max(2, args.steps // 3)):
+            ha.copy_(ha_src)
+            hb.copy_(hb_src)
+            t0 = time.perf_counter()
+            r = AB.clapack_dgesv(AB.CblasColMajor, n, 1, ha, n, hip, hb, n)
+            t1 = time.perf_counter()
+            assert r == 0
+            if i >= 2:
+                e2e_t.append(t1 - t0)
+        e2e_val = world / (sum(e2e_t) / len(e2e_t))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -280,27 +287,27 @@ def main():
             lu, ip, _ = O.dgetrf(a)
             O.dgetrs(111, lu, ip, bb.copy(order="F"))
             ts.append(time.perf_counter() - t0)
-        tcpu = min(ts) * lu_flops(N) / lu_flops(ns)
+        tcpu = min(ts) * lu_flops(n) / lu_flops(ns)
         cpu = {"value": 1.0 / tcpu, "unit": "solves/s (N=8192, 1 RHS)", "cores": cores, "kind": "port",
-               "sample": f"oracle getrf+getrs N={ns}, scaled by flop ratio to N={N}"}
+               "sample": f"oracle getrf+getrs N={ns}, scaled by flop ratio to N={n}"}
 
     if rank == 0:
-        gflops = lu_flops(N) / (ms * 1e-3) / 1e9
+        gflops = lu_flops(n) / (ms * 1e-3) / 1e9
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s (N=8192, 1 RHS)", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, on device)",
             "config": {"workload": "dgesv N=8192 1 RHS, FP64 getrf+getrs (kappa=1e2 Q1 diag(s) Q2^T)",
-                       "n": N, "nrhs": 1, "kappa": KAPPA, "parallelism": f"replicas x{world}",
+                       "n": n, "nrhs": 1, "kappa": KAPPA, "parallelism": f"replicas x{world}",
                        "l2": "inputs 512 MiB > L2, no flush"},
-            "fp64_dgesv_gflops": gflops, "backward_error": berr, "bwd_err_bound": N * 2.0 ** -53,
+            "fp64_dgesv_gflops": gflops, "backward_error": berr, "bwd_err_bound": n * 2.0 ** -53,
             "dgemm_8192": {"ms": dgemm_ms, "tflops": dgemm_tf, "cublas_fp64_tflops": cublas_tf},
             "roofline": {"bound": "tensor", "achieved": dgemm_tf, "peak": cublas_tf, "unit": "TFLOP/s",
                          "frac": dgemm_tf / cublas_tf, "traffic": None,
                          "peak_note": "FP64: no measured peak in MEASURED_PEAKS.json; denominator = cuBLAS DGEMM 8192^3 measured in this run"},
             "clocks": clk.summary(),
-            "e2e": {"value": e2e_val, "unit": "solves/s (N=8192, 1 RHS)", "h2d_bytes_per_step": N * N * 8 + N * 8,
-                    "d2h_bytes_per_step": N * N * 8 + N * 8 + N * 4},
+            "e2e": {"value": e2e_val, "unit": "solves/s (N=8192, 1 RHS)", "h2d_bytes_per_step": n * n * 8 + n * 8,
+                    "d2h_bytes_per_step": n * n * 8 + n * 8 + n * 4},
             "cpu_baseline": cpu,
             "gpu_launches": None,
         }

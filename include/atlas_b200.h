@@ -114,6 +114,11 @@ int atlb_dgemm_dev(int TransA, int TransB, int M, int N, int K, double alpha, co
                    int lda, const double *B, int ldb, double beta, double *C, int ldc);
 int atlb_sgemm_dev(int TransA, int TransB, int M, int N, int K, float alpha, const float *A,
                    int lda, const float *B, int ldb, float beta, float *C, int ldc);
+/* FP32 GEMM on the tensor cores: operands rounded to TF32 (prec 1) or BF16
+ * (prec 2), FP32 accumulation (tcgen05, TMEM accumulators). */
+int atlb_sgemm_tc_dev(int prec, int TransA, int TransB, int M, int N, int K, float alpha,
+                      const float *A, int lda, const float *B, int ldb, float beta, float *C,
+                      int ldc);
 int atlb_dtrsm_dev(int Side, int Uplo, int TransA, int Diag, int M, int N, double alpha,
                    const double *A, int lda, double *B, int ldb);
 int atlb_dsyrk_dev(int Uplo, int Trans, int N, int K, double alpha, const double *A, int lda,
@@ -124,6 +129,21 @@ int atlb_dgetrs_dev(int Trans, int N, int NRHS, const double *A, int lda, const 
 int atlb_dpotrf_dev(int Uplo, int N, double *A, int lda, int *dinfo);
 int atlb_dpotrs_dev(int Uplo, int N, int NRHS, const double *A, int lda, double *B, int ldb);
 int atlb_dgeqrf_dev(int M, int N, double *A, int lda, double *tau);
+
+/* Mixed-precision solvers (no counterpart in the reference; LAPACK's
+ * dsgesv/dsposv contract).  Factor an FP32 copy of A on the GPU -- trailing
+ * updates in FP32 (prec 0), on the tensor cores in TF32 (1) or BF16 with FP32
+ * accumulation (2) -- then refine in FP64 until every column reaches a
+ * normwise backward error ||b-Ax||_inf/(||A||_inf ||x||_inf + ||b||_inf) <=
+ * N*2^-53.  A and B are unchanged and *iter >= 0 (refinement steps) on
+ * success; otherwise the FP64 solver runs, A/ipiv hold its factors and *iter
+ * < 0 (-3: FP32 factorization broke down, -31: no convergence).  Returns
+ * info (0, > 0 singular / not positive definite, < 0 bad argument).  Host or
+ * device pointers; synchronous. */
+int atlb_dsgesv(int N, int NRHS, double *A, int lda, int *ipiv, double *B, int ldb, double *X,
+                int ldx, int prec, int *iter);
+int atlb_dsposv(int Uplo, int N, int NRHS, double *A, int lda, double *B, int ldb, double *X,
+                int ldx, int prec, int *iter);
 
 #ifdef __cplusplus
 }

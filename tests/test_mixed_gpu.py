@@ -1,0 +1,88 @@
+"""Mixed-precision solvers (FP32 / TF32 / BF16 factorization + FP64
+iterative refinement): the solution reaches a normwise backward error
+<= N * 2^-53 (the criterion the refinement stops on, recomputed here on the
+host in FP64), A and B are left unchanged when refinement succeeds, and the
+FP64 fallback engages (iter < 0) when it cannot."""
+import numpy as np
+import pytest
+
+import atlas_b200 as AB
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def kappa_matrix(n, kappa, seed):
+    rng = np.random.default_rng(seed)
+    q1, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    q2, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    s = np.logspace(0, -np.log10(kappa), n)
+    return np.asfortranarray((q1 * s) @ q2.T)
+
+
+def bwd_err(a, x, b):
+    r = b - a @ x
+    return np.max(np.abs(r), axis=0) / (np.max(np.sum(np.abs(a), axis=1)) * np.max(np.abs(x), axis=0)
+                                        + np.max(np.abs(b), axis=0))
+
+
+@pytest.mark.parametrize("prec", [0, 1, 2])
+@pytest.mark.parametrize("n,nrhs", [(300, 1), (1000, 3)])
+def test_dsgesv_kappa_1e2(gpu, prec, n, nrhs):
+    a0 = kappa_matrix(n, 1e2, n + prec)
+    b0 = np.asfortranarray(np.random.default_rng(5).uniform(-1, 1, (n, nrhs)))
+    a, b = a0.copy(order="F"), b0.copy(order="F")
+    x = np.zeros((n, nrhs), order="F")
+    ipiv = np.zeros(n, dtype=np.int32)
+    it = np.zeros(1, dtype=np.int32)
+    info = AB.atlb_dsgesv(n, nrhs, a, n, ipiv, b, n, x, n, prec, it)
+    assert info == 0
+    assert it[0] >= 0, f"refinement did not converge (iter={it[0]})"
+    assert np.all(bwd_err(a0, x, b0) <= n * 2.0 ** -53)
+    assert np.array_equal(a, a0) and np.array_equal(b, b0)
+
+
+def test_dsgesv_bf16_kappa_1e6_falls_back_or_converges(gpu):
+    n = 400
+    a0 = kappa_matrix(n, 1e6, 9)
+    b0 = np.asfortranarray(np.random.default_rng(6).uniform(-1, 1, (n, 1)))
+    a, b = a0.copy(order="F"), b0.copy(order="F")
+    x = np.zeros((n, 1), order="F")
+    ipiv = np.zeros(n, dtype=np.int32)
+    it = np.zeros(1, dtype=np.int32)
+    assert AB.atlb_dsgesv(n, 1, a, n, ipiv, b, n, x, n, 2, it) == 0
+    assert np.all(bwd_err(a0, x, b0) <= n * 2.0 ** -53)
+    if it[0] < 0:   # FP64 fallback: A holds the FP64 factors, like dgesv
+        ref, rpiv, _ = O.dgetrf(a0.copy(order="F"))
+        np.testing.assert_array_equal(ipiv, rpiv)
+
+
+def test_dsgesv_singular(gpu):
+    n = 64
+    a0 = O.lu_matrix(n, 3)
+    a0[:, 10] = 0.0
+    x = np.zeros((n, 1), order="F")
+    b = np.ones((n, 1), order="F")
+    it = np.zeros(1, dtype=np.int32)
+    ipiv = np.zeros(n, dtype=np.int32)
+    assert AB.atlb_dsgesv(n, 1, a0.copy(order="F"), n, ipiv, b, n, x, n, 1, it) == 11
+    assert it[0] == -3
+
+
+@pytest.mark.parametrize("prec", [0, 1, 2])
+@pytest.mark.parametrize("uplo", [121, 122])
+def test_dsposv(gpu, prec, uplo):
+    n, nrhs = 500, 2
+    g = np.random.default_rng(prec + uplo).standard_normal((n, n))
+    a0 = np.asfortranarray(g @ g.T / n + np.eye(n))
+    b0 = np.asfortranarray(np.random.default_rng(1).uniform(-1, 1, (n, nrhs)))
+    a = a0.copy(order="F")
+    tri = np.triu(np.ones((n, n), bool), 1) if uplo == 122 else np.tril(np.ones((n, n), bool), -1)
+    a[tri] = np.nan       # the unreferenced triangle must not be read
+    a_in = a.copy(order="F")
+    x = np.zeros((n, nrhs), order="F")
+    it = np.zeros(1, dtype=np.int32)
+    assert AB.atlb_dsposv(uplo, n, nrhs, a, n, b0, n, x, n, prec, it) == 0
+    assert it[0] >= 0
+    assert np.all(bwd_err(a0, x, b0) <= n * 2.0 ** -53)
+    np.testing.assert_array_equal(np.isnan(a), np.isnan(a_in))
