@@ -96,10 +96,30 @@ void potrf_rec(int upper, int off, int N, T *A, long lda, int *dinfo, cudaStream
 
 }  // namespace
 
+// Outer loop: NBO-wide diagonal blocks factored by the recursion above, then
+// one TRSM for the block column below (right of) the diagonal block and one
+// SYRK for the trailing matrix.
+constexpr int NBO = 256;
+
 template <typename T>
 void potrf_dev(int uplo, int N, T *A, long lda, int *dinfo, cudaStream_t st, SgemmFn gemm) {
   set_info_kernel_launch(dinfo, st);
-  potrf_rec<T>(uplo == kUpper, 0, N, A, lda, dinfo, st, gemm);
+  const bool up = uplo == kUpper;
+  for (int j = 0; j < N; j += NBO) {
+    const int jb = std::min(NBO, N - j), nr = N - j - jb;
+    T *Ad = A + j + (long)j * lda;
+    potrf_rec<T>(up, j, jb, A, lda, dinfo, st, gemm);
+    if (nr <= 0) break;
+    if (!up) {
+      T *A21 = Ad + jb, *A22 = Ad + jb + (long)jb * lda;
+      trsm_dev<T>(kRight, kLower, kTrans, kNonUnit, nr, jb, T(1), Ad, lda, A21, lda, st, gemm);
+      syrk_update(gemm, 0, nr, jb, A21, A22, lda, st);
+    } else {
+      T *A12 = Ad + (long)jb * lda, *A22 = Ad + jb + (long)jb * lda;
+      trsm_dev<T>(kLeft, kUpper, kTrans, kNonUnit, jb, nr, T(1), Ad, lda, A12, lda, st, gemm);
+      syrk_update(gemm, 1, nr, jb, A12, A22, lda, st);
+    }
+  }
   finish_info_kernel_launch(dinfo, st);
 }
 template void potrf_dev<double>(int, int, double *, long, int *, cudaStream_t, SgemmFn);

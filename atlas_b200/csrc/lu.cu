@@ -348,11 +348,31 @@ void getrf_rec(int off, int M, int N, T *A, long lda, int *ipiv, int *dinfo, cud
 
 }  // namespace
 
+// Outer loop: NBO-column block panels, each factored by the recursion above
+// (restricted to the panel's columns); the panel's row interchanges are then
+// applied to the columns on both sides and the trailing matrix is updated with
+// one TRSM and one large GEMM (the reference's recursion would issue the same
+// updates as a cascade of smaller ones; the pivots are the same).
+constexpr int NBO = 256;
+
 template <typename T>
 void getrf_dev(int M, int N, T *A, long lda, int *ipiv, int *dinfo, cudaStream_t st,
                SgemmFn gemm) {
   set_info_kernel_launch(dinfo, st);
-  getrf_rec<T>(0, M, N, A, lda, ipiv, dinfo, st, gemm);
+  const int MN = std::min(M, N);
+  for (int j = 0; j < MN; j += NBO) {
+    const int jb = std::min(NBO, MN - j);
+    T *Ad = A + j + (long)j * lda;
+    getrf_rec<T>(j, M - j, jb, A, lda, ipiv, dinfo, st, gemm);   // panel: rows j.., columns j..j+jb
+    if (j > 0) laswp_dev<T>(j, A, lda, j, j + jb, ipiv, 1, st);  // left of the panel
+    const int nr = N - j - jb;
+    if (nr > 0) {
+      T *A12 = Ad + (long)jb * lda;
+      laswp_dev<T>(nr, A + (long)(j + jb) * lda, lda, j, j + jb, ipiv, 1, st);
+      trsm_dev<T>(kLeft, kLower, kNoTrans, kUnit, jb, nr, T(1), Ad, lda, A12, lda, st, gemm);
+      if (M - j - jb > 0) update_gemm(gemm, M - j - jb, nr, jb, Ad + jb, A12, A12 + jb, lda, st);
+    }
+  }
   finish_info_kernel_launch(dinfo, st);
 }
 template void getrf_dev<double>(int, int, double *, long, int *, int *, cudaStream_t, SgemmFn);

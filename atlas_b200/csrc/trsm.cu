@@ -2,7 +2,9 @@
 //
 // TRSM follows the reference's recursive method (src/blas/ulevel3/ATL_trsm.c:
 // 13-228: halve the triangle, solve one half, GEMM-update the other, solve
-// it), down to 64x64 leaves that one CTA solves in shared memory / registers.
+// it), down to 64x64 leaves.  The leaves multiply by the inverted diagonal
+// blocks (all inverted by one launch per solve), so each leaf is a small
+// in-place matrix product over every right-hand side at once.
 // Every side/uplo/trans case is reduced to an "effective" forward or backward
 // solve T*X = B with T and B addressed through (row, column) strides, so one
 // leaf kernel serves all eight cases.
@@ -29,49 +31,42 @@ namespace {
 
 constexpr int LEAF = 64;
 
-// Solve T*X = B in place for one 64-column block of B.  T(i,k) =
-// Tp[i*tr + k*tc] (n x n, n <= 64), B(i,j) = Bp[i*br + j*bc].  lower: forward
-// substitution, else backward.  One thread per right-hand side, its column
-// held in registers; T broadcast from shared memory.
+// Invert the 64x64 (or smaller, last) diagonal blocks of the effective
+// triangle T (T(i,k) = Tp[i*tr + k*tc]) into W: block b is stored dense,
+// column-major 64x64 at W + b*64*64, zero outside its triangle.  One CTA per
+// block, one thread per column of the inverse (forward / backward
+// substitution against the identity, the column held in registers).
 template <typename T>
 __global__ void __launch_bounds__(LEAF)
-trsm_leaf_kernel(int n, int m, const T *__restrict__ Tp, long tr, long tc, T *__restrict__ Bp,
-                 long br, long bc, int lower, int unit) {
-  extern __shared__ __align__(16) unsigned char trsm_smem[];
-  T(*sT)[LEAF + 1] = reinterpret_cast<T(*)[LEAF + 1]>(trsm_smem);
-  T(*sB)[LEAF + 1] = sT + LEAF;
-  const int j0 = blockIdx.x * LEAF, tid = threadIdx.x;
-  for (int idx = tid; idx < n * n; idx += LEAF) {
+trinv_kernel(int n, const T *__restrict__ Tp, long tr, long tc, int lower, int unit, T *__restrict__ W) {
+  __shared__ T sT[LEAF][LEAF + 1];
+  const int b = blockIdx.x, r0 = b * LEAF, nb = min(LEAF, n - r0), j = threadIdx.x;
+  const T *Tb = Tp + r0 * tr + r0 * tc;
+  for (int idx = j; idx < nb * nb; idx += LEAF) {
     int i, k;
-    if (tr == 1) { i = idx % n; k = idx / n; } else { k = idx % n; i = idx / n; }
-    sT[i][k] = Tp[i * tr + k * tc];
-  }
-  const int mcols = min(LEAF, m - j0);
-  for (int idx = tid; idx < n * mcols; idx += LEAF) {
-    int i, j;
-    if (br == 1) { i = idx % n; j = idx / n; } else { j = idx % mcols; i = idx / mcols; }
-    sB[i][j] = Bp[i * br + (long)(j0 + j) * bc];
+    if (tr == 1) { i = idx % nb; k = idx / nb; } else { k = idx % nb; i = idx / nb; }
+    sT[i][k] = Tb[i * tr + k * tc];
   }
   __syncthreads();
-  if (tid < mcols) {
-    T x[LEAF];
+  T x[LEAF];
 #pragma unroll
-    for (int i = 0; i < LEAF; i++) x[i] = (i < n) ? sB[i][tid] : T(0);
+  for (int i = 0; i < LEAF; i++) x[i] = (i == j) ? T(1) : T(0);
+  if (j < nb) {
     if (lower) {
 #pragma unroll
       for (int k = 0; k < LEAF; k++) {
-        if (k < n) {
+        if (k < nb && k >= j) {
           T xk = unit ? x[k] : x[k] / sT[k][k];
           x[k] = xk;
 #pragma unroll
           for (int i = k + 1; i < LEAF; i++)
-            if (i < n) x[i] -= sT[i][k] * xk;
+            if (i < nb) x[i] -= sT[i][k] * xk;
         }
       }
     } else {
 #pragma unroll
       for (int k = LEAF - 1; k >= 0; k--) {
-        if (k < n) {
+        if (k < nb && k <= j) {
           T xk = unit ? x[k] : x[k] / sT[k][k];
           x[k] = xk;
 #pragma unroll
@@ -79,14 +74,49 @@ trsm_leaf_kernel(int n, int m, const T *__restrict__ Tp, long tr, long tc, T *__
         }
       }
     }
+  }
+  T *Wb = W + (long)b * LEAF * LEAF;
 #pragma unroll
-    for (int i = 0; i < LEAF; i++)
-      if (i < n) sB[i][tid] = x[i];
+  for (int i = 0; i < LEAF; i++) Wb[i + (long)j * LEAF] = x[i];
+}
+
+// B_blk (nb x m, effective strides) = W_b (nb x nb) * B_blk, in place: one
+// CTA per 64-column tile holds W_b and its tile in shared memory.
+template <typename T>
+__global__ void __launch_bounds__(256)
+tri_apply_kernel(int nb, int m, const T *__restrict__ Wb, T *__restrict__ Bp, long br, long bc) {
+  extern __shared__ __align__(16) unsigned char tri_smem[];
+  T(*sW)[LEAF + 1] = reinterpret_cast<T(*)[LEAF + 1]>(tri_smem);
+  T(*sB)[LEAF + 1] = sW + LEAF;
+  const int j0 = blockIdx.x * LEAF, tid = threadIdx.x;
+  const int mcols = min(LEAF, m - j0);
+  for (int idx = tid; idx < LEAF * LEAF; idx += 256) {
+    int i = idx % LEAF, k = idx / LEAF;
+    sW[i][k] = (i < nb && k < nb) ? Wb[i + (long)k * LEAF] : T(0);
+  }
+  for (int idx = tid; idx < LEAF * LEAF; idx += 256) {
+    int i, j;
+    if (br == 1) { i = idx % LEAF; j = idx / LEAF; } else { j = idx % LEAF; i = idx / LEAF; }
+    sB[i][j] = (i < nb && j < mcols) ? Bp[i * br + (long)(j0 + j) * bc] : T(0);
   }
   __syncthreads();
-  for (int idx = tid; idx < n * mcols; idx += LEAF) {
+  const int r = tid % LEAF, cg = tid / LEAF;  // 4 column groups
+  T acc[16];
+#pragma unroll
+  for (int q = 0; q < 16; q++) acc[q] = T(0);
+#pragma unroll 8
+  for (int k = 0; k < LEAF; k++) {
+    const T w = sW[r][k];
+#pragma unroll
+    for (int q = 0; q < 16; q++) acc[q] = fma(w, sB[k][cg + 4 * q], acc[q]);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 16; q++) sB[r][cg + 4 * q] = acc[q];
+  __syncthreads();
+  for (int idx = tid; idx < nb * mcols; idx += 256) {
     int i, j;
-    if (br == 1) { i = idx % n; j = idx / n; } else { j = idx % mcols; i = idx / mcols; }
+    if (br == 1) { i = idx % nb; j = idx / nb; } else { j = idx % mcols; i = idx / mcols; }
     Bp[i * br + (long)(j0 + j) * bc] = sB[i][j];
   }
 }
@@ -107,6 +137,7 @@ struct Eff {  // effective problem T*X = B
   const T *Tp; long tr, tc;
   T *Bp; long br, bc;
   int lower, unit;
+  const T *W;   // inverted 64x64 diagonal blocks (trinv_kernel)
 };
 
 template <typename T>
@@ -150,13 +181,12 @@ void eff_solve(const Eff<T> &e, int r0, int n, int m, SgemmFn fn, cudaStream_t s
     constexpr int smem = 2 * LEAF * (LEAF + 1) * (int)sizeof(T);
     static bool configured = false;
     if (!configured) {
-      ATLB_CUDA_CHECK(cudaFuncSetAttribute(trsm_leaf_kernel<T>,
+      ATLB_CUDA_CHECK(cudaFuncSetAttribute(tri_apply_kernel<T>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
       configured = true;
     }
-    trsm_leaf_kernel<T><<<cdiv(m, LEAF), LEAF, smem, st>>>(
-        n, m, e.Tp + r0 * e.tr + r0 * e.tc, e.tr, e.tc, e.Bp + r0 * e.br, e.br, e.bc, e.lower,
-        e.unit);
+    tri_apply_kernel<T><<<cdiv(m, LEAF), 256, smem, st>>>(
+        n, m, e.W + (long)(r0 / LEAF) * LEAF * LEAF, e.Bp + r0 * e.br, e.br, e.bc);
     ATLB_CUDA_CHECK(cudaGetLastError());
     return;
   }
@@ -172,21 +202,34 @@ void eff_solve(const Eff<T> &e, int r0, int n, int m, SgemmFn fn, cudaStream_t s
   }
 }
 
+// Row interchanges on ncols columns (one thread per column); the pivot
+// indices are staged 256 at a time in shared memory so the sequential swap
+// loop runs on broadcast shared-memory reads.
 template <typename T>
-__global__ void laswp_kernel(int ncols, T *A, long lda, int k1, int k2, const int *__restrict__ ipiv,
-                             int inc) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncols) return;
-  T *col = A + (long)c * lda;
-  if (inc > 0) {
-    for (int k = k1; k < k2; k++) {
-      int p = ipiv[k];
-      if (p != k) { T t = col[k]; col[k] = col[p]; col[p] = t; }
-    }
-  } else {
-    for (int k = k2 - 1; k >= k1; k--) {
-      int p = ipiv[k];
-      if (p != k) { T t = col[k]; col[k] = col[p]; col[p] = t; }
+__global__ void __launch_bounds__(256)
+laswp_kernel(int ncols, T *A, long lda, int k1, int k2, const int *__restrict__ ipiv, int inc) {
+  __shared__ int sp[256];
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  T *col = A + (long)min(c, ncols - 1) * lda;
+  const int n = k2 - k1, nch = (n + 255) / 256;
+  for (int ci = 0; ci < nch; ci++) {
+    const int ch = inc > 0 ? ci : nch - 1 - ci;
+    const int base = k1 + ch * 256, cnt = min(256, k2 - base);
+    __syncthreads();
+    if ((int)threadIdx.x < cnt) sp[threadIdx.x] = ipiv[base + threadIdx.x];
+    __syncthreads();
+    if (c < ncols) {
+      if (inc > 0) {
+        for (int i = 0; i < cnt; i++) {
+          const int p = sp[i], k = base + i;
+          if (p != k) { T t = col[k]; col[k] = col[p]; col[p] = t; }
+        }
+      } else {
+        for (int i = cnt - 1; i >= 0; i--) {
+          const int p = sp[i], k = base + i;
+          if (p != k) { T t = col[k]; col[k] = col[p]; col[p] = t; }
+        }
+      }
     }
   }
 }
@@ -256,6 +299,11 @@ void trsm_dev(int side, int uplo, int trans, int diag, int M, int N, T alpha, co
         n, m, alpha, e.Bp, e.br, e.bc);
     ATLB_CUDA_CHECK(cudaGetLastError());
   }
+  const int nblk = cdiv(n, LEAF);
+  T *W = (T *)scratch(kSlotTrsmW, sizeof(T) * (size_t)nblk * LEAF * LEAF);
+  trinv_kernel<T><<<nblk, LEAF, 0, st>>>(n, e.Tp, e.tr, e.tc, e.lower, e.unit, W);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+  e.W = W;
   eff_solve(e, 0, n, m, gemm, st);
 }
 
@@ -287,7 +335,7 @@ template <typename T>
 void laswp_dev(int ncols, T *A, long lda, int k1, int k2, const int *ipiv, int inc,
                cudaStream_t st) {
   if (ncols <= 0 || k2 <= k1) return;
-  laswp_kernel<T><<<cdiv(ncols, 128), 128, 0, st>>>(ncols, A, lda, k1, k2, ipiv, inc);
+  laswp_kernel<T><<<cdiv(ncols, 256), 256, 0, st>>>(ncols, A, lda, k1, k2, ipiv, inc);
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
 template void laswp_dev<double>(int, double *, long, int, int, const int *, int, cudaStream_t);

@@ -223,6 +223,25 @@ def main():
     assert int(info.item()) == 0
     value = world * 1000.0 / ms
 
+    # mixed-precision solves of the same system (factor FP32 / TF32 / BF16, FP64 refinement)
+    mixed = {}
+    xm = torch.empty(n, dtype=torch.float64, device=dev)
+    ipm = torch.empty(n, dtype=torch.int32, device=dev)
+    it = np.zeros(1, dtype=np.int32)
+    for name, prec in (("tf32", 1), ("bf16", 2), ("fp32", 0)):
+        for _ in range(2):
+            AB.atlb_dsgesv(n, 1, acol0, n, ipm, b0, n, xm, n, prec, it)
+        ts = []
+        for _ in range(max(2, args.steps // 2)):
+            e0m, e1m = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0m.record(stream)
+            r = AB.atlb_dsgesv(n, 1, acol0, n, ipm, b0, n, xm, n, prec, it)
+            e1m.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0m.elapsed_time(e1m))
+        mixed[name] = {"ms": sum(ts) / len(ts), "iter": int(it[0]), "info": int(r),
+                       "backward_error": backward_error(torch, acol0, xm, b0)}
+
     # dominant kernel: the FP64 DMMA GEMM, timed alone at 8192^3
     M = 8192
     ga = torch.rand(M, M, dtype=torch.float64, device=dev) * 2 - 1
@@ -300,7 +319,7 @@ def main():
             "config": {"workload": "dgesv N=8192 1 RHS, FP64 getrf+getrs (kappa=1e2 Q1 diag(s) Q2^T)",
                        "n": n, "nrhs": 1, "kappa": KAPPA, "parallelism": f"replicas x{world}",
                        "l2": "inputs 512 MiB > L2, no flush"},
-            "fp64_dgesv_gflops": gflops, "backward_error": berr, "bwd_err_bound": n * 2.0 ** -53,
+            "fp64_dgesv_gflops": gflops, "mixed_dgesv": mixed, "backward_error": berr, "bwd_err_bound": n * 2.0 ** -53,
             "dgemm_8192": {"ms": dgemm_ms, "tflops": dgemm_tf, "cublas_fp64_tflops": cublas_tf},
             "roofline": {"bound": "tensor", "achieved": dgemm_tf, "peak": cublas_tf, "unit": "TFLOP/s",
                          "frac": dgemm_tf / cublas_tf, "traffic": None,
