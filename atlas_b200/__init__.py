@@ -65,6 +65,8 @@ _SIGS = {
     "atlb_dpotrf_dev": (_I, [_I, _I, _P, _I, _P]),
     "atlb_dpotrs_dev": (_I, [_I, _I, _I, _P, _I, _P, _I]),
     "atlb_dgeqrf_dev": (_I, [_I, _I, _P, _I, _P]),
+    "atlb_dgemm_ozaki_dev": (_I, [_I, _I, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I, _I]),
+    "atlb_dgemm_ozaki": (_I, [_I, _I, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I, _I]),
     "atlb_dsgesv": (_I, [_I, _I, _P, _I, _P, _P, _I, _P, _I, _I, _P]),
     "atlb_dsposv": (_I, [_I, _I, _I, _P, _I, _P, _I, _P, _I, _I, _P]),
 }

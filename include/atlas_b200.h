@@ -145,6 +145,20 @@ int atlb_dsgesv(int N, int NRHS, double *A, int lda, int *ipiv, double *B, int l
 int atlb_dsposv(int Uplo, int N, int NRHS, double *A, int lda, double *B, int ldb, double *X,
                 int ldx, int prec, int *iter);
 
+/* Split-integer (Ozaki) DGEMM: C = alpha*op(A)*op(B) + beta*C with FP64
+ * operands cut into `slices` (2..12) signed 7-bit digit planes after exact
+ * per-row / per-column power-of-two scaling, the digit-plane products run on
+ * the INT8 tensor cores with exact INT32 accumulation and are recombined in
+ * FP64.  `slices` = 7-8 gives FP64-level accuracy.  No counterpart in the
+ * reference.  _dev: device pointers, asynchronous; the other form accepts
+ * host or device pointers and is synchronous.  Returns 0 or -(bad argument). */
+int atlb_dgemm_ozaki_dev(int TransA, int TransB, int M, int N, int K, double alpha,
+                         const double *A, int lda, const double *B, int ldb, double beta,
+                         double *C, int ldc, int slices);
+int atlb_dgemm_ozaki(int TransA, int TransB, int M, int N, int K, double alpha, const double *A,
+                     int lda, const double *B, int ldb, double beta, double *C, int ldc,
+                     int slices);
+
 #ifdef __cplusplus
 }
 #endif
