@@ -271,9 +271,11 @@ __global__ void finish_info_kernel(int *d) { if (*d == 0x7fffffff) *d = 0; }
 
 }  // namespace
 
+// The solve proper; W receives the inverted diagonal blocks (ceil(n/64)
+// blocks of 64x64 elements, n = order of the triangle).
 template <typename T>
-void trsm_dev(int side, int uplo, int trans, int diag, int M, int N, T alpha, const T *A, long lda,
-              T *B, long ldb, cudaStream_t st, SgemmFn gemm) {
+void trsm_impl(int side, int uplo, int trans, int diag, int M, int N, T alpha, const T *A, long lda,
+               T *B, long ldb, cudaStream_t st, SgemmFn gemm, T *W) {
   if (M <= 0 || N <= 0) return;
   const bool tr = trans != kNoTrans;
   Eff<T> e;
@@ -300,11 +302,19 @@ void trsm_dev(int side, int uplo, int trans, int diag, int M, int N, T alpha, co
     ATLB_CUDA_CHECK(cudaGetLastError());
   }
   const int nblk = cdiv(n, LEAF);
-  T *W = (T *)scratch(kSlotTrsmW, sizeof(T) * (size_t)nblk * LEAF * LEAF);
   trinv_kernel<T><<<nblk, LEAF, 0, st>>>(n, e.Tp, e.tr, e.tc, e.lower, e.unit, W);
   ATLB_CUDA_CHECK(cudaGetLastError());
   e.W = W;
   eff_solve(e, 0, n, m, gemm, st);
+}
+
+template <typename T>
+void trsm_dev(int side, int uplo, int trans, int diag, int M, int N, T alpha, const T *A, long lda,
+              T *B, long ldb, cudaStream_t st, SgemmFn gemm) {
+  if (M <= 0 || N <= 0) return;
+  const int n = side == kLeft ? M : N;
+  T *W = (T *)scratch(kSlotTrsmW, sizeof(T) * (size_t)cdiv(n, LEAF) * LEAF * LEAF);
+  trsm_impl<T>(side, uplo, trans, diag, M, N, alpha, A, lda, B, ldb, st, gemm, W);
 }
 
 template void trsm_dev<double>(int, int, int, int, int, int, double, const double *, long,
