@@ -26,7 +26,7 @@ CblasNonUnit, CblasUnit = 131, 132
 CblasLeft, CblasRight = 141, 142
 
 # factor precisions of the mixed-precision solvers
-PREC_FP32, PREC_TF32, PREC_BF16 = 0, 1, 2
+PREC_FP32, PREC_TF32, PREC_BF16, PREC_TF32X3 = 0, 1, 2, 3
 
 _lib = None
 
@@ -68,6 +68,7 @@ _SIGS = {
     "atlb_dgemm_ozaki_dev": (_I, [_I, _I, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I, _I]),
     "atlb_dgemm_ozaki": (_I, [_I, _I, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I, _I]),
     "atlb_dsgesv": (_I, [_I, _I, _P, _I, _P, _P, _I, _P, _I, _I, _P]),
+    "atlb_dsgesv_ex": (_I, [_I, _I, _P, _I, _P, _P, _I, _P, _I, _I, _I, _P]),
     "atlb_dsposv": (_I, [_I, _I, _I, _P, _I, _P, _I, _P, _I, _I, _P]),
 }
 

@@ -514,7 +514,7 @@ int atlb_sgemm_dev(int TA, int TB, int M, int N, int K, float alpha, const float
 
 int atlb_sgemm_tc_dev(int prec, int TA, int TB, int M, int N, int K, float alpha, const float *A,
                       int lda, const float *B, int ldb, float beta, float *C, int ldc) {
-  if (prec != 1 && prec != 2) return -1;
+  if (prec != 1 && prec != 2 && prec != 3) return -1;
   if (bad_trans(TA)) return -2;
   if (bad_trans(TB)) return -3;
   if (M < 0) return -4;
@@ -523,7 +523,7 @@ int atlb_sgemm_tc_dev(int prec, int TA, int TB, int M, int N, int K, float alpha
   if (lda < std::max(1, TA == kNoTrans ? M : K)) return -9;
   if (ldb < std::max(1, TB == kNoTrans ? K : N)) return -11;
   if (ldc < std::max(1, M)) return -14;
-  (prec == 1 ? sgemm_tf32_dev : sgemm_bf16_dev)(TA == kNoTrans ? kNoTrans : kTrans,
+  (prec == 1 ? sgemm_tf32_dev : prec == 2 ? sgemm_bf16_dev : sgemm_tf32x3_dev)(TA == kNoTrans ? kNoTrans : kTrans,
                                                 TB == kNoTrans ? kNoTrans : kTrans, M, N, K, alpha,
                                                 A, lda, B, ldb, beta, C, ldc, stream(), 0);
   return 0;

@@ -130,6 +130,16 @@ void potrs_dev(int uplo, int N, int NRHS, const T *A, long lda, T *B, long ldb, 
                SgemmFn gemm) {
   // ATL_potrs column-major (src/lapack/ATL_potrs.c:41-60)
   if (N <= 0 || NRHS <= 0) return;
+  if (NRHS <= 8) {  // few right-hand sides: one-launch blocked solves
+    if (uplo == kUpper) {
+      trsv_dev<T>(kUpper, kTrans, kNonUnit, N, NRHS, A, lda, B, ldb, st);
+      trsv_dev<T>(kUpper, kNoTrans, kNonUnit, N, NRHS, A, lda, B, ldb, st);
+    } else {
+      trsv_dev<T>(kLower, kNoTrans, kNonUnit, N, NRHS, A, lda, B, ldb, st);
+      trsv_dev<T>(kLower, kTrans, kNonUnit, N, NRHS, A, lda, B, ldb, st);
+    }
+    return;
+  }
   if (uplo == kUpper) {
     trsm_dev<T>(kLeft, kUpper, kTrans, kNonUnit, N, NRHS, T(1), A, lda, B, ldb, st, gemm);
     trsm_dev<T>(kLeft, kUpper, kNoTrans, kNonUnit, N, NRHS, T(1), A, lda, B, ldb, st, gemm);

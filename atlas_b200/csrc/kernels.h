@@ -28,6 +28,11 @@ void sgemm_tf32_dev(int ta, int tb, int M, int N, int K, float alpha, const floa
 void sgemm_bf16_dev(int ta, int tb, int M, int N, int K, float alpha, const float *A, long lda,
                     const float *B, long ldb, float beta, float *C, long ldc, cudaStream_t st,
                     int tri);
+// FP32-accurate GEMM on the TF32 tensor cores (operands split into TF32 high
+// and low parts, three products summed in one K-concatenated GEMM).
+void sgemm_tf32x3_dev(int ta, int tb, int M, int N, int K, float alpha, const float *A, long lda,
+                      const float *B, long ldb, float beta, float *C, long ldc, cudaStream_t st,
+                      int tri);
 
 template <typename T>
 void gemm_dev(int ta, int tb, int M, int N, int K, T alpha, const T *A, long lda, const T *B,
@@ -38,6 +43,15 @@ void gemm_dev(int ta, int tb, int M, int N, int K, T alpha, const T *A, long lda
 template <typename T>
 void trsm_dev(int side, int uplo, int trans, int diag, int M, int N, T alpha, const T *A, long lda,
               T *B, long ldb, cudaStream_t st, SgemmFn gemm = nullptr);
+// Inverses of the 64x64 diagonal blocks of the triangle T(i,k) = Tp[i*tr + k*tc]
+// (n x n), block b stored dense 64x64 column-major at W + b*4096.
+template <typename T>
+void trinv_dev(int n, const T *Tp, long tr, long tc, int lower, int unit, T *W, cudaStream_t st);
+// op(A) X = B (Left side) for nrhs <= 8 in one launch.
+template <typename T>
+void trsv_dev(int uplo, int trans, int diag, int n, int nrhs, const T *A, long lda, T *B, long ldb,
+              cudaStream_t st);
+
 // B = alpha*op(A)*B (Left) or alpha*B*op(A) (Right), A triangular.
 void dtrmm_dev(int side, int uplo, int trans, int diag, int M, int N, double alpha,
                const double *A, long lda, double *B, long ldb, cudaStream_t st);
@@ -55,6 +69,10 @@ void laswp_dev(int ncols, T *A, long lda, int k1, int k2, const int *ipiv, int i
 template <typename T>
 void getrf_dev(int M, int N, T *A, long lda, int *ipiv, int *dinfo, cudaStream_t st,
                SgemmFn gemm = nullptr);
+// LU without pivoting (for matrices made pivot-safe by a random butterfly
+// transformation); dinfo as above.
+template <typename T>
+void getrf_nopiv_dev(int N, T *A, long lda, int *dinfo, cudaStream_t st, SgemmFn gemm = nullptr);
 template <typename T>
 void getrs_dev(int trans, int N, int NRHS, const T *A, long lda, const int *ipiv, T *B, long ldb,
                cudaStream_t st, SgemmFn gemm = nullptr);

@@ -117,9 +117,11 @@ getf2_cluster_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restr
 
   if (MN > 0) publish(0);
 
-#pragma unroll
-  for (int j = 0; j < NB; j++) {
-    if (j >= MN) break;
+  // The column loop is deliberately not unrolled (an unrolled NB x NB body
+  // overflows the instruction cache); register rows are addressed through
+  // compare-and-select over the NB columns instead.
+#pragma unroll 1
+  for (int j = 0; j < MN; j++) {
     const int b = j & 1;
     // gather every CTA's candidate (one distributed-shared-memory round trip)
     for (int idx = tid; idx < C * (NB + 2); idx += PT) {
@@ -144,6 +146,7 @@ getf2_cluster_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restr
     }
     const bool use_rcp = fabs(piv) >= safmin<T>();
     const T rcp = T(1) / piv;
+    const T *u = grow[w];
 #pragma unroll
     for (int q = 0; q < RPT; q++) {
       if (!act[q]) continue;
@@ -154,10 +157,16 @@ getf2_cluster_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restr
       }
       if (pos[q] == j) pos[q] = p;  // the row displaced by the swap
       if (piv != T(0)) {
-        T l = use_rcp ? a[q][j] * rcp : a[q][j] / piv;
-        a[q][j] = l;
+        T aj = T(0);
 #pragma unroll
-        for (int k = j + 1; k < NB; k++) a[q][k] = fma(-l, grow[w][k], a[q][k]);
+        for (int k = 0; k < NB; k++)
+          if (k == j) aj = a[q][k];
+        const T l = use_rcp ? aj * rcp : aj / piv;
+#pragma unroll
+        for (int k = 0; k < NB; k++) {
+          if (k == j) a[q][k] = l;
+          else if (k > j) a[q][k] = fma(-l, u[k], a[q][k]);
+        }
       }
     }
     if (j + 1 < MN) publish(j + 1);
@@ -383,6 +392,18 @@ void getrs_dev(int trans, int N, int NRHS, const T *A, long lda, const int *ipiv
                cudaStream_t st, SgemmFn gemm) {
   // ATL_getrs column-major (src/lapack/ATL_getrs.c:34-50)
   if (N <= 0 || NRHS <= 0) return;
+  if (NRHS <= 8) {  // few right-hand sides: one-launch blocked solves
+    if (trans == kNoTrans) {
+      laswp_dev<T>(NRHS, B, ldb, 0, N, ipiv, 1, st);
+      trsv_dev<T>(kLower, kNoTrans, kUnit, N, NRHS, A, lda, B, ldb, st);
+      trsv_dev<T>(kUpper, kNoTrans, kNonUnit, N, NRHS, A, lda, B, ldb, st);
+    } else {
+      trsv_dev<T>(kUpper, kTrans, kNonUnit, N, NRHS, A, lda, B, ldb, st);
+      trsv_dev<T>(kLower, kTrans, kUnit, N, NRHS, A, lda, B, ldb, st);
+      laswp_dev<T>(NRHS, B, ldb, 0, N, ipiv, -1, st);
+    }
+    return;
+  }
   if (trans == kNoTrans) {
     laswp_dev<T>(NRHS, B, ldb, 0, N, ipiv, 1, st);
     trsm_dev<T>(kLeft, kLower, kNoTrans, kUnit, N, NRHS, T(1), A, lda, B, ldb, st, gemm);
@@ -397,5 +418,80 @@ template void getrs_dev<double>(int, int, int, const double *, long, const int *
                                 cudaStream_t, SgemmFn);
 template void getrs_dev<float>(int, int, int, const float *, long, const int *, float *, long,
                                cudaStream_t, SgemmFn);
+
+}  // namespace atlb
+
+// ---------------------------------------------------------------------------
+// LU without pivoting, used by the mixed-precision solver after a random
+// butterfly transformation has made pivoting unnecessary (rbt.cu).  Blocked
+// right-looking: each NBD x NBD diagonal block is factored by one CTA in
+// shared memory, the block column below it and the block row right of it by
+// TRSM, and the trailing matrix by one GEMM.  A zero pivot lowers *dinfo.
+namespace atlb {
+namespace {
+
+constexpr int NBD = 128;
+
+template <typename T>
+__global__ void __launch_bounds__(512)
+lu_nopiv_diag_kernel(int n, T *A, long lda, int *dinfo, int ioff) {
+  extern __shared__ __align__(16) unsigned char nopiv_smem[];
+  T(*s)[NBD + 1] = reinterpret_cast<T(*)[NBD + 1]>(nopiv_smem);
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < n * n; idx += blockDim.x) {
+    int i = idx % n, k = idx / n;
+    s[i][k] = A[i + (long)k * lda];
+  }
+  __syncthreads();
+  for (int j = 0; j < n; j++) {
+    const T p = s[j][j];
+    if (p == T(0)) {
+      if (tid == 0) atomicMin(dinfo, ioff + j + 1);
+      break;  // uniform: every thread read the same pivot
+    }
+    const T r = T(1) / p;
+    for (int i = j + 1 + tid; i < n; i += blockDim.x) s[i][j] *= r;
+    __syncthreads();
+    const int m = n - j - 1;
+    for (int idx = tid; idx < m * m; idx += blockDim.x) {
+      const int i = j + 1 + idx % m, k = j + 1 + idx / m;
+      s[i][k] = fma(-s[i][j], s[j][k], s[i][k]);
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  for (int idx = tid; idx < n * n; idx += blockDim.x) {
+    int i = idx % n, k = idx / n;
+    A[i + (long)k * lda] = s[i][k];
+  }
+}
+
+}  // namespace
+
+template <typename T>
+void getrf_nopiv_dev(int N, T *A, long lda, int *dinfo, cudaStream_t st, SgemmFn gemm) {
+  set_info_kernel_launch(dinfo, st);
+  constexpr int smem = NBD * (NBD + 1) * (int)sizeof(T);
+  static bool configured = false;
+  if (!configured) {
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(lu_nopiv_diag_kernel<T>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    configured = true;
+  }
+  for (int j = 0; j < N; j += NBD) {
+    const int jb = std::min(NBD, N - j), nr = N - j - jb;
+    T *Ad = A + j + (long)j * lda;
+    lu_nopiv_diag_kernel<T><<<1, 512, smem, st>>>(jb, Ad, lda, dinfo, j);
+    ATLB_CUDA_CHECK(cudaGetLastError());
+    if (nr <= 0) break;
+    T *A21 = Ad + jb, *A12 = Ad + (long)jb * lda;
+    trsm_dev<T>(kRight, kUpper, kNoTrans, kNonUnit, nr, jb, T(1), Ad, lda, A21, lda, st, gemm);
+    trsm_dev<T>(kLeft, kLower, kNoTrans, kUnit, jb, nr, T(1), Ad, lda, A12, lda, st, gemm);
+    update_gemm(gemm, nr, nr, jb, A21, A12, A12 + jb, lda, st);
+  }
+  finish_info_kernel_launch(dinfo, st);
+}
+template void getrf_nopiv_dev<double>(int, double *, long, int *, cudaStream_t, SgemmFn);
+template void getrf_nopiv_dev<float>(int, float *, long, int *, cudaStream_t, SgemmFn);
 
 }  // namespace atlb

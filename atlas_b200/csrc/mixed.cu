@@ -170,6 +170,7 @@ void symmetrize_dev(int uplo, int N, const double *A, long lda, double *F, long 
 SgemmFn factor_gemm(int prec) {
   if (prec == kPrecTF32) return sgemm_tf32_dev;
   if (prec == kPrecBF16) return sgemm_bf16_dev;
+  if (prec == kPrecTF32x3) return sgemm_tf32x3_dev;
   return sgemm_dev;
 }
 
@@ -216,24 +217,22 @@ void add_s2d_dev(int M, int N, const float *S, long lds, double *X, long ldx, cu
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
 
-// Refinement driver shared by dsgesv and dsposv.  `factor` factors the FP32
-// copy (returns info), `solve` solves in FP32 in place; A, B, X device.
-template <class Factor, class Solve, class Fallback>
+// Refinement driver shared by the solvers.  `factor()` factors the low
+// precision copy and returns its info; `correct(R, ldr, X, ldx)` adds an
+// approximate solution of A D = R to X (R, X FP64 device); `fallback()` runs
+// the FP64 solver.  X is overwritten with the solution.
+template <class Factor, class Correct, class Fallback>
 int refine(int N, int nrhs, const double *A, long lda, const double *B, long ldb, double *X,
-           long ldx, int *iter, Factor factor, Solve solve, Fallback fallback, cudaStream_t st,
+           long ldx, int *iter, Factor factor, Correct correct, Fallback fallback, cudaStream_t st,
            MixedStats *stats) {
   const int nch = cdiv(N, GV_COLS);
-  const long lds = N;
-  float *S = (float *)scratch(kSlotMixedA, sizeof(float) * (size_t)N * N);
-  float *Rs = (float *)scratch(kSlotMixedX, sizeof(float) * (size_t)N * nrhs);
   double *R = (double *)scratch(kSlotMixedR, sizeof(double) * (size_t)N * nrhs);
   double *part = (double *)scratch(kSlotMixedD, sizeof(double) * (size_t)nch * N * 8 + 64);
   unsigned long long *red = (unsigned long long *)scratch(kSlotWork2, sizeof(unsigned long long) * (3 * nrhs + 8));
   unsigned long long *hred = (unsigned long long *)pinned(kSlotWork2, sizeof(unsigned long long) * (3 * nrhs + 8));
 
   dnorm_inf_dev(N, A, lda, part, red + 3 * nrhs, st);
-  d2s_dev(N, N, A, lda, S, lds, st);
-  int finfo = factor(S, lds);
+  int finfo = factor();
   double anrm = 0.0;
   {
     ATLB_CUDA_CHECK(cudaMemcpyAsync(hred, red + 3 * nrhs, 8, cudaMemcpyDeviceToHost, st));
@@ -242,10 +241,9 @@ int refine(int N, int nrhs, const double *A, long lda, const double *B, long ldb
   }
   const double tol = N * std::ldexp(1.0, -53);
   if (finfo == 0) {
-    // x0 = solve(b) in FP32
-    d2s_dev(N, nrhs, B, ldb, Rs, N, st);
-    solve(S, lds, Rs, N);
-    s2d_dev(N, nrhs, Rs, N, X, ldx, st);
+    for (int r = 0; r < nrhs; r++)
+      ATLB_CUDA_CHECK(cudaMemsetAsync(X + (long)r * ldx, 0, sizeof(double) * N, st));
+    correct(B, ldb, X, ldx);  // x0
     for (int it = 0; it <= ITERMAX; it++) {
       dresid_dev(N, nrhs, A, lda, X, ldx, B, ldb, R, N, part, red, st);
       ATLB_CUDA_CHECK(cudaMemcpyAsync(hred, red, sizeof(unsigned long long) * 3 * nrhs,
@@ -266,14 +264,12 @@ int refine(int N, int nrhs, const double *A, long lda, const double *B, long ldb
         *iter = it;
         return 0;
       }
-      if (it == ITERMAX) break;
-      d2s_dev(N, nrhs, R, N, Rs, N, st);
-      solve(S, lds, Rs, N);
-      add_s2d_dev(N, nrhs, Rs, N, X, ldx, st);
+      if (it == ITERMAX || !(worst < 1e300)) break;
+      correct(R, N, X, ldx);
     }
     *iter = -(ITERMAX + 1);
   } else {
-    *iter = -3;  // FP32 factorization broke down (LAPACK dsgesv: ITER = -3)
+    *iter = -3;  // the low-precision factorization broke down (LAPACK dsgesv: ITER = -3)
   }
   return fallback();
 }
@@ -293,14 +289,15 @@ int read_info(const int *dinfo, cudaStream_t st) {
 
 extern "C" {
 
-int atlb_dsgesv(int N, int NRHS, double *A, int lda, int *ipiv, double *B, int ldb, double *X,
-                int ldx, int prec, int *iter) {
+int atlb_dsgesv_ex(int N, int NRHS, double *A, int lda, int *ipiv, double *B, int ldb, double *X,
+                   int ldx, int prec, int pivoting, int *iter) {
   if (N < 0) return -1;
   if (NRHS < 0) return -2;
   if (lda < std::max(1, N)) return -4;
   if (ldb < std::max(1, N)) return -7;
   if (ldx < std::max(1, N)) return -9;
-  if (prec < kPrecFP32 || prec > kPrecBF16) return -10;
+  if (prec < kPrecFP32 || prec > kPrecTF32x3) return -10;
+  if (pivoting != 0 && pivoting != 1) return -11;
   int it_local = 0;
   if (!iter) iter = &it_local;
   *iter = 0;
@@ -312,12 +309,38 @@ int atlb_dsgesv(int N, int NRHS, double *A, int lda, int *ipiv, double *B, int l
   int *dip = stage_vec_in<int>(kSlotIpiv, ipiv, N, false, st);
   int *dinfo = (int *)scratch(kSlotInfo, 64);
   SgemmFn g = factor_gemm(prec);
-  auto factor = [&](float *S, long lds) {
-    getrf_dev<float>(N, N, S, lds, dip, dinfo, st, g);
+  const int n4 = rbt_order(N);
+  const long lds = pivoting ? n4 : N;
+  float *S = (float *)scratch(kSlotMixedA, sizeof(float) * (size_t)lds * lds);
+  float *Rs = (float *)scratch(kSlotMixedX, sizeof(float) * (size_t)lds * NRHS);
+  double *rd = pivoting ? (double *)scratch(kSlotTc1, sizeof(double) * 4 * n4) : nullptr;
+  auto factor = [&]() {
+    if (pivoting) {
+      rbt_init_dev(n4, rd, st);
+      rbt_matrix_dev(N, dA.d, dA.ld, rd, S, st);
+      getrf_nopiv_dev<float>(n4, S, lds, dinfo, st, g);
+    } else {
+      d2s_dev(N, N, dA.d, dA.ld, S, lds, st);
+      getrf_dev<float>(N, N, S, lds, dip, dinfo, st, g);
+    }
     return read_info(dinfo, st);
   };
-  auto solve = [&](const float *S, long lds, float *R, long ldr) {
-    getrs_dev<float>(kNoTrans, N, NRHS, S, lds, dip, R, ldr, st, g);
+  auto correct = [&](const double *R, long ldr, double *Xc, long ldxc) {
+    if (pivoting) {
+      rbt_left_vec_dev(N, NRHS, R, ldr, rd, Rs, st);
+      if (NRHS <= 8) {
+        trsv_dev<float>(kLower, kNoTrans, kUnit, n4, NRHS, S, lds, Rs, n4, st);
+        trsv_dev<float>(kUpper, kNoTrans, kNonUnit, n4, NRHS, S, lds, Rs, n4, st);
+      } else {
+        trsm_dev<float>(kLeft, kLower, kNoTrans, kUnit, n4, NRHS, 1.f, S, lds, Rs, n4, st, g);
+        trsm_dev<float>(kLeft, kUpper, kNoTrans, kNonUnit, n4, NRHS, 1.f, S, lds, Rs, n4, st, g);
+      }
+      rbt_right_add_dev(N, NRHS, Rs, rd, Xc, ldxc, st);
+    } else {
+      d2s_dev(N, NRHS, R, ldr, Rs, N, st);
+      getrs_dev<float>(kNoTrans, N, NRHS, S, lds, dip, Rs, N, st, g);
+      add_s2d_dev(N, NRHS, Rs, N, Xc, ldxc, st);
+    }
   };
   bool fell_back = false;
   auto fallback = [&]() {
@@ -333,8 +356,8 @@ int atlb_dsgesv(int N, int NRHS, double *A, int lda, int *ipiv, double *B, int l
     }
     return info;
   };
-  int info = refine(N, NRHS, dA.d, dA.ld, dB.d, dB.ld, dX.d, dX.ld, iter, factor, solve, fallback, st,
-                    nullptr);
+  int info = refine(N, NRHS, dA.d, dA.ld, dB.d, dB.ld, dX.d, dX.ld, iter, factor, correct, fallback,
+                    st, nullptr);
   stage_out(X, ldx, dX, N, NRHS, st);
   if (fell_back) {
     stage_out(A, lda, dA, N, N, st);
@@ -342,6 +365,11 @@ int atlb_dsgesv(int N, int NRHS, double *A, int lda, int *ipiv, double *B, int l
   }
   ATLB_CUDA_CHECK(cudaStreamSynchronize(st));
   return info;
+}
+
+int atlb_dsgesv(int N, int NRHS, double *A, int lda, int *ipiv, double *B, int ldb, double *X,
+                int ldx, int prec, int *iter) {
+  return atlb_dsgesv_ex(N, NRHS, A, lda, ipiv, B, ldb, X, ldx, prec, 0, iter);
 }
 
 int atlb_dsposv(int Uplo, int N, int NRHS, double *A, int lda, double *B, int ldb, double *X,
@@ -352,7 +380,7 @@ int atlb_dsposv(int Uplo, int N, int NRHS, double *A, int lda, double *B, int ld
   if (lda < std::max(1, N)) return -5;
   if (ldb < std::max(1, N)) return -7;
   if (ldx < std::max(1, N)) return -9;
-  if (prec < kPrecFP32 || prec > kPrecBF16) return -10;
+  if (prec < kPrecFP32 || prec > kPrecTF32x3) return -10;
   int it_local = 0;
   if (!iter) iter = &it_local;
   *iter = 0;
@@ -367,12 +395,17 @@ int atlb_dsposv(int Uplo, int N, int NRHS, double *A, int lda, double *B, int ld
   // referenced one by symmetry (a full symmetric copy, FP64).
   double *Af = (double *)scratch(kSlotWork, sizeof(double) * (size_t)N * N);
   symmetrize_dev(Uplo, N, dA.d, dA.ld, Af, N, st);
-  auto factor = [&](float *S, long lds) {
-    potrf_dev<float>(Uplo, N, S, lds, dinfo, st, g);
+  float *S = (float *)scratch(kSlotMixedA, sizeof(float) * (size_t)N * N);
+  float *Rs = (float *)scratch(kSlotMixedX, sizeof(float) * (size_t)N * NRHS);
+  auto factor = [&]() {
+    d2s_dev(N, N, Af, N, S, N, st);
+    potrf_dev<float>(Uplo, N, S, N, dinfo, st, g);
     return read_info(dinfo, st);
   };
-  auto solve = [&](const float *S, long lds, float *R, long ldr) {
-    potrs_dev<float>(Uplo, N, NRHS, S, lds, R, ldr, st, g);
+  auto correct = [&](const double *R, long ldr, double *Xc, long ldxc) {
+    d2s_dev(N, NRHS, R, ldr, Rs, N, st);
+    potrs_dev<float>(Uplo, N, NRHS, S, N, Rs, N, st, g);
+    add_s2d_dev(N, NRHS, Rs, N, Xc, ldxc, st);
   };
   bool fell_back = false;
   auto fallback = [&]() {
@@ -387,7 +420,7 @@ int atlb_dsposv(int Uplo, int N, int NRHS, double *A, int lda, double *B, int ld
     }
     return info;
   };
-  int info = refine(N, NRHS, Af, N, dB.d, dB.ld, dX.d, dX.ld, iter, factor, solve, fallback, st,
+  int info = refine(N, NRHS, Af, N, dB.d, dB.ld, dX.d, dX.ld, iter, factor, correct, fallback, st,
                     nullptr);
   stage_out(X, ldx, dX, N, NRHS, st);
   if (fell_back) stage_out(A, lda, dA, N, N, st);

@@ -6,7 +6,7 @@
 
 namespace atlb {
 
-enum { kPrecFP32 = 0, kPrecTF32 = 1, kPrecBF16 = 2 };
+enum { kPrecFP32 = 0, kPrecTF32 = 1, kPrecBF16 = 2, kPrecTF32x3 = 3 };
 
 struct MixedStats {
   double bwd_err;  // worst normwise backward error at exit
@@ -20,6 +20,13 @@ inline double bits_to_double(unsigned long long u) {
 }
 
 SgemmFn factor_gemm(int prec);
+int rbt_order(int n);
+void rbt_init_dev(int n4, double *d, cudaStream_t st);
+void rbt_matrix_dev(int n, const double *A, long lda, const double *d, float *S, cudaStream_t st);
+void rbt_left_vec_dev(int n, int nrhs, const double *R, long ldr, const double *d, float *C,
+                      cudaStream_t st);
+void rbt_right_add_dev(int n, int nrhs, const float *Y, const double *d, double *X, long ldx,
+                       cudaStream_t st);
 void symmetrize_dev(int uplo, int N, const double *A, long lda, double *F, long ldf, cudaStream_t st);
 void dnorm_inf_dev(int N, const double *A, long lda, double *part, unsigned long long *out,
                    cudaStream_t st);

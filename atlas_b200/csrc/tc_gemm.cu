@@ -365,6 +365,63 @@ __global__ void to_kmajor_kernel(int rows, int K, const float *__restrict__ X, l
   }
 }
 
+// 3xTF32: op(X) -> rows of [p0 | p1 | p2] K-blocks (each ldk wide) where
+// block q holds the TF32-rounded high part (pat bit q = 0) or the
+// TF32-rounded remainder x - hi(x) (bit q = 1).  A uses [hi lo hi], B uses
+// [hi hi lo], so one GEMM over K' = 3*ldk sums hi*hi + lo*hi + hi*lo, the
+// FP32-accurate product (the lo*lo term is below FP32 rounding).
+__global__ void to_kmajor_split_kernel(int rows, int K, const float *__restrict__ X, long ld,
+                                       int rcontig, float *__restrict__ out, long ldk, int pat) {
+  __shared__ float t[32][33];
+  const int r0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int j = ty; j < 32; j += 8) {
+    int r, k;
+    if (rcontig) { r = r0 + tx; k = k0 + j; } else { k = k0 + tx; r = r0 + j; }
+    float v = (r < rows && k < K) ? X[rcontig ? (r + (long)k * ld) : (k + (long)r * ld)] : 0.f;
+    if (rcontig) t[j][tx] = v; else t[tx][j] = v;
+  }
+  __syncthreads();
+  for (int j = ty; j < 32; j += 8) {
+    const int r = r0 + j, k = k0 + tx;
+    if (r < rows && k < K) {
+      const float v = t[tx][j];
+      uint32_t hi, lo;
+      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(v));
+      const float rem = v - __uint_as_float(hi);
+      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(rem));
+      float *o = out + (long)r * 3 * ldk + k;
+#pragma unroll
+      for (int q = 0; q < 3; q++) o[q * ldk] = __uint_as_float(((pat >> q) & 1) ? lo : hi);
+    }
+  }
+}
+
+void sgemm_tf32x3(int ta, int tb, int M, int N, int K, float alpha, const float *A, long lda,
+                  const float *B, long ldb, float beta, float *C, long ldc, cudaStream_t st, int tri) {
+  if (M <= 0 || N <= 0) return;
+  EpiParams ep = {};
+  ep.Cf = C; ep.ldc = ldc; ep.alpha = alpha; ep.beta = beta; ep.tri = tri;
+  if (K <= 0 || alpha == 0.f) {
+    sgemm_dev(ta, tb, M, N, 0, alpha, A, lda, B, ldb, beta, C, ldc, st, tri);
+    return;
+  }
+  // each K-block padded to a whole 32-element TMA slab so the three blocks line up
+  const long ldk = (long)cdiv(K, 32) * 32;
+  const size_t abytes = (size_t)M * 3 * ldk * 4, bbytes = (size_t)N * 3 * ldk * 4;
+  unsigned char *buf = (unsigned char *)scratch(kSlotTc0, abytes + bbytes + 256);
+  float *Ak = (float *)buf;
+  float *Bk = (float *)(buf + ((abytes + 255) / 256) * 256);
+  if (ldk != K) {  // zero the K padding once per call
+    ATLB_CUDA_CHECK(cudaMemsetAsync(buf, 0, abytes + bbytes + 256, st));
+  }
+  dim3 blk(32, 8);
+  to_kmajor_split_kernel<<<dim3(cdiv(K, 32), cdiv(M, 32)), blk, 0, st>>>(M, K, A, lda, ta == kNoTrans, Ak, ldk, 0b010);
+  to_kmajor_split_kernel<<<dim3(cdiv(K, 32), cdiv(N, 32)), blk, 0, st>>>(N, K, B, ldb, tb != kNoTrans, Bk, ldk, 0b100);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+  tc_gemm(kKindTF32, kEpiF32, Ak, 3 * ldk, Bk, 3 * ldk, M, N, (int)(3 * ldk), ep, st);
+}
+
 template <int KIND>
 void sgemm_tc(int ta, int tb, int M, int N, int K, float alpha, const float *A, long lda,
               const float *B, long ldb, float beta, float *C, long ldc, cudaStream_t st, int tri) {
@@ -396,6 +453,11 @@ void sgemm_tf32_dev(int ta, int tb, int M, int N, int K, float alpha, const floa
                     const float *B, long ldb, float beta, float *C, long ldc, cudaStream_t st,
                     int tri) {
   tc::sgemm_tc<tc::kKindTF32>(ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, st, tri);
+}
+void sgemm_tf32x3_dev(int ta, int tb, int M, int N, int K, float alpha, const float *A, long lda,
+                      const float *B, long ldb, float beta, float *C, long ldc, cudaStream_t st,
+                      int tri) {
+  tc::sgemm_tf32x3(ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, st, tri);
 }
 void sgemm_bf16_dev(int ta, int tb, int M, int N, int K, float alpha, const float *A, long lda,
                     const float *B, long ldb, float beta, float *C, long ldc, cudaStream_t st,

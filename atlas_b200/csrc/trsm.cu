@@ -39,45 +39,42 @@ constexpr int LEAF = 64;
 template <typename T>
 __global__ void __launch_bounds__(LEAF)
 trinv_kernel(int n, const T *__restrict__ Tp, long tr, long tc, int lower, int unit, T *__restrict__ W) {
-  __shared__ T sT[LEAF][LEAF + 1];
+  extern __shared__ __align__(16) unsigned char trinv_smem[];
+  T(*sT)[LEAF + 1] = reinterpret_cast<T(*)[LEAF + 1]>(trinv_smem);
+  T(*sW)[LEAF + 1] = sT + LEAF;  // column j of the inverse is owned by thread j
   const int b = blockIdx.x, r0 = b * LEAF, nb = min(LEAF, n - r0), j = threadIdx.x;
   const T *Tb = Tp + r0 * tr + r0 * tc;
-  for (int idx = j; idx < nb * nb; idx += LEAF) {
+  for (int idx = j; idx < LEAF * LEAF; idx += LEAF) {
     int i, k;
-    if (tr == 1) { i = idx % nb; k = idx / nb; } else { k = idx % nb; i = idx / nb; }
-    sT[i][k] = Tb[i * tr + k * tc];
+    if (tr == 1) { i = idx % LEAF; k = idx / LEAF; } else { k = idx % LEAF; i = idx / LEAF; }
+    sT[i][k] = (i < nb && k < nb) ? Tb[i * tr + k * tc] : T(0);
+    sW[i][k] = (i == k) ? T(1) : T(0);
   }
   __syncthreads();
-  T x[LEAF];
-#pragma unroll
-  for (int i = 0; i < LEAF; i++) x[i] = (i == j) ? T(1) : T(0);
   if (j < nb) {
     if (lower) {
-#pragma unroll
-      for (int k = 0; k < LEAF; k++) {
-        if (k < nb && k >= j) {
-          T xk = unit ? x[k] : x[k] / sT[k][k];
-          x[k] = xk;
-#pragma unroll
-          for (int i = k + 1; i < LEAF; i++)
-            if (i < nb) x[i] -= sT[i][k] * xk;
-        }
+#pragma unroll 1
+      for (int k = j; k < nb; k++) {
+        T xk = sW[k][j];
+        if (!unit) xk = xk / sT[k][k];
+        sW[k][j] = xk;
+#pragma unroll 4
+        for (int i = k + 1; i < nb; i++) sW[i][j] -= sT[i][k] * xk;
       }
     } else {
-#pragma unroll
-      for (int k = LEAF - 1; k >= 0; k--) {
-        if (k < nb && k <= j) {
-          T xk = unit ? x[k] : x[k] / sT[k][k];
-          x[k] = xk;
-#pragma unroll
-          for (int i = 0; i < k; i++) x[i] -= sT[i][k] * xk;
-        }
+#pragma unroll 1
+      for (int k = j; k >= 0; k--) {
+        T xk = sW[k][j];
+        if (!unit) xk = xk / sT[k][k];
+        sW[k][j] = xk;
+#pragma unroll 4
+        for (int i = 0; i < k; i++) sW[i][j] -= sT[i][k] * xk;
       }
     }
   }
+  __syncthreads();
   T *Wb = W + (long)b * LEAF * LEAF;
-#pragma unroll
-  for (int i = 0; i < LEAF; i++) Wb[i + (long)j * LEAF] = x[i];
+  for (int idx = j; idx < LEAF * LEAF; idx += LEAF) Wb[idx] = sW[idx % LEAF][idx / LEAF];
 }
 
 // B_blk (nb x m, effective strides) = W_b (nb x nb) * B_blk, in place: one
@@ -202,34 +199,96 @@ void eff_solve(const Eff<T> &e, int r0, int n, int m, SgemmFn fn, cudaStream_t s
   }
 }
 
-// Row interchanges on ncols columns (one thread per column); the pivot
-// indices are staged 256 at a time in shared memory so the sequential swap
-// loop runs on broadcast shared-memory reads.
+// Row interchanges.  The swaps k1..k2-1 of one call (at most LSW_MAXP of
+// them; longer ranges are split) are first reduced to their net effect by one
+// CTA: a permutation of the rows [k1, hi) simulated in shared memory, then
+// compacted into the list of (destination, source) row moves.  The apply
+// kernel then moves only those rows, in parallel over columns (16 per CTA):
+// all sources are read into shared memory before any destination is written,
+// so the in-place permutation needs no ordering.
+constexpr int LSW_MAXP = 256;               // pivots per plan
+constexpr int LSW_SPAN = 24576;             // rows a plan can track in shared memory
+constexpr int LSW_COLS = 16;
+
+__global__ void __launch_bounds__(1024)
+laswp_plan_kernel(int k1, int k2, const int *__restrict__ ipiv, int inc, int *__restrict__ moves,
+                  int *__restrict__ nmoves, int *__restrict__ ok) {
+  extern __shared__ int perm[];  // LSW_SPAN entries
+  __shared__ int s_hi, s_cnt;
+  const int tid = threadIdx.x;
+  if (tid == 0) { s_hi = k2; s_cnt = 0; }
+  __syncthreads();
+  for (int k = k1 + tid; k < k2; k += blockDim.x) atomicMax(&s_hi, ipiv[k] + 1);
+  __syncthreads();
+  const int span = s_hi - k1;
+  if (span > LSW_SPAN) {  // rows too far apart for the plan: caller falls back
+    if (tid == 0) { *ok = 0; *nmoves = 0; }
+    return;
+  }
+  for (int r = tid; r < span; r += blockDim.x) perm[r] = k1 + r;
+  __syncthreads();
+  if (tid == 0) {
+    if (inc > 0) {
+      for (int k = k1; k < k2; k++) {
+        const int a = k - k1, b = ipiv[k] - k1;
+        const int t = perm[a]; perm[a] = perm[b]; perm[b] = t;
+      }
+    } else {
+      for (int k = k2 - 1; k >= k1; k--) {
+        const int a = k - k1, b = ipiv[k] - k1;
+        const int t = perm[a]; perm[a] = perm[b]; perm[b] = t;
+      }
+    }
+  }
+  __syncthreads();
+  for (int r = tid; r < span; r += blockDim.x) {
+    if (perm[r] != k1 + r) {
+      const int slot = atomicAdd(&s_cnt, 1);
+      moves[2 * slot] = k1 + r;     // destination row
+      moves[2 * slot + 1] = perm[r];  // source row
+    }
+  }
+  __syncthreads();
+  if (tid == 0) { *nmoves = s_cnt; *ok = 1; }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256)
-laswp_kernel(int ncols, T *A, long lda, int k1, int k2, const int *__restrict__ ipiv, int inc) {
-  __shared__ int sp[256];
+laswp_apply_kernel(int ncols, T *A, long lda, const int *__restrict__ moves, const int *__restrict__ nmoves) {
+  extern __shared__ __align__(16) unsigned char lsw_smem[];
+  T *buf = reinterpret_cast<T *>(lsw_smem);  // [2*LSW_MAXP][LSW_COLS]
+  const int nm = *nmoves, c0 = blockIdx.x * LSW_COLS, tid = threadIdx.x;
+  const int nc = min(LSW_COLS, ncols - c0);
+  for (int idx = tid; idx < nm * LSW_COLS; idx += 256) {
+    const int m = idx / LSW_COLS, c = idx % LSW_COLS;
+    if (c < nc) buf[idx] = A[moves[2 * m + 1] + (long)(c0 + c) * lda];
+  }
+  __syncthreads();
+  for (int idx = tid; idx < nm * LSW_COLS; idx += 256) {
+    const int m = idx / LSW_COLS, c = idx % LSW_COLS;
+    if (c < nc) A[moves[2 * m] + (long)(c0 + c) * lda] = buf[idx];
+  }
+}
+
+// Sequential fallback (one thread per column) for pivots spread over more
+// rows than a plan can track.
+template <typename T>
+__global__ void __launch_bounds__(256)
+laswp_seq_kernel(int ncols, T *A, long lda, int k1, int k2, const int *__restrict__ ipiv, int inc,
+                 const int *__restrict__ ok) {
+  if (*ok) return;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  T *col = A + (long)min(c, ncols - 1) * lda;
-  const int n = k2 - k1, nch = (n + 255) / 256;
-  for (int ci = 0; ci < nch; ci++) {
-    const int ch = inc > 0 ? ci : nch - 1 - ci;
-    const int base = k1 + ch * 256, cnt = min(256, k2 - base);
-    __syncthreads();
-    if ((int)threadIdx.x < cnt) sp[threadIdx.x] = ipiv[base + threadIdx.x];
-    __syncthreads();
-    if (c < ncols) {
-      if (inc > 0) {
-        for (int i = 0; i < cnt; i++) {
-          const int p = sp[i], k = base + i;
-          if (p != k) { T t = col[k]; col[k] = col[p]; col[p] = t; }
-        }
-      } else {
-        for (int i = cnt - 1; i >= 0; i--) {
-          const int p = sp[i], k = base + i;
-          if (p != k) { T t = col[k]; col[k] = col[p]; col[p] = t; }
-        }
-      }
+  if (c >= ncols) return;
+  T *col = A + (long)c * lda;
+  if (inc > 0) {
+    for (int k = k1; k < k2; k++) {
+      const int p = ipiv[k];
+      if (p != k) { T t = col[k]; col[k] = col[p]; col[p] = t; }
+    }
+  } else {
+    for (int k = k2 - 1; k >= k1; k--) {
+      const int p = ipiv[k];
+      if (p != k) { T t = col[k]; col[k] = col[p]; col[p] = t; }
     }
   }
 }
@@ -271,6 +330,20 @@ __global__ void finish_info_kernel(int *d) { if (*d == 0x7fffffff) *d = 0; }
 
 }  // namespace
 
+template <typename T>
+void trinv_dev(int n, const T *Tp, long tr, long tc, int lower, int unit, T *W, cudaStream_t st) {
+  constexpr int smem = 2 * LEAF * (LEAF + 1) * (int)sizeof(T);
+  static bool configured = false;
+  if (!configured) {
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(trinv_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    configured = true;
+  }
+  trinv_kernel<T><<<cdiv(n, LEAF), LEAF, smem, st>>>(n, Tp, tr, tc, lower, unit, W);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
+template void trinv_dev<double>(int, const double *, long, long, int, int, double *, cudaStream_t);
+template void trinv_dev<float>(int, const float *, long, long, int, int, float *, cudaStream_t);
+
 // The solve proper; W receives the inverted diagonal blocks (ceil(n/64)
 // blocks of 64x64 elements, n = order of the triangle).
 template <typename T>
@@ -302,8 +375,8 @@ void trsm_impl(int side, int uplo, int trans, int diag, int M, int N, T alpha, c
     ATLB_CUDA_CHECK(cudaGetLastError());
   }
   const int nblk = cdiv(n, LEAF);
-  trinv_kernel<T><<<nblk, LEAF, 0, st>>>(n, e.Tp, e.tr, e.tc, e.lower, e.unit, W);
-  ATLB_CUDA_CHECK(cudaGetLastError());
+  (void)nblk;
+  trinv_dev<T>(n, e.Tp, e.tr, e.tc, e.lower, e.unit, W, st);
   e.W = W;
   eff_solve(e, 0, n, m, gemm, st);
 }
@@ -345,7 +418,24 @@ template <typename T>
 void laswp_dev(int ncols, T *A, long lda, int k1, int k2, const int *ipiv, int inc,
                cudaStream_t st) {
   if (ncols <= 0 || k2 <= k1) return;
-  laswp_kernel<T><<<cdiv(ncols, 256), 256, 0, st>>>(ncols, A, lda, k1, k2, ipiv, inc);
+  int *ws = (int *)scratch(kSlotLaswp, sizeof(int) * (4 * LSW_MAXP + 64));
+  int *moves = ws + 64, *nmoves = ws, *ok = ws + 1;
+  constexpr int smem = 2 * LSW_MAXP * LSW_COLS * (int)sizeof(T);
+  static bool configured = false;
+  if (!configured) {
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(laswp_apply_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(laswp_plan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         LSW_SPAN * (int)sizeof(int)));
+    configured = true;
+  }
+  const int nchunk = cdiv(k2 - k1, LSW_MAXP);
+  for (int ci = 0; ci < nchunk; ci++) {
+    const int ch = inc > 0 ? ci : nchunk - 1 - ci;
+    const int a = k1 + ch * LSW_MAXP, b = std::min(k2, a + LSW_MAXP);
+    laswp_plan_kernel<<<1, 1024, LSW_SPAN * sizeof(int), st>>>(a, b, ipiv, inc, moves, nmoves, ok);
+    laswp_apply_kernel<T><<<cdiv(ncols, LSW_COLS), 256, smem, st>>>(ncols, A, lda, moves, nmoves);
+    laswp_seq_kernel<T><<<cdiv(ncols, 256), 256, 0, st>>>(ncols, A, lda, a, b, ipiv, inc, ok);
+  }
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
 template void laswp_dev<double>(int, double *, long, int, int, const int *, int, cudaStream_t);

@@ -1,0 +1,130 @@
+// Triangular solve for a few right-hand sides (NRHS <= 8) in ONE launch.
+//
+// The recursive TRSM (trsm.cu) issues ~2n/64 launches, which for one
+// right-hand side is all latency.  Here one CTA owns one 64-row block of the
+// solution: it takes a ticket from an atomic counter (tickets are handed out
+// in launch order, so every block it depends on is owned by a CTA that is
+// already running and never waits on it), accumulates the products with the
+// solved blocks as their "done" flags appear, multiplies by the inverted
+// diagonal block (trinv_kernel's W) and publishes its block.  Every wait on a
+// flag is bounded: after ~1 s the kernel records an error in *err and stops
+// waiting (the result is then wrong but the GPU is released).  The launcher
+// clears the ticket counter and the flags before each launch.
+#include <algorithm>
+#include "common.cuh"
+#include "kernels.h"
+
+namespace atlb {
+namespace {
+
+constexpr int BS = 64;
+
+__device__ __forceinline__ uint64_t gtimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ int ld_acquire(const int *p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+template <typename T, int NR>
+__global__ void __launch_bounds__(256)
+trsv_kernel(int n, int nrhs, const T *__restrict__ Tp, long tr, long tc, int lower,
+            const T *__restrict__ W, T *X, long ldx, int *counter, int *flags, int epoch, int *err) {
+  __shared__ T sacc[4][BS][NR];
+  __shared__ T sx[BS][NR];
+  __shared__ int s_bi;
+  const int tid = threadIdx.x, nb = (n + BS - 1) / BS;
+  if (tid == 0) {
+    const int t = atomicAdd(counter, 1);
+    s_bi = lower ? t : nb - 1 - t;
+  }
+  __syncthreads();
+  const int bi = s_bi, r0 = bi * BS, rows = min(BS, n - r0);
+  const int r = tid % BS, part = tid / BS;  // 4 partial sums per row
+  T acc[NR];
+#pragma unroll
+  for (int q = 0; q < NR; q++) acc[q] = T(0);
+  // contributions of the already-solved blocks, in dependency order
+  for (int d = 0; d < (lower ? bi : nb - 1 - bi); d++) {
+    const int bj = lower ? d : nb - 1 - d, c0 = bj * BS, cols = min(BS, n - c0);
+    if (tid == 0) {
+      const uint64_t t0 = gtimer();
+      while (ld_acquire(flags + bj) != epoch) {
+        if (gtimer() - t0 > 1000000000ull) { atomicExch(err, 1); break; }
+        __nanosleep(64);
+      }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < cols * NR; idx += 256) {
+      const int c = idx % cols, q = idx / cols;
+      sx[c][q] = q < nrhs ? __ldcg(X + c0 + c + (long)q * ldx) : T(0);
+    }
+    __syncthreads();
+    if (r < rows) {
+      const T *tp = Tp + (long)(r0 + r) * tr + (long)c0 * tc;
+      for (int c = part; c < cols; c += 4) {
+        const T t = tp[(long)c * tc];
+#pragma unroll
+        for (int q = 0; q < NR; q++) acc[q] = fma(t, sx[c][q], acc[q]);
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < NR; q++) sacc[part][r][q] = acc[q];
+  __syncthreads();
+  // right-hand side minus the accumulated products, then times inv(T_ii)
+  for (int idx = tid; idx < BS * NR; idx += 256) {
+    const int rr = idx % BS, q = idx / BS;
+    T v = T(0);
+    if (rr < rows && q < nrhs)
+      v = X[r0 + rr + (long)q * ldx] - (sacc[0][rr][q] + sacc[1][rr][q] + sacc[2][rr][q] + sacc[3][rr][q]);
+    sx[rr][q] = v;
+  }
+  __syncthreads();
+  const T *Wb = W + (long)bi * BS * BS;
+  if (tid < BS * NR && tid % BS < rows) {
+    const int rr = tid % BS, q = tid / BS;
+    T v = T(0);
+    for (int c = 0; c < rows; c++) v = fma(Wb[rr + (long)c * BS], sx[c][q], v);
+    if (q < nrhs) X[r0 + rr + (long)q * ldx] = v;
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(flags + bi), "r"(epoch) : "memory");
+  }
+}
+
+}  // namespace
+
+// Solve op(A) X = B in place for nrhs <= 8 right-hand sides (Left side only).
+template <typename T>
+void trsv_dev(int uplo, int trans, int diag, int n, int nrhs, const T *A, long lda, T *B, long ldb,
+              cudaStream_t st) {
+  if (n <= 0 || nrhs <= 0) return;
+  const bool tr = trans != kNoTrans;
+  const long tstr = tr ? lda : 1, tcol = tr ? 1 : lda;  // effective T(i,k) = A[i*tstr + k*tcol]
+  const int lower = (uplo == kLower) != tr;
+  const int nb = cdiv(n, BS);
+  // workspace: inverted diagonal blocks, ticket counter, flags, error word
+  T *W = (T *)scratch(kSlotTrsmW, sizeof(T) * (size_t)nb * BS * BS);
+  int *ctl = (int *)scratch(kSlotTrsvCtl, sizeof(int) * (nb + 64));
+  const int epoch = 1;
+  int *counter = ctl, *err = ctl + 1, *flags = ctl + 64;
+  ATLB_CUDA_CHECK(cudaMemsetAsync(ctl, 0, sizeof(int) * (nb + 64), st));  // counter, flags
+  trinv_dev<T>(n, A, tstr, tcol, lower, diag == kUnit, W, st);
+  if (nrhs == 1) trsv_kernel<T, 1><<<nb, 256, 0, st>>>(n, nrhs, A, tstr, tcol, lower, W, B, ldb, counter, flags, epoch, err);
+  else if (nrhs <= 4) trsv_kernel<T, 4><<<nb, 256, 0, st>>>(n, nrhs, A, tstr, tcol, lower, W, B, ldb, counter, flags, epoch, err);
+  else trsv_kernel<T, 8><<<nb, 256, 0, st>>>(n, nrhs, A, tstr, tcol, lower, W, B, ldb, counter, flags, epoch, err);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
+template void trsv_dev<double>(int, int, int, int, int, const double *, long, double *, long, cudaStream_t);
+template void trsv_dev<float>(int, int, int, int, int, const float *, long, float *, long, cudaStream_t);
+
+}  // namespace atlb

@@ -5,10 +5,17 @@
 Workload (one "step"): solve A x = b with N = 8192 (one right-hand side),
 A = Q1 diag(s) Q2^T with Q1, Q2 from QR of Gaussian matrices and s geometric
 from 1 to 1/kappa (kappa = 1e2), b uniform[-1, 1]; the solution must reach a
-normwise backward error <= N * 2^-53.  Inputs are seeded synthetic data
-generated on the device; they are larger than L2 (512 MiB), so no flush is
-needed between steps.  Each step restores A from a pristine copy (the solver
-overwrites it), like a caller that keeps its matrix.
+normwise backward error ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf)
+<= N * 2^-53.  The headline `value` is the mixed-precision solver (FP32-class
+factorization on the tensor cores + FP64 iterative refinement, library entry
+atlb_dsgesv_ex); the plain FP64 GPU dgesv (getrf + getrs) on the same system
+is reported beside it, with the speed-up.  Inputs are seeded synthetic data
+generated on the device (larger than L2: 512 MiB, so no flush is needed).
+The FP64 solver overwrites A, so each of its steps restores A from a copy.
+
+Also reported: the FP64 DMMA DGEMM at 8192^3 (the roofline kernel, against
+cuBLAS DGEMM measured in the same run) and the split-integer (Ozaki) DGEMM at
+8192^3 with its error against a double-double oracle on a sampled block.
 
 Every rank runs an independent replica (the factorization of one matrix
 does not shard); value = solves of all ranks / max-over-ranks time.
@@ -29,8 +36,14 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "dgesv N=8192 time @bwd err<=N*eps64: mixed vs FP64 GPU; DGEMM GFLOP/s vs peak"
-N = 8192
+N_DEFAULT = 8192
 KAPPA = 1e2
+UNIT = "solves/s (N=8192, 1 RHS, bwd err <= N*2^-53)"
+# headline mixed configuration: (name, factor precision, pivoting)
+#   precision 0 FP32, 1 TF32, 2 BF16, 3 split TF32 (FP32-accurate); pivoting 0 partial, 1 RBT
+HEADLINE = ("rbt_tf32x3", 3, 1)
+VARIANTS = [("rbt_tf32x3", 3, 1), ("rbt_tf32", 1, 1), ("rbt_fp32", 0, 1), ("pp_tf32x3", 3, 0),
+            ("pp_tf32", 1, 0), ("pp_fp32", 0, 0), ("pp_bf16", 2, 0)]
 
 
 def lu_flops(n):
@@ -116,7 +129,6 @@ def run_reference(args, rank, world):
     """CPU restatement of the reference's dgesv on host cores, bounded sample."""
     if rank != 0:
         return
-    import numpy as np
     from oracle import oracle as O
     cores = os.cpu_count() or 1
     O.orc().orc_set_threads(cores)
@@ -134,20 +146,31 @@ def run_reference(args, rank, world):
         if i >= args.warmup:
             times.append(t1 - t0)
     t_sample = sum(times) / len(times)
-    t_full = t_sample * lu_flops(N) / lu_flops(ns)
+    t_full = t_sample * lu_flops(N_DEFAULT) / lu_flops(ns)
     val = 1.0 / t_full
     line = {
-        "impl": "reference", "metric": METRIC, "value": val, "unit": "solves/s (N=8192, 1 RHS)",
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_full * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded)",
         "config": {"workload": "dgesv N=8192, 1 RHS, FP64 (host CPU restatement of ATLAS getrfC+getrs)"},
-        "cpu_baseline": {"value": val, "unit": "solves/s (N=8192, 1 RHS)", "cores": cores, "kind": "port",
-                         "sample": f"dgesv N={ns} timed, scaled by flop ratio to N={N}"},
-        "e2e": {"value": val, "unit": "solves/s (N=8192, 1 RHS)", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"dgesv N={ns} timed, scaled by flop ratio to N={N_DEFAULT}"},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def timed(torch, stream, fn, reps):
+    """Mean ms of fn() over reps runs, CUDA events on the shared stream."""
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
 
 
 def main():
@@ -157,8 +180,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="atlas", choices=["atlas", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--n", type=int, default=N, help="matrix order (default 8192; smaller for profiling)")
+    ap.add_argument("--n", type=int, default=N_DEFAULT, help="matrix order (default 8192; smaller for profiling)")
     ap.add_argument("--skip-e2e", action="store_true", help="omit the host-buffer leg (profiling)")
+    ap.add_argument("--skip-extras", action="store_true", help="only the headline and FP64 solves (profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     n = args.n
@@ -170,9 +194,9 @@ def main():
     if args.impl == "reference":
         return run_reference(args, rank, world)
 
+    import numpy as np
     import torch
     import torch.distributed as dist
-    import numpy as np
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     if world > 1:
@@ -188,20 +212,18 @@ def main():
     AB.atlb_set_stream(stream.cuda_stream)
 
     acol0, b0 = make_system(torch, n, KAPPA, 1234 + rank, dev)
-    A = torch.empty_like(acol0)
     x = torch.empty_like(b0)
     ipiv = torch.empty(n, dtype=torch.int32, device=dev)
-    info = torch.zeros(1, dtype=torch.int32, device=dev)
-    launches = {"n": 0}
+    it = np.zeros(1, dtype=np.int32)
+    _, hprec, hpiv = HEADLINE
 
-    def step():
-        A.copy_(acol0)
-        x.copy_(b0)
-        AB.atlb_dgetrf_dev(n, n, A, n, ipiv, info)
-        AB.atlb_dgetrs_dev(111, n, 1, A, n, ipiv, x, n)
+    def mixed_step():
+        r = AB.atlb_dsgesv_ex(n, 1, acol0, n, ipiv, b0, n, x, n, hprec, hpiv, it)
+        assert r == 0
 
+    # ---- headline: mixed-precision solve, timed steps
     for _ in range(args.warmup):
-        step()
+        mixed_step()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -210,7 +232,7 @@ def main():
         torch.cuda.synchronize()
         ev0.record(stream)
         for _ in range(args.steps):
-            step()
+            mixed_step()
         ev1.record(stream)
         torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1) / args.steps
@@ -219,77 +241,113 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = t.item()
         dist.barrier()
-    berr = backward_error(torch, acol0, x, b0)
-    assert int(info.item()) == 0
+    head_iter = int(it[0])
+    head_berr = backward_error(torch, acol0, x, b0)
     value = world * 1000.0 / ms
 
-    # mixed-precision solves of the same system (factor FP32 / TF32 / BF16, FP64 refinement)
-    mixed = {}
-    xm = torch.empty(n, dtype=torch.float64, device=dev)
-    ipm = torch.empty(n, dtype=torch.int32, device=dev)
-    it = np.zeros(1, dtype=np.int32)
-    for name, prec in (("tf32", 1), ("bf16", 2), ("fp32", 0)):
+    # ---- plain FP64 GPU dgesv (getrf + getrs) on the same system
+    A = torch.empty_like(acol0)
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def fp64_step():
+        A.copy_(acol0)
+        x.copy_(b0)
+        AB.atlb_dgetrf_dev(n, n, A, n, ipiv, info)
+        AB.atlb_dgetrs_dev(111, n, 1, A, n, ipiv, x, n)
+
+    for _ in range(2):
+        fp64_step()
+    fp64_ms = timed(torch, stream, fp64_step, max(2, args.steps // 2))
+    assert int(info.item()) == 0
+    fp64_berr = backward_error(torch, acol0, x, b0)
+    del A
+
+    out = {}
+    if not args.skip_extras:
+        # ---- every mixed configuration (iterations, time, backward error)
+        mixed = {}
+        for name, prec, piv in VARIANTS:
+            call = lambda: AB.atlb_dsgesv_ex(n, 1, acol0, n, ipiv, b0, n, x, n, prec, piv, it)
+            for _ in range(2):
+                call()
+            t_ms = timed(torch, stream, call, max(2, args.steps // 3))
+            mixed[name] = {"ms": t_ms, "iter": int(it[0]), "backward_error": backward_error(torch, acol0, x, b0)}
+        out["mixed_variants"] = mixed
+
+        # ---- the roofline kernel: FP64 DMMA DGEMM 8192^3 vs cuBLAS DGEMM (denominator)
+        M = 8192
+        flop = 2.0 * M ** 3
+        ga = torch.rand(M, M, dtype=torch.float64, device=dev) * 2 - 1
+        gb = torch.rand(M, M, dtype=torch.float64, device=dev) * 2 - 1
+        gc = torch.zeros(M, M, dtype=torch.float64, device=dev)
+        dg = lambda: AB.atlb_dgemm_dev(111, 111, M, M, M, 1.0, ga, M, gb, M, 0.0, gc, M)
         for _ in range(2):
-            AB.atlb_dsgesv(n, 1, acol0, n, ipm, b0, n, xm, n, prec, it)
-        ts = []
-        for _ in range(max(2, args.steps // 2)):
-            e0m, e1m = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0m.record(stream)
-            r = AB.atlb_dsgesv(n, 1, acol0, n, ipm, b0, n, xm, n, prec, it)
-            e1m.record(stream)
-            torch.cuda.synchronize()
-            ts.append(e0m.elapsed_time(e1m))
-        mixed[name] = {"ms": sum(ts) / len(ts), "iter": int(it[0]), "info": int(r),
-                       "backward_error": backward_error(torch, acol0, xm, b0)}
+            dg()
+        dgemm_ms = timed(torch, stream, dg, 5)
+        for _ in range(2):
+            torch.matmul(ga, gb, out=gc)
+        cublas_ms = timed(torch, stream, lambda: torch.matmul(ga, gb, out=gc), 5)
+        dgemm_tf, cublas_tf = flop / dgemm_ms / 1e9, flop / cublas_ms / 1e9
+        out["dgemm_8192"] = {"ms": dgemm_ms, "tflops": dgemm_tf, "cublas_fp64_tflops": cublas_tf}
+        out["roofline"] = {"bound": "tensor", "achieved": dgemm_tf, "peak": cublas_tf, "unit": "TFLOP/s",
+                           "frac": dgemm_tf / cublas_tf, "traffic": None,
+                           "kernel": "dgemm_dmma_kernel 8192^3 (2*M*N*K flop per launch)",
+                           "peak_note": "no FP64 figure in MEASURED_PEAKS.json; peak = cuBLAS DGEMM 8192^3 measured in this run"}
+        del ga, gb
 
-    # dominant kernel: the FP64 DMMA GEMM, timed alone at 8192^3
-    M = 8192
-    ga = torch.rand(M, M, dtype=torch.float64, device=dev) * 2 - 1
-    gb = torch.rand(M, M, dtype=torch.float64, device=dev) * 2 - 1
-    gc = torch.zeros(M, M, dtype=torch.float64, device=dev)
-    for _ in range(2):
-        AB.atlb_dgemm_dev(111, 111, M, M, M, 1.0, ga, M, gb, M, 0.0, gc, M)
-    reps = 5
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(reps):
-        AB.atlb_dgemm_dev(111, 111, M, M, M, 1.0, ga, M, gb, M, 0.0, gc, M)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    dgemm_ms = e0.elapsed_time(e1) / reps
-    dgemm_tf = 2.0 * M ** 3 / (dgemm_ms * 1e-3) / 1e12
-    # measured FP64 denominator: cuBLAS DGEMM at the same size (library, denominator only)
-    for _ in range(2):
-        torch.matmul(ga, gb, out=gc)
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(reps):
-        torch.matmul(ga, gb, out=gc)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    cublas_tf = 2.0 * M ** 3 / (e0.elapsed_time(e1) / reps * 1e-3) / 1e12
-    del ga, gb, gc
+        # ---- split-integer (Ozaki) DGEMM 8192^3 on the INT8 tensor cores
+        # operands x = u * 2^e, u ~ U[-1,1], e ~ U{-10..10}; storage tensors hold
+        # the column-major matrices, i.e. logical A = oa^T, B = ob^T, C = gc^T
+        g = torch.Generator(device=dev)
+        g.manual_seed(99)
+        oa = (torch.rand(M, M, dtype=torch.float64, device=dev, generator=g) * 2 - 1) * \
+            torch.exp2(torch.randint(-10, 11, (M, M), device=dev, generator=g).double())
+        ob = (torch.rand(M, M, dtype=torch.float64, device=dev, generator=g) * 2 - 1) * \
+            torch.exp2(torch.randint(-10, 11, (M, M), device=dev, generator=g).double())
+        from oracle import oracle as O
+        O.orc().orc_set_threads(os.cpu_count() or 1)
+        idx = torch.arange(0, M, M // 48, device=dev)[:48]
+        a_rows = np.asfortranarray(oa[:, idx].T.cpu().numpy())     # A[idx, :]
+        b_cols = np.asfortranarray(ob[idx, :].T.cpu().numpy())     # B[:, idx]
+        hi, lo = O.ddgemm(a_rows, b_cols)                          # double-double C[idx, idx]
 
-    # end to end through the drop-in C ABI with pinned host buffers
-    e2e_val = None
+        def block(c):
+            return np.asfortranarray(c[idx][:, idx].T.cpu().numpy())
+
+        AB.atlb_dgemm_dev(111, 111, M, M, M, 1.0, oa, M, ob, M, 0.0, gc, M)
+        oz = {"plain_fp64_err": O.normwise_err_dd(block(gc), hi, lo),
+              "sample": "48x48 block of C vs double-double oracle"}
+        for s in (6, 7, 8):
+            f = lambda: AB.atlb_dgemm_ozaki_dev(111, 111, M, M, M, 1.0, oa, M, ob, M, 0.0, gc, M, s)
+            f()
+            t_ms = timed(torch, stream, f, 3)
+            oz[f"slices{s}"] = {"ms": t_ms, "effective_tflops": flop / t_ms / 1e9,
+                                 "err_vs_dd": O.normwise_err_dd(block(gc), hi, lo),
+                                 "speedup_vs_dmma_dgemm": dgemm_ms / t_ms}
+        out["ozaki_8192"] = oz
+        del gc, oa, ob
+
+    # ---- end to end through the C ABI with pinned host buffers (H2D of A and b,
+    # D2H of x inside the timed region)
+    e2e = None
     if not args.skip_e2e:
         ha = torch.empty(n * n, dtype=torch.float64, pin_memory=True)
         hb = torch.empty(n, dtype=torch.float64, pin_memory=True)
-        ha_src = acol0.reshape(-1).cpu()
-        hb_src = b0.cpu()
+        hx = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        ha.copy_(acol0.reshape(-1).cpu())
+        hb.copy_(b0.cpu())
         hip = np.zeros(n, dtype=np.int32)
         e2e_t = []
         for i in range(2 + max(2, args.steps // 3)):
-            ha.copy_(ha_src)
-            hb.copy_(hb_src)
             t0 = time.perf_counter()
-            r = AB.clapack_dgesv(AB.CblasColMajor, n, 1, ha, n, hip, hb, n)
+            r = AB.atlb_dsgesv_ex(n, 1, ha, n, hip, hb, n, hx, n, hprec, hpiv, it)
             t1 = time.perf_counter()
             assert r == 0
             if i >= 2:
                 e2e_t.append(t1 - t0)
-        e2e_val = world / (sum(e2e_t) / len(e2e_t))
+        e2e = {"value": world / (sum(e2e_t) / len(e2e_t)), "unit": UNIT,
+               "h2d_bytes_per_step": n * n * 8 + n * 8, "d2h_bytes_per_step": n * 8,
+               "path": "atlb_dsgesv_ex with pinned host A, b, x"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -306,30 +364,28 @@ def main():
             lu, ip, _ = O.dgetrf(a)
             O.dgetrs(111, lu, ip, bb.copy(order="F"))
             ts.append(time.perf_counter() - t0)
-        tcpu = min(ts) * lu_flops(n) / lu_flops(ns)
-        cpu = {"value": 1.0 / tcpu, "unit": "solves/s (N=8192, 1 RHS)", "cores": cores, "kind": "port",
-               "sample": f"oracle getrf+getrs N={ns}, scaled by flop ratio to N={n}"}
+        tcpu = min(ts) * lu_flops(N_DEFAULT) / lu_flops(ns)
+        cpu = {"value": 1.0 / tcpu, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"oracle getrf+getrs N={ns}, scaled by flop ratio to N={N_DEFAULT}"}
 
     if rank == 0:
-        gflops = lu_flops(n) / (ms * 1e-3) / 1e9
         line = {
-            "metric": METRIC, "value": value, "unit": "solves/s (N=8192, 1 RHS)", "n_gpus": world,
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, on device)",
-            "config": {"workload": "dgesv N=8192 1 RHS, FP64 getrf+getrs (kappa=1e2 Q1 diag(s) Q2^T)",
+            "config": {"workload": f"mixed dgesv N={n} 1 RHS ({HEADLINE[0]}) vs FP64 dgesv, kappa=1e2 Q1 diag(s) Q2^T",
                        "n": n, "nrhs": 1, "kappa": KAPPA, "parallelism": f"replicas x{world}",
                        "l2": "inputs 512 MiB > L2, no flush"},
-            "fp64_dgesv_gflops": gflops, "mixed_dgesv": mixed, "backward_error": berr, "bwd_err_bound": n * 2.0 ** -53,
-            "dgemm_8192": {"ms": dgemm_ms, "tflops": dgemm_tf, "cublas_fp64_tflops": cublas_tf},
-            "roofline": {"bound": "tensor", "achieved": dgemm_tf, "peak": cublas_tf, "unit": "TFLOP/s",
-                         "frac": dgemm_tf / cublas_tf, "traffic": None,
-                         "peak_note": "FP64: no measured peak in MEASURED_PEAKS.json; denominator = cuBLAS DGEMM 8192^3 measured in this run"},
+            "headline": {"solver": HEADLINE[0], "ms": ms, "iter": head_iter, "backward_error": head_berr,
+                         "bwd_err_bound": n * 2.0 ** -53},
+            "fp64_dgesv": {"ms": fp64_ms, "gflops": lu_flops(n) / fp64_ms / 1e6, "backward_error": fp64_berr},
+            "speedup_mixed_vs_fp64": fp64_ms / ms,
             "clocks": clk.summary(),
-            "e2e": {"value": e2e_val, "unit": "solves/s (N=8192, 1 RHS)", "h2d_bytes_per_step": n * n * 8 + n * 8,
-                    "d2h_bytes_per_step": n * n * 8 + n * 8 + n * 4},
+            "e2e": e2e,
             "cpu_baseline": cpu,
             "gpu_launches": None,
         }
+        line.update(out)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -115,7 +115,8 @@ int atlb_dgemm_dev(int TransA, int TransB, int M, int N, int K, double alpha, co
 int atlb_sgemm_dev(int TransA, int TransB, int M, int N, int K, float alpha, const float *A,
                    int lda, const float *B, int ldb, float beta, float *C, int ldc);
 /* FP32 GEMM on the tensor cores: operands rounded to TF32 (prec 1) or BF16
- * (prec 2), FP32 accumulation (tcgen05, TMEM accumulators). */
+ * (prec 2), or split into TF32 high/low parts for an FP32-accurate product
+ * (prec 3); FP32 accumulation (tcgen05, TMEM accumulators). */
 int atlb_sgemm_tc_dev(int prec, int TransA, int TransB, int M, int N, int K, float alpha,
                       const float *A, int lda, const float *B, int ldb, float beta, float *C,
                       int ldc);
@@ -132,8 +133,8 @@ int atlb_dgeqrf_dev(int M, int N, double *A, int lda, double *tau);
 
 /* Mixed-precision solvers (no counterpart in the reference; LAPACK's
  * dsgesv/dsposv contract).  Factor an FP32 copy of A on the GPU -- trailing
- * updates in FP32 (prec 0), on the tensor cores in TF32 (1) or BF16 with FP32
- * accumulation (2) -- then refine in FP64 until every column reaches a
+ * updates in FP32 (prec 0), on the tensor cores in TF32 (1), BF16 with FP32
+ * accumulation (2), or FP32-accurate split TF32 (3) -- then refine in FP64 until every column reaches a
  * normwise backward error ||b-Ax||_inf/(||A||_inf ||x||_inf + ||b||_inf) <=
  * N*2^-53.  A and B are unchanged and *iter >= 0 (refinement steps) on
  * success; otherwise the FP64 solver runs, A/ipiv hold its factors and *iter
@@ -144,6 +145,14 @@ int atlb_dsgesv(int N, int NRHS, double *A, int lda, int *ipiv, double *B, int l
                 int ldx, int prec, int *iter);
 int atlb_dsposv(int Uplo, int N, int NRHS, double *A, int lda, double *B, int ldb, double *X,
                 int ldx, int prec, int *iter);
+/* atlb_dsgesv with a choice of factorization: pivoting 0 = partial pivoting
+ * (as atlb_dsgesv), 1 = random butterfly transformation U^T A V of the
+ * matrix followed by LU without pivoting (no column-by-column pivot search;
+ * the FP64 refinement against the original A restores accuracy, and the FP64
+ * fallback covers a failed factorization).  ipiv is only written by the
+ * fallback. */
+int atlb_dsgesv_ex(int N, int NRHS, double *A, int lda, int *ipiv, double *B, int ldb, double *X,
+                   int ldx, int prec, int pivoting, int *iter);
 
 /* Split-integer (Ozaki) DGEMM: C = alpha*op(A)*op(B) + beta*C with FP64
  * operands cut into `slices` (2..12) signed 7-bit digit planes after exact

@@ -26,8 +26,8 @@ def bwd_err(a, x, b):
                                         + np.max(np.abs(b), axis=0))
 
 
-@pytest.mark.parametrize("prec", [0, 1, 2])
-@pytest.mark.parametrize("n,nrhs", [(300, 1), (1000, 3)])
+@pytest.mark.parametrize("prec", [0, 1, 2, 3])
+@pytest.mark.parametrize("n,nrhs", [(300, 1), (1000, 3), (700, 12)])
 def test_dsgesv_kappa_1e2(gpu, prec, n, nrhs):
     a0 = kappa_matrix(n, 1e2, n + prec)
     b0 = np.asfortranarray(np.random.default_rng(5).uniform(-1, 1, (n, nrhs)))
@@ -69,7 +69,7 @@ def test_dsgesv_singular(gpu):
     assert it[0] == -3
 
 
-@pytest.mark.parametrize("prec", [0, 1, 2])
+@pytest.mark.parametrize("prec", [0, 1, 2, 3])
 @pytest.mark.parametrize("uplo", [121, 122])
 def test_dsposv(gpu, prec, uplo):
     n, nrhs = 500, 2
@@ -86,3 +86,31 @@ def test_dsposv(gpu, prec, uplo):
     assert it[0] >= 0
     assert np.all(bwd_err(a0, x, b0) <= n * 2.0 ** -53)
     np.testing.assert_array_equal(np.isnan(a), np.isnan(a_in))
+
+
+@pytest.mark.parametrize("prec", [0, 1, 3])
+@pytest.mark.parametrize("n,nrhs", [(512, 1), (1001, 2), (258, 9)])
+def test_dsgesv_rbt_nopivot(gpu, prec, n, nrhs):
+    a0 = kappa_matrix(n, 1e2, 3 * n + prec)
+    b0 = np.asfortranarray(np.random.default_rng(7).uniform(-1, 1, (n, nrhs)))
+    a, b = a0.copy(order="F"), b0.copy(order="F")
+    x = np.zeros((n, nrhs), order="F")
+    ipiv = np.zeros(n, dtype=np.int32)
+    it = np.zeros(1, dtype=np.int32)
+    assert AB.atlb_dsgesv_ex(n, nrhs, a, n, ipiv, b, n, x, n, prec, 1, it) == 0
+    assert it[0] >= 0, it[0]
+    assert np.all(bwd_err(a0, x, b0) <= n * 2.0 ** -53)
+    assert np.array_equal(a, a0) and np.array_equal(b, b0)
+
+
+def test_dsgesv_rbt_matrix_without_pivot_needs(gpu):
+    # a matrix that defeats LU without pivoting (zero leading entry) is handled
+    n = 64
+    a0 = O.lu_matrix(n, 11)
+    a0[0, 0] = 0.0
+    b0 = np.ones((n, 1), order="F")
+    x = np.zeros((n, 1), order="F")
+    it = np.zeros(1, dtype=np.int32)
+    ipiv = np.zeros(n, dtype=np.int32)
+    assert AB.atlb_dsgesv_ex(n, 1, a0.copy(order="F"), n, ipiv, b0, n, x, n, 3, 1, it) == 0
+    assert np.all(bwd_err(a0, x, b0) <= n * 2.0 ** -53)

@@ -20,7 +20,7 @@ def _round(x, prec):
     return np.frombuffer(u.astype(np.uint32).tobytes(), dtype=np.float32).reshape(x.shape).astype(np.float64)
 
 
-@pytest.mark.parametrize("prec", [1, 2])
+@pytest.mark.parametrize("prec", [1, 2, 3])
 @pytest.mark.parametrize("ta,tb", [(111, 111), (111, 112), (112, 111), (112, 112)])
 @pytest.mark.parametrize("m,n,k", [(128, 128, 64), (300, 200, 517), (1000, 257, 96), (77, 1030, 33)])
 def test_tc_sgemm(gpu, orc, prec, ta, tb, m, n, k):
@@ -36,10 +36,16 @@ def test_tc_sgemm(gpu, orc, prec, ta, tb, m, n, k):
     assert AB.atlb_sgemm_tc_dev(prec, ta, tb, m, n, k, 1.5, dA, lda, dB, ldb, -0.5, dC, m) == 0
     AB.atlb_sync()
     C = dC.cpu().numpy().T
-    opA = _round(A, prec) if ta == 111 else _round(A, prec).T
-    opB = _round(B, prec) if tb == 111 else _round(B, prec).T
+    if prec == 3:   # split TF32: FP32-accurate products of the FP32 operands
+        opA = (A if ta == 111 else A.T).astype(np.float64)
+        opB = (B if tb == 111 else B.T).astype(np.float64)
+    else:
+        opA = _round(A, prec) if ta == 111 else _round(A, prec).T
+        opB = _round(B, prec) if tb == 111 else _round(B, prec).T
     ref = 1.5 * (opA @ opB) - 0.5 * C0.astype(np.float64)
     bound = 1.5 * k * 2.0 ** -22 * (np.abs(opA) @ np.abs(opB)) + 2.0 ** -22 * np.abs(ref) + 1e-6
+    if prec == 3:   # plus the dropped lo*lo term and the TF32 rounding of the low parts
+        bound = bound + 1.5 * 2.0 ** -19 * (np.abs(opA) @ np.abs(opB))
     assert np.all(np.abs(C - ref) <= bound), np.max(np.abs(C - ref) / bound)
 
 
