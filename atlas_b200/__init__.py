@@ -69,6 +69,13 @@ _SIGS = {
     "atlb_dgemm_ozaki": (_I, [_I, _I, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I, _I]),
     "atlb_dsgesv": (_I, [_I, _I, _P, _I, _P, _P, _I, _P, _I, _I, _P]),
     "atlb_dsgesv_ex": (_I, [_I, _I, _P, _I, _P, _P, _I, _P, _I, _I, _I, _P]),
+    "atlb_dgemm_batched_dev": (_I, [_I, _I, _I, _P, _P, _P, _D, _P, _P, _P, _P, _D, _P, _P]),
+    "atlb_dposv_batched": (_I, [_I, _P, _P, _P, _P, _P, _P, _P]),
+    "atlb_dgesv_batched": (_I, [_I, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "atlb_dpotrf_adjoint_dev": (_I, [_I, _P, _I, _P, _I, _P, _I]),
+    "atlb_dpotrs_adjoint_dev": (_I, [_I, _I, _P, _I, _P, _I, _P, _I, _P, _I, _P, _I]),
+    "atlb_dgetrs_adjoint_dev": (_I, [_I, _I, _P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I]),
+    "atlb_dgetrf_adjoint_dev": (_I, [_I, _P, _I, _P, _P, _I, _P, _I, _P, _I]),
     "atlb_dsposv": (_I, [_I, _I, _I, _P, _I, _P, _I, _P, _I, _I, _P]),
 }
 
@@ -96,6 +103,8 @@ def ptr(x):
         return None
     if isinstance(x, int):
         return x
+    if isinstance(x, ctypes.Array):
+        return ctypes.addressof(x)
     if hasattr(x, "data_ptr"):  # torch tensor
         return x.data_ptr()
     if hasattr(x, "ctypes"):  # numpy array

@@ -7,6 +7,7 @@
 // transposed factorization for getrf/getrs/potrf/potrs, LQ-of-the-view for
 // geqrf).
 #include <algorithm>
+#include <vector>
 #include "common.cuh"
 #include "kernels.h"
 #include "../../include/atlas_b200.h"
@@ -526,6 +527,29 @@ int atlb_sgemm_tc_dev(int prec, int TA, int TB, int M, int N, int K, float alpha
   (prec == 1 ? sgemm_tf32_dev : prec == 2 ? sgemm_bf16_dev : sgemm_tf32x3_dev)(TA == kNoTrans ? kNoTrans : kTrans,
                                                 TB == kNoTrans ? kNoTrans : kTrans, M, N, K, alpha,
                                                 A, lda, B, ldb, beta, C, ldc, stream(), 0);
+  return 0;
+}
+
+int atlb_dgemm_batched_dev(int TA, int TB, int count, const int *M, const int *N, const int *K,
+                           double alpha, const double *const *A, const int *lda,
+                           const double *const *B, const int *ldb, double beta, double *const *C,
+                           const int *ldc) {
+  if (bad_trans(TA)) return -1;
+  if (bad_trans(TB)) return -2;
+  if (count < 0) return -3;
+  if (count == 0) return 0;
+  std::vector<GemmProb> P(count);
+  for (int i = 0; i < count; i++) {
+    if (M[i] < 0) return -4;
+    if (N[i] < 0) return -5;
+    if (K[i] < 0) return -6;
+    if (lda[i] < std::max(1, TA == kNoTrans ? M[i] : K[i])) return -9;
+    if (ldb[i] < std::max(1, TB == kNoTrans ? K[i] : N[i])) return -11;
+    if (ldc[i] < std::max(1, M[i])) return -14;
+    P[i] = {A[i], B[i], C[i], M[i], N[i], K[i], lda[i], ldb[i], ldc[i], alpha, beta};
+  }
+  dgemm_grouped_dev(TA == kNoTrans ? kNoTrans : kTrans, TB == kNoTrans ? kNoTrans : kTrans, P.data(),
+                    count, stream());
   return 0;
 }
 

@@ -8,6 +8,9 @@
 // 64x32 block of C in registers with DMMA.  The same kernel computes one
 // triangle of C for SYRK (tiles outside the triangle exit at once; elements
 // outside it are not stored).
+#include <algorithm>
+#include <cstring>
+#include <vector>
 #include "common.cuh"
 #include "kernels.h"
 
@@ -93,29 +96,17 @@ __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
       : "d"(a), "d"(b));
 }
 
-// C = alpha*op(A)*op(B) + beta*C (column-major).  tri: 0 full, 1 lower
-// (store row >= col), 2 upper (row <= col).
+// One 128x128 tile of C = alpha*op(A)*op(B) + beta*C (column-major) at
+// (m0, n0).  tri: 0 full, 1 lower (store row >= col), 2 upper (row <= col).
 template <bool TA, bool TB, int VEC>
-__global__ void __launch_bounds__(THREADS, 1)
-dgemm_dmma_kernel(int M, int N, int K, double alpha, const double *__restrict__ A, long lda,
-                  const double *__restrict__ B, long ldb, double beta, double *__restrict__ C,
-                  long ldc, int tri) {
-  extern __shared__ __align__(16) double smem[];
+__device__ __forceinline__ void dgemm_tile(int M, int N, int K, double alpha, const double *__restrict__ A,
+                                           long lda, const double *__restrict__ B, long ldb, double beta,
+                                           double *__restrict__ C, long ldc, int tri, int m0, int n0,
+                                           double *smem) {
   using LA = Lay<TA>;   // A k-contiguous when transposed
   using LB = Lay<!TB>;  // B k-contiguous when not transposed
   double *sA = smem;
   double *sB = smem + STAGES * LA::SIZE;
-
-  const int tiles_m = (M + BM - 1) / BM, tiles_n = (N + BN - 1) / BN;
-  // grouped rasterisation: 8 tile-rows share B panels in L2
-  const int bid = blockIdx.x, G = 8;
-  const int per_group = G * tiles_n, group = bid / per_group;
-  const int first_m = group * G, gsz = min(tiles_m - first_m, G);
-  const int tm = first_m + (bid % per_group) % gsz, tn = (bid % per_group) / gsz;
-  const int m0 = tm * BM, n0 = tn * BN;
-  if (tri == 1 && m0 + BM - 1 < n0) return;
-  if (tri == 2 && m0 > n0 + BN - 1) return;
-
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = (warp & 1) * 64, wn = (warp >> 1) * 32;
 
@@ -187,6 +178,53 @@ dgemm_dmma_kernel(int M, int N, int K, double alpha, const double *__restrict__ 
   }
 }
 
+template <bool TA, bool TB, int VEC>
+__global__ void __launch_bounds__(THREADS, 1)
+dgemm_dmma_kernel(int M, int N, int K, double alpha, const double *__restrict__ A, long lda,
+                  const double *__restrict__ B, long ldb, double beta, double *__restrict__ C,
+                  long ldc, int tri) {
+  extern __shared__ __align__(16) double smem[];
+  const int tiles_m = (M + BM - 1) / BM, tiles_n = (N + BN - 1) / BN;
+  // grouped rasterisation: 8 tile-rows share B panels in L2
+  const int bid = blockIdx.x, G = 8;
+  const int per_group = G * tiles_n, group = bid / per_group;
+  const int first_m = group * G, gsz = min(tiles_m - first_m, G);
+  const int tm = first_m + (bid % per_group) % gsz, tn = (bid % per_group) / gsz;
+  const int m0 = tm * BM, n0 = tn * BN;
+  if (tri == 1 && m0 + BM - 1 < n0) return;
+  if (tri == 2 && m0 > n0 + BN - 1) return;
+  dgemm_tile<TA, TB, VEC>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, tri, m0, n0, smem);
+}
+
+// Grouped (batched, uneven) GEMM: a persistent grid walks the 128x128 tiles
+// of all problems; tile t belongs to problem order[p] where tile_start[p] <= t
+// < tile_start[p+1] (problems sorted by decreasing size on the host).
+template <bool TA, bool TB, int VEC>
+__global__ void __launch_bounds__(THREADS, 1)
+dgemm_grouped_kernel(const GemmProb *__restrict__ probs, const int *__restrict__ order,
+                     const int *__restrict__ tile_start, int count, int *__restrict__ next) {
+  extern __shared__ __align__(16) double smem[];
+  __shared__ int s_t;
+  const int total = tile_start[count];
+  while (true) {
+    if (threadIdx.x == 0) s_t = atomicAdd(next, 1);
+    __syncthreads();
+    const int t = s_t;
+    if (t >= total) return;
+    int lo = 0, hi = count - 1;  // last p with tile_start[p] <= t
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (tile_start[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    const GemmProb pr = probs[order[lo]];
+    const int local = t - tile_start[lo], tiles_n = (pr.N + BN - 1) / BN;
+    const int m0 = (local / tiles_n) * BM, n0 = (local % tiles_n) * BN;
+    dgemm_tile<TA, TB, VEC>(pr.M, pr.N, pr.K, pr.alpha, pr.A, pr.lda, pr.B, pr.ldb, pr.beta, pr.C,
+                            pr.ldc, 0, m0, n0, smem);
+    __syncthreads();  // shared memory is reused by the next tile
+  }
+}
+
 __global__ void scale_kernel(int M, int N, double beta, double *C, long ldc, int tri) {
   long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
   long total = (long)M * N;
@@ -241,6 +279,61 @@ void dgemm_dev(int ta, int tb, int M, int N, int K, double alpha, const double *
   else if (tA && !tB) { ATLB_DG(true, false) }
   else { ATLB_DG(true, true) }
 #undef ATLB_DG
+}
+
+namespace {
+template <bool TA, bool TB, int VEC>
+void launch_grouped(const GemmProb *probs, const int *order, const int *tile_start, int count,
+                    int *next, cudaStream_t st) {
+  constexpr int smem = STAGES * (Lay<TA>::SIZE + Lay<!TB>::SIZE) * (int)sizeof(double);
+  static bool configured = false;
+  if (!configured) {
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(dgemm_grouped_kernel<TA, TB, VEC>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    configured = true;
+  }
+  dgemm_grouped_kernel<TA, TB, VEC><<<num_sms(), THREADS, smem, st>>>(probs, order, tile_start, count, next);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
+
+}  // namespace
+
+void dgemm_grouped_dev(int ta, int tb, const GemmProb *hp, int count, cudaStream_t st) {
+  if (count <= 0) return;
+  std::vector<int> order(count);
+  for (int i = 0; i < count; i++) order[i] = i;
+  auto work = [&](int i) { return (long)hp[i].M * hp[i].N * hp[i].K; };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work(a) > work(b); });
+  std::vector<int> ts(count + 1, 0);
+  bool v2 = true;
+  for (int i = 0; i < count; i++) {
+    const GemmProb &p = hp[order[i]];
+    ts[i + 1] = ts[i] + ((p.M > 0 && p.N > 0) ? cdiv(p.M, BM) * cdiv(p.N, BN) : 0);
+    v2 = v2 && al16(p.A, p.lda) && al16(p.B, p.ldb);
+  }
+  const size_t bytes = sizeof(GemmProb) * count + sizeof(int) * (2 * count + 1 + 16);
+  unsigned char *d = (unsigned char *)scratch(kSlotBatch3, bytes);
+  unsigned char *h = (unsigned char *)pinned(kSlotBatch3, bytes);
+  memcpy(h, hp, sizeof(GemmProb) * count);
+  memcpy(h + sizeof(GemmProb) * count, order.data(), sizeof(int) * count);
+  memcpy(h + sizeof(GemmProb) * count + sizeof(int) * count, ts.data(), sizeof(int) * (count + 1));
+  memset(h + sizeof(GemmProb) * count + sizeof(int) * (2 * count + 1), 0, sizeof(int) * 16);
+  ATLB_CUDA_CHECK(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st));
+  const GemmProb *dp = (const GemmProb *)d;
+  const int *dord = (const int *)(d + sizeof(GemmProb) * count);
+  const int *dts = dord + count;
+  int *next = (int *)(dts + count + 1);
+  const bool tA = ta != kNoTrans, tB = tb != kNoTrans;
+#define ATLB_GG(TA_, TB_)                                                     \
+  if (v2) launch_grouped<TA_, TB_, 2>(dp, dord, dts, count, next, st);       \
+  else launch_grouped<TA_, TB_, 1>(dp, dord, dts, count, next, st);
+  if (!tA && !tB) { ATLB_GG(false, false) }
+  else if (!tA && tB) { ATLB_GG(false, true) }
+  else if (tA && !tB) { ATLB_GG(true, false) }
+  else { ATLB_GG(true, true) }
+#undef ATLB_GG
+  // the host staging buffer must outlive the copy: wait for it here
+  ATLB_CUDA_CHECK(cudaStreamSynchronize(st));
 }
 
 }  // namespace atlb

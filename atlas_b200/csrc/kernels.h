@@ -14,6 +14,17 @@ void sgemm_dev(int ta, int tb, int M, int N, int K, float alpha, const float *A,
                const float *B, long ldb, float beta, float *C, long ldc, cudaStream_t st,
                int tri = 0);
 
+// One problem of a grouped (batched, uneven) DGEMM: C = alpha*op(A)*op(B) + beta*C.
+struct GemmProb {
+  const double *A, *B;
+  double *C;
+  int M, N, K;
+  long lda, ldb, ldc;
+  double alpha, beta;
+};
+// All problems share TransA / TransB; device pointers; one persistent launch.
+void dgemm_grouped_dev(int ta, int tb, const GemmProb *hprobs, int count, cudaStream_t st);
+
 // A FP32 GEMM entry with the sgemm_dev signature; the mixed-precision LU and
 // Cholesky take one of these for their trailing updates.
 typedef void (*SgemmFn)(int ta, int tb, int M, int N, int K, float alpha, const float *A,
@@ -43,6 +54,11 @@ void gemm_dev(int ta, int tb, int M, int N, int K, T alpha, const T *A, long lda
 template <typename T>
 void trsm_dev(int side, int uplo, int trans, int diag, int M, int N, T alpha, const T *A, long lda,
               T *B, long ldb, cudaStream_t st, SgemmFn gemm = nullptr);
+// The TRSM with its workspace supplied: W holds ceil(n/64) blocks of 64x64
+// elements (n = order of the triangle).
+template <typename T>
+void trsm_impl(int side, int uplo, int trans, int diag, int M, int N, T alpha, const T *A, long lda,
+               T *B, long ldb, cudaStream_t st, SgemmFn gemm, T *W);
 // Inverses of the 64x64 diagonal blocks of the triangle T(i,k) = Tp[i*tr + k*tc]
 // (n x n), block b stored dense 64x64 column-major at W + b*4096.
 template <typename T>

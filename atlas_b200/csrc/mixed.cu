@@ -117,9 +117,11 @@ __global__ void resid_finish_kernel(int N, int nrhs, int nchunks, const double *
     for (int ch = 0; ch < nchunks; ch++) s += part[((long)ch * nrhs + r) * N + i];
     const double b = B[i + (long)r * ldb];
     const double v = b - s;
+    const double xv = X[i + (long)r * ldx];
     R[i + (long)r * ldr] = v;
-    mr = fmax(mr, fabs(v));
-    mx = fmax(mx, fabs(X[i + (long)r * ldx]));
+    // NaN must not vanish in the maximum (fmax drops it): count it as infinite
+    mr = fmax(mr, v == v ? fabs(v) : INFINITY);
+    mx = fmax(mx, xv == xv ? fabs(xv) : INFINITY);
     mb = fmax(mb, fabs(b));
   }
   for (int o = 16; o; o >>= 1) {
@@ -156,6 +158,12 @@ __global__ void symmetrize_kernel(int uplo, int N, const double *__restrict__ A,
     bool stored = (uplo == kLower) ? (i >= j) : (i <= j);
     F[i + (long)j * ldf] = stored ? A[i + (long)j * lda] : A[j + (long)i * lda];
   }
+}
+
+bool debug_ir() {
+  static int v = -1;
+  if (v < 0) { const char *e = getenv("ATLAS_B200_DEBUG_IR"); v = (e && *e && *e != '0') ? 1 : 0; }
+  return v == 1;
 }
 
 inline int grid_for(long total) { return (int)std::min<long>((total + 255) / 256, 148L * 8); }
@@ -260,6 +268,7 @@ int refine(int N, int nrhs, const double *A, long lda, const double *B, long ldb
         worst = std::max(worst, std::isfinite(eta) ? eta : 1e300);
       }
       if (stats) { stats->bwd_err = worst; stats->anrm = anrm; }
+      if (debug_ir()) fprintf(stderr, "atlas_b200 refine: iter %d backward error %.3e (target %.3e)\n", it, worst, tol);
       if (ok) {
         *iter = it;
         return 0;

@@ -37,44 +37,55 @@ constexpr int LEAF = 64;
 // block, one thread per column of the inverse (forward / backward
 // substitution against the identity, the column held in registers).
 template <typename T>
-__global__ void __launch_bounds__(LEAF)
+__global__ void __launch_bounds__(4 * LEAF)
 trinv_kernel(int n, const T *__restrict__ Tp, long tr, long tc, int lower, int unit, T *__restrict__ W) {
   extern __shared__ __align__(16) unsigned char trinv_smem[];
   T(*sT)[LEAF + 1] = reinterpret_cast<T(*)[LEAF + 1]>(trinv_smem);
-  T(*sW)[LEAF + 1] = sT + LEAF;  // column j of the inverse is owned by thread j
-  const int b = blockIdx.x, r0 = b * LEAF, nb = min(LEAF, n - r0), j = threadIdx.x;
+  T(*sW)[LEAF + 1] = sT + LEAF;
+  // four threads (consecutive lanes of one warp) per column of the inverse:
+  // column j = tid / 4, the substitution's inner loop split over i mod 4
+  const int b = blockIdx.x, r0 = b * LEAF, nb = min(LEAF, n - r0), tid = threadIdx.x;
+  const int j = tid >> 2, part = tid & 3;
   const T *Tb = Tp + r0 * tr + r0 * tc;
-  for (int idx = j; idx < LEAF * LEAF; idx += LEAF) {
+  for (int idx = tid; idx < LEAF * LEAF; idx += 4 * LEAF) {
     int i, k;
     if (tr == 1) { i = idx % LEAF; k = idx / LEAF; } else { k = idx % LEAF; i = idx / LEAF; }
     sT[i][k] = (i < nb && k < nb) ? Tb[i * tr + k * tc] : T(0);
     sW[i][k] = (i == k) ? T(1) : T(0);
   }
   __syncthreads();
-  if (j < nb) {
-    if (lower) {
+  const bool active = j < nb;
+  // every lane of a warp runs the same k range (the warp's 8 columns start at
+  // j0 = 8 * warp); for k outside a column's own range the update is zero
+  const int j0 = (tid >> 5) * 8;
+  if (lower) {
 #pragma unroll 1
-      for (int k = j; k < nb; k++) {
-        T xk = sW[k][j];
-        if (!unit) xk = xk / sT[k][k];
-        sW[k][j] = xk;
-#pragma unroll 4
-        for (int i = k + 1; i < nb; i++) sW[i][j] -= sT[i][k] * xk;
-      }
-    } else {
+    for (int k = j0; k < nb; k++) {
+      const bool on = active && k >= j;
+      T xk = sW[k][j];
+      if (!unit && on) xk = xk / sT[k][k];
+      __syncwarp();
+      if (part == 0 && on) sW[k][j] = xk;
+      if (on)
+        for (int i = k + 1 + part; i < nb; i += 4) sW[i][j] -= sT[i][k] * xk;
+      __syncwarp();
+    }
+  } else {
 #pragma unroll 1
-      for (int k = j; k >= 0; k--) {
-        T xk = sW[k][j];
-        if (!unit) xk = xk / sT[k][k];
-        sW[k][j] = xk;
-#pragma unroll 4
-        for (int i = 0; i < k; i++) sW[i][j] -= sT[i][k] * xk;
-      }
+    for (int k = min(j0 + 7, nb - 1); k >= 0; k--) {
+      const bool on = active && k <= j;
+      T xk = sW[k][j];
+      if (!unit && on) xk = xk / sT[k][k];
+      __syncwarp();
+      if (part == 0 && on) sW[k][j] = xk;
+      if (on)
+        for (int i = part; i < k; i += 4) sW[i][j] -= sT[i][k] * xk;
+      __syncwarp();
     }
   }
   __syncthreads();
   T *Wb = W + (long)b * LEAF * LEAF;
-  for (int idx = j; idx < LEAF * LEAF; idx += LEAF) Wb[idx] = sW[idx % LEAF][idx / LEAF];
+  for (int idx = tid; idx < LEAF * LEAF; idx += 4 * LEAF) Wb[idx] = sW[idx % LEAF][idx / LEAF];
 }
 
 // B_blk (nb x m, effective strides) = W_b (nb x nb) * B_blk, in place: one
@@ -338,7 +349,7 @@ void trinv_dev(int n, const T *Tp, long tr, long tc, int lower, int unit, T *W, 
     ATLB_CUDA_CHECK(cudaFuncSetAttribute(trinv_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     configured = true;
   }
-  trinv_kernel<T><<<cdiv(n, LEAF), LEAF, smem, st>>>(n, Tp, tr, tc, lower, unit, W);
+  trinv_kernel<T><<<cdiv(n, LEAF), 4 * LEAF, smem, st>>>(n, Tp, tr, tc, lower, unit, W);
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
 template void trinv_dev<double>(int, const double *, long, long, int, int, double *, cudaStream_t);
@@ -380,6 +391,9 @@ void trsm_impl(int side, int uplo, int trans, int diag, int M, int N, T alpha, c
   e.W = W;
   eff_solve(e, 0, n, m, gemm, st);
 }
+
+template void trsm_impl<double>(int, int, int, int, int, int, double, const double *, long, double *,
+                                long, cudaStream_t, SgemmFn, double *);
 
 template <typename T>
 void trsm_dev(int side, int uplo, int trans, int diag, int M, int N, T alpha, const T *A, long lda,

@@ -88,11 +88,12 @@ trsv_kernel(int n, int nrhs, const T *__restrict__ Tp, long tr, long tc, int low
   }
   __syncthreads();
   const T *Wb = W + (long)bi * BS * BS;
-  if (tid < BS * NR && tid % BS < rows) {
-    const int rr = tid % BS, q = tid / BS;
+  for (int idx = tid; idx < BS * NR; idx += 256) {
+    const int rr = idx % BS, q = idx / BS;
+    if (rr >= rows || q >= nrhs) continue;
     T v = T(0);
     for (int c = 0; c < rows; c++) v = fma(Wb[rr + (long)c * BS], sx[c][q], v);
-    if (q < nrhs) X[r0 + rr + (long)q * ldx] = v;
+    X[r0 + rr + (long)q * ldx] = v;
   }
   __threadfence();
   __syncthreads();

@@ -168,6 +168,48 @@ int atlb_dgemm_ozaki(int TransA, int TransB, int M, int N, int K, double alpha, 
                      int lda, const double *B, int ldb, double beta, double *C, int ldc,
                      int slices);
 
+/* Batched, uneven-size problems (no counterpart in the reference).  All
+ * pointers inside the arrays are DEVICE pointers; the arrays themselves are
+ * host arrays of `count` entries.  Each batch runs as one persistent launch
+ * whose CTAs take work (problems, or GEMM tiles) largest first from an atomic
+ * counter.  Column-major; returns 0 or -(bad argument).
+ *   atlb_dgemm_batched_dev: C[i] = alpha*op(A[i])*op(B[i]) + beta*C[i]; returns
+ *     after the launch is enqueued (asynchronous on the library stream).
+ *   atlb_dposv_batched: Cholesky (lower triangle) + solve of nrhs[i] right-hand
+ *     sides, orders up to 256; info[i] (host) = potrf info; synchronous.
+ *   atlb_dgesv_batched: LU with partial pivoting (ipiv[i]: device, 0-based) and,
+ *     when B is not NULL, the solve; orders up to 256; synchronous. */
+int atlb_dgemm_batched_dev(int TransA, int TransB, int count, const int *M, const int *N,
+                           const int *K, double alpha, const double *const *A, const int *lda,
+                           const double *const *B, const int *ldb, double beta, double *const *C,
+                           const int *ldc);
+int atlb_dposv_batched(int count, const int *n, double *const *A, const int *lda, double *const *B,
+                       const int *ldb, const int *nrhs, int *info);
+int atlb_dgesv_batched(int count, const int *n, double *const *A, const int *lda, int *const *ipiv,
+                       double *const *B, const int *ldb, const int *nrhs, int *info);
+
+/* Adjoints (reverse-mode derivatives) of the factorizations and solves, for
+ * gradient-based callers; no counterpart in the reference.  Device pointers,
+ * column-major, asynchronous on the library stream; return 0 or -(bad arg).
+ *   atlb_dpotrf_adjoint_dev: A = L L^T (L lower): Abar = (S + S^T)/2 with
+ *     S = L^-T Phi(L^T Lbar) L^-1 (Phi: lower triangle, diagonal halved).
+ *   atlb_dpotrs_adjoint_dev: X = A^-1 B with A = L L^T: Bbar = A^-1 Xbar and
+ *     Abar -= (Bbar X^T + X Bbar^T)/2 (accumulates into Abar).
+ *   atlb_dgetrs_adjoint_dev: X = A^-1 B with the getrf factors: Bbar = A^-T Xbar
+ *     and Abar -= Bbar X^T (accumulates).
+ *   atlb_dgetrf_adjoint_dev: A = P L U: Abar = P L^-T (stril(L^T Lbar) +
+ *     triu(Ubar U^T)) U^-T (overwrites Abar). */
+int atlb_dpotrf_adjoint_dev(int N, const double *L, int ldl, const double *Lbar, int ldlb,
+                            double *Abar, int ldab);
+int atlb_dpotrs_adjoint_dev(int N, int NRHS, const double *L, int ldl, const double *X, int ldx,
+                            const double *Xbar, int ldxb, double *Bbar, int ldbb, double *Abar,
+                            int ldab);
+int atlb_dgetrs_adjoint_dev(int N, int NRHS, const double *LU, int ldlu, const int *ipiv,
+                            const double *X, int ldx, const double *Xbar, int ldxb, double *Bbar,
+                            int ldbb, double *Abar, int ldab);
+int atlb_dgetrf_adjoint_dev(int N, const double *LU, int ldlu, const int *ipiv, const double *Lbar,
+                            int ldlb, const double *Ubar, int ldub, double *Abar, int ldab);
+
 #ifdef __cplusplus
 }
 #endif
