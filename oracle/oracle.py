@@ -99,7 +99,12 @@ def ref():
 
 
 def P(a):
-    return None if a is None else a.ctypes.data
+    """Address of a column-major array (a C-ordered 2-D array would be read transposed)."""
+    if a is None:
+        return None
+    if a.ndim == 2 and a.shape[1] > 1 and not a.flags.f_contiguous:
+        raise ValueError("oracle arrays are column-major: pass np.asfortranarray(...)")
+    return a.ctypes.data
 
 
 # ---------------------------------------------------------------- generators

@@ -50,6 +50,12 @@ def atl():
 
 @pytest.fixture(scope="session")
 def gpu(atl):
-    """The library on a GPU (device 0)."""
+    """The library on a GPU (device 0), sharing one stream with torch: the
+    tensors a test creates are ordered before the library's kernels that read
+    them (the library's own stream would not wait for torch's)."""
+    import torch
     assert atl.atlb_init(0) == 0
+    s = torch.cuda.Stream(device=0)
+    torch.cuda.set_stream(s)
+    atl.atlb_set_stream(s.cuda_stream)
     return atl

@@ -85,7 +85,8 @@ def test_batched_gesv_matches_oracle(gpu, orc):
         np.testing.assert_array_equal(Ps[i].cpu().numpy(), rpiv)
         assert np.max(np.abs(As[i].cpu().numpy().T - lu)) < 1e-10
         x = Bs[i].cpu().numpy().T
-        assert orc.resid_slv(a0s[i], np.asfortranarray(x), np.linalg.solve(a0s[i], b0s[i])) <= 100
+        xt = np.asfortranarray(np.linalg.solve(a0s[i], b0s[i]))   # the oracle reads column-major
+        assert orc.resid_slv(a0s[i], np.asfortranarray(x), xt) <= 100
 
 
 def test_batched_dgemm_uneven(gpu, orc):
