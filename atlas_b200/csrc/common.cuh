@@ -4,6 +4,8 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <functional>
+#include <vector>
 
 #define ATLB_CUDA_CHECK(expr)                                                  \
   do {                                                                         \
@@ -33,15 +35,34 @@ int num_sms();
 // so the hot path performs no cudaMalloc once warm.
 void *scratch(int slot, size_t bytes);
 void *pinned(int slot, size_t bytes);
+// A second, high-priority stream per host thread for work that runs beside
+// the main stream (look-ahead panels).  While a SideScope is alive on a
+// thread, scratch() and pinned() hand out a second set of buffers, so work
+// enqueued on the two streams never shares a workspace.
+cudaStream_t side_stream();
+cudaEvent_t side_event(int i);  // four reusable events per thread (i < 4)
+struct SideScope {
+  SideScope();
+  ~SideScope();
+};
 enum ScratchSlot {
   kSlotA = 0, kSlotB, kSlotC, kSlotIpiv, kSlotTau, kSlotWork, kSlotWork2,
   kSlotInfo, kSlotMixedA, kSlotMixedR, kSlotMixedX, kSlotMixedD,
   kSlotOzA, kSlotOzB, kSlotOzScale, kSlotBatch0, kSlotBatch1, kSlotBatch2,
   kSlotBatch3, kSlotAdj0, kSlotAdj1, kSlotAdj2, kSlotTc0, kSlotTc1, kSlotTrsmW, kSlotTrsvCtl, kSlotLaswp,
+  kSlotMixedWL, kSlotMixedWU, kSlotMixedPerm,
   kNumSlots
 };
 
 inline int cdiv(long a, long b) { return (int)((a + b - 1) / b); }
+
+// Replay cache for launch sequences that depend only on their arguments
+// (sizes, pointers, stream): the first call with a key runs `enqueue`
+// eagerly (sizing every workspace), the second captures it into a CUDA graph,
+// later calls launch the graph.  A workspace that moves invalidates the
+// cached graphs; ATLAS_B200_GRAPHS=0 turns the cache off.
+void run_graph(const std::vector<unsigned long long> &key, cudaStream_t st,
+               const std::function<void()> &enqueue);
 
 }  // namespace atlb
 

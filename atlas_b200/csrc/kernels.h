@@ -67,6 +67,15 @@ void trinv_dev(int n, const T *Tp, long tr, long tc, int lower, int unit, T *W, 
 template <typename T>
 void trsv_dev(int uplo, int trans, int diag, int n, int nrhs, const T *A, long lda, T *B, long ldb,
               cudaStream_t st);
+template <typename T>
+void trsv_inverse_dev(int uplo, int trans, int diag, int n, const T *A, long lda, T *W, cudaStream_t st);
+template <typename T>
+void trsv_w_dev(int uplo, int trans, int n, int nrhs, const T *A, long lda, const T *W, T *B, long ldb,
+                cudaStream_t st);
+// net row permutation of ipiv[0..n) applied forward: row i of P*B is row perm[i] of B
+void ipiv_to_perm_dev(int n, const int *ipiv, int *perm, cudaStream_t st);
+// depth-one look-ahead in the blocked factorizations (ATLAS_B200_LOOKAHEAD=0 turns it off)
+bool lookahead_enabled();
 
 // B = alpha*op(A)*B (Left) or alpha*B*op(A) (Right), A triangular.
 void dtrmm_dev(int side, int uplo, int trans, int diag, int M, int N, double alpha,

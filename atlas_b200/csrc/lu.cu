@@ -15,8 +15,11 @@
 // panel: each row carries its current position and the final permutation is
 // applied when the rows are written back.
 #include <algorithm>
+#include <vector>
 #include <cfloat>
 #include <climits>
+#include <cstdlib>
+#include <cstring>
 #include <cooperative_groups.h>
 #include "common.cuh"
 #include "kernels.h"
@@ -185,6 +188,163 @@ getf2_cluster_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restr
   cl.sync();  // keep this CTA's shared memory alive until every peer is done
 }
 
+// Panel kernel for up to 32 columns and up to 512 rows per CTA (one row per
+// thread), organised so that a column costs one CTA barrier and one cluster
+// barrier and no runtime-indexed register access:
+//   * each thread keeps its row SHIFTED: a[0] always holds the current
+//     column, so the rank-1 update of column j is a[k-1] = a[k] - l * u[k]
+//     over fixed register indices (the shift is free: each FMA writes the
+//     register the previous column just vacated);
+//   * the finished part of each row goes to shared memory (L multipliers as
+//     they are produced; the U part of a pivot row when it is chosen) and is
+//     written to its final row position at the end;
+//   * per column: warp arg-max -> CTA arg-max (one __syncthreads); the CTA's
+//     winner publishes (|value|, position, row) in its shared memory; one
+//     cluster barrier; every warp then reads the C candidates over
+//     distributed shared memory (one load per lane), reduces them to the
+//     same global winner, and fetches that row (one load per lane) into a
+//     per-warp buffer from which all lanes read the update row.
+// Pivot order: largest |value|, lowest current row position on ties (the
+// first maximum, like cblas_idamax); a NaN entry ranks below every number.
+template <typename T, int NB>
+struct ShiftPub {
+  T row[NB];
+  T val;
+  int pos;
+};
+
+template <typename T>
+__device__ __forceinline__ void argmax_step(T &v, int &p, int &w, int o) {
+  const T ov = __shfl_xor_sync(0xffffffffu, v, o);
+  const int op = __shfl_xor_sync(0xffffffffu, p, o);
+  const int ow = __shfl_xor_sync(0xffffffffu, w, o);
+  if (ov > v || (ov == v && op < p)) { v = ov; p = op; w = ow; }
+}
+
+__device__ __forceinline__ void cluster_arrive() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait() {
+  asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
+template <typename T, int NB>
+__global__ void __launch_bounds__(PT, 1)
+getf2_shift_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restrict__ ipiv,
+                   int roff, int *__restrict__ dinfo) {
+  static_assert(NB == 32, "one pivot-row element per lane");
+  cg::cluster_group cl = cg::this_cluster();
+  const int C = (int)cl.num_blocks(), crank = (int)cl.block_rank();
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int MN = min(M, ncols);
+  extern __shared__ __align__(16) unsigned char shift_smem[];
+  T *Lsm = reinterpret_cast<T *>(shift_smem);  // [NB][PT]: finished row parts
+  __shared__ ShiftPub<T, NB> pub[2];
+  __shared__ __align__(16) T wu[PT / 32][NB];  // per-warp copy of the pivot row
+  __shared__ T wv[PT / 32];
+  __shared__ int wp[PT / 32];
+  __shared__ T zrow[NB];
+  if (tid < NB) zrow[tid] = T(0);  // ordered before its first use by publish's barriers
+
+  const int r = crank * PT + tid;
+  bool act = r < M;
+  int pos = r;
+  T a[NB];
+  {
+    const T *src = A + (act ? r : 0);
+#pragma unroll
+    for (int k = 0; k < NB; k++) {
+      a[k] = (act && k < ncols) ? __ldg(src) : T(0);
+      if (k + 1 < ncols) src += lda;
+    }
+  }
+
+  // CTA-level candidate for the current column (a[0]); publishes into pub[b]
+  auto publish = [&](int b) {
+    T v = T(-1);
+    int p = INT_MAX, w = 0;
+    if (act) {
+      const T t = fabs(a[0]);
+      v = t >= T(0) ? t : T(-0.5);  // NaN ranks below every number
+      p = pos;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) argmax_step(v, p, w, o);
+    if (lane == 0) { wv[warp] = v; wp[warp] = p; }
+    __syncthreads();
+    v = lane < PT / 32 ? wv[lane] : T(-1);
+    p = lane < PT / 32 ? wp[lane] : INT_MAX;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) argmax_step(v, p, w, o);
+    if (tid == 0) { pub[b].val = v; pub[b].pos = p; }
+    if (act && pos == p) {
+#pragma unroll
+      for (int k = 0; k < NB; k++) pub[b].row[k] = a[k];
+    }
+    __syncwarp();
+    cluster_arrive();
+    cluster_wait();
+  };
+
+  if (MN > 0) publish(0);
+#pragma unroll 1
+  for (int j = 0; j < MN; j++) {
+    const int b = j & 1;
+    // every warp reduces the C published candidates to the same winner
+    T v = T(-1);
+    int p = INT_MAX, w = 0;
+    if (lane < C) {
+      const ShiftPub<T, NB> *rp = cl.map_shared_rank(&pub[b], lane);
+      v = rp->val;
+      p = rp->pos;
+      w = lane;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) argmax_step(v, p, w, o);
+    {
+      const ShiftPub<T, NB> *rp = cl.map_shared_rank(&pub[b], w);
+      wu[warp][lane] = rp->row[lane];
+    }
+    __syncwarp();
+    const T piv = wu[warp][0];
+    if (crank == 0 && tid == 0) {
+      ipiv[j] = roff + p;
+      if (piv == T(0)) atomicMin(dinfo, roff + j + 1);
+    }
+    if (act) {
+      if (pos == p) {  // this row becomes row j of U: its remaining part is final
+        act = false;
+        pos = j;
+        T *dst = Lsm + j * PT + tid;
+#pragma unroll
+        for (int k = 0; k < NB; k++)
+          if (j + k < ncols) dst[k * PT] = a[k];
+      } else {
+        if (pos == j) pos = p;  // the row displaced by the interchange
+        // a zero pivot leaves the column unscaled and the row unchanged: the
+        // update then runs with l = 0 against a zero row (exact: a - 0*0 = a)
+        const bool nz = piv != T(0);
+        const T l = !nz ? a[0] : (fabs(piv) >= safmin<T>() ? a[0] * (T(1) / piv) : a[0] / piv);
+        const T lm = nz ? l : T(0);
+        const T *u = nz ? wu[warp] : zrow;
+        Lsm[j * PT + tid] = l;
+#pragma unroll
+        for (int k = 1; k < NB; k++) a[k - 1] = fma(-lm, u[k], a[k]);
+        a[NB - 1] = T(0);
+      }
+    }
+    if (j + 1 < MN) publish(b ^ 1);
+  }
+
+  if (r < M) {
+#pragma unroll 4
+    for (int k = 0; k < ncols; k++) A[pos + (long)k * lda] = Lsm[k * PT + tid];
+  }
+  __syncwarp();
+  cluster_arrive();  // peers may still be reading this CTA's last candidate
+  cluster_wait();
+}
+
 // Fallback for panels taller than a cluster can hold: one CTA, global memory.
 template <typename T>
 __global__ void __launch_bounds__(1024)
@@ -297,6 +457,73 @@ void init_max_cluster() {
   g_max_cluster = n > 0 ? 16 : 8;
 }
 
+template <typename T>
+constexpr int shift_smem_bytes() { return 32 * PT * (int)sizeof(T); }
+
+// Largest cluster of the shift kernel (<= 16 CTAs, ~130 KB shared memory
+// each) the device can co-schedule; 0 when none.
+template <typename T>
+int max_cluster_shift() {
+  static int cached = -1;
+  if (cached >= 0) return cached;
+  auto kern = getf2_shift_kernel<T, 32>;
+  cached = 0;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, shift_smem_bytes<T>()) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    return cached;
+  }
+  for (int c : {16, 8}) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(c, 1, 1);
+    cfg.blockDim = dim3(PT, 1, 1);
+    cfg.dynamicSmemBytes = shift_smem_bytes<T>();
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = c;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess) { cudaGetLastError(); n = 0; }
+    if (n > 0) { cached = c; break; }
+  }
+  return cached;
+}
+
+template <typename T>
+bool launch_shift_panel(int M, int ncols, T *A, long lda, int *ipiv, int roff, int *dinfo,
+                        cudaStream_t st) {
+  if (ncols > 32) return false;
+  const int C = cdiv(M, PT);
+  if (C > max_cluster_shift<T>()) return false;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(C, 1, 1);
+  cfg.blockDim = dim3(PT, 1, 1);
+  cfg.dynamicSmemBytes = shift_smem_bytes<T>();
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  ATLB_CUDA_CHECK(cudaLaunchKernelEx(&cfg, getf2_shift_kernel<T, 32>, M, ncols, A, lda, ipiv, roff, dinfo));
+  return true;
+}
+
+bool shift_panel_disabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = getenv("ATLAS_B200_PANEL");
+    v = (e && strcmp(e, "cluster") == 0) ? 1 : 0;
+  }
+  return v == 1;
+}
+
 // Panel width the cluster kernel supports for M rows.
 int panel_nb(int M) {
   init_max_cluster();
@@ -308,7 +535,8 @@ int panel_nb(int M) {
 
 template <typename T>
 void panel(int M, int ncols, T *A, long lda, int *ipiv, int roff, int *dinfo, cudaStream_t st) {
-  bool ok = false;
+  bool ok = !shift_panel_disabled() && launch_shift_panel<T>(M, ncols, A, lda, ipiv, roff, dinfo, st);
+  if (ok) return;
   if (ncols <= 32 && M <= g_max_cluster * PT) ok = launch_cluster_panel<T, 32, 1>(M, ncols, A, lda, ipiv, roff, dinfo, st);
   else if (ncols <= 16 && M <= g_max_cluster * PT * 2) ok = launch_cluster_panel<T, 16, 2>(M, ncols, A, lda, ipiv, roff, dinfo, st);
   else if (ncols <= 8 && M <= g_max_cluster * PT * 4) ok = launch_cluster_panel<T, 8, 4>(M, ncols, A, lda, ipiv, roff, dinfo, st);
@@ -357,6 +585,15 @@ void getrf_rec(int off, int M, int N, T *A, long lda, int *ipiv, int *dinfo, cud
 
 }  // namespace
 
+bool lookahead_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = getenv("ATLAS_B200_LOOKAHEAD");
+    v = (e && e[0] == '0') ? 0 : 1;
+  }
+  return v == 1;
+}
+
 // Outer loop: NBO-column block panels, each factored by the recursion above
 // (restricted to the panel's columns); the panel's row interchanges are then
 // applied to the columns on both sides and the trailing matrix is updated with
@@ -367,22 +604,66 @@ constexpr int NBO = 256;
 template <typename T>
 void getrf_dev(int M, int N, T *A, long lda, int *ipiv, int *dinfo, cudaStream_t st,
                SgemmFn gemm) {
-  set_info_kernel_launch(dinfo, st);
-  const int MN = std::min(M, N);
-  for (int j = 0; j < MN; j += NBO) {
-    const int jb = std::min(NBO, MN - j);
-    T *Ad = A + j + (long)j * lda;
-    getrf_rec<T>(j, M - j, jb, A, lda, ipiv, dinfo, st, gemm);   // panel: rows j.., columns j..j+jb
-    if (j > 0) laswp_dev<T>(j, A, lda, j, j + jb, ipiv, 1, st);  // left of the panel
-    const int nr = N - j - jb;
-    if (nr > 0) {
-      T *A12 = Ad + (long)jb * lda;
-      laswp_dev<T>(nr, A + (long)(j + jb) * lda, lda, j, j + jb, ipiv, 1, st);
-      trsm_dev<T>(kLeft, kLower, kNoTrans, kUnit, jb, nr, T(1), Ad, lda, A12, lda, st, gemm);
-      if (M - j - jb > 0) update_gemm(gemm, M - j - jb, nr, jb, Ad + jb, A12, A12 + jb, lda, st);
+  // the launch sequence depends only on (M, N, lda, pointers): replayed as a graph
+  const std::vector<unsigned long long> key = {1ull + sizeof(T), (unsigned long long)M,
+      (unsigned long long)N, (unsigned long long)lda, (unsigned long long)(uintptr_t)A,
+      (unsigned long long)(uintptr_t)ipiv, (unsigned long long)(uintptr_t)dinfo,
+      (unsigned long long)(uintptr_t)gemm, (unsigned long long)(uintptr_t)st};
+  run_graph(key, st, [&]() {
+    set_info_kernel_launch(dinfo, st);
+    const int MN = std::min(M, N), nblk = cdiv(MN, NBO);
+    if (nblk <= 1 || !lookahead_enabled()) {
+      for (int j = 0; j < MN; j += NBO) {
+        const int jb = std::min(NBO, MN - j);
+        T *Ad = A + j + (long)j * lda;
+        getrf_rec<T>(j, M - j, jb, A, lda, ipiv, dinfo, st, gemm);   // panel: rows j.., columns j..j+jb
+        if (j > 0) laswp_dev<T>(j, A, lda, j, j + jb, ipiv, 1, st);  // left of the panel
+        const int nr = N - j - jb;
+        if (nr > 0) {
+          T *A12 = Ad + (long)jb * lda;
+          laswp_dev<T>(nr, A + (long)(j + jb) * lda, lda, j, j + jb, ipiv, 1, st);
+          trsm_dev<T>(kLeft, kLower, kNoTrans, kUnit, jb, nr, T(1), Ad, lda, A12, lda, st, gemm);
+          if (M - j - jb > 0) update_gemm(gemm, M - j - jb, nr, jb, Ad + jb, A12, A12 + jb, lda, st);
+        }
+      }
+    } else {
+      // Look-ahead of depth one: while the main stream applies block k to
+      // the trailing matrix, the side stream (higher priority) first applies
+      // block k to the next block column only and then factors it, so the
+      // latency-bound panel runs under the bandwidth/tensor-bound update.
+      // Writes of the two streams never overlap: the side stream owns the
+      // next block column, the main stream everything to its right and the
+      // interchanges on the left.
+      cudaStream_t s1 = side_stream();
+      getrf_rec<T>(0, M, std::min(NBO, MN), A, lda, ipiv, dinfo, st, gemm);
+      for (int k = 0; k < nblk; k++) {
+        const int j = k * NBO, jb = std::min(NBO, MN - j), jn = j + jb;
+        const int jbn = k + 1 < nblk ? std::min(NBO, MN - jn) : 0;
+        T *Ad = A + j + (long)j * lda;
+        if (k > 0) ATLB_CUDA_CHECK(cudaStreamWaitEvent(st, side_event(2 + (k & 1)), 0));  // block k factored
+        if (jbn > 0) {
+          ATLB_CUDA_CHECK(cudaEventRecord(side_event(k & 1), st));  // updates by blocks < k are in
+          ATLB_CUDA_CHECK(cudaStreamWaitEvent(s1, side_event(k & 1), 0));
+          SideScope side;
+          T *An = A + (long)jn * lda;
+          laswp_dev<T>(jbn, An, lda, j, jn, ipiv, 1, s1);
+          trsm_dev<T>(kLeft, kLower, kNoTrans, kUnit, jb, jbn, T(1), Ad, lda, An + j, lda, s1, gemm);
+          if (M - jn > 0) update_gemm(gemm, M - jn, jbn, jb, Ad + jb, An + j, An + jn, lda, s1);
+          getrf_rec<T>(jn, M - jn, jbn, A, lda, ipiv, dinfo, s1, gemm);
+          ATLB_CUDA_CHECK(cudaEventRecord(side_event(2 + ((k + 1) & 1)), s1));
+        }
+        if (j > 0) laswp_dev<T>(j, A, lda, j, jn, ipiv, 1, st);
+        const int c0 = jn + jbn, nr = N - c0;
+        if (nr > 0) {
+          T *Ar = A + (long)c0 * lda;
+          laswp_dev<T>(nr, Ar, lda, j, jn, ipiv, 1, st);
+          trsm_dev<T>(kLeft, kLower, kNoTrans, kUnit, jb, nr, T(1), Ad, lda, Ar + j, lda, st, gemm);
+          if (M - jn > 0) update_gemm(gemm, M - jn, nr, jb, Ad + jb, Ar + j, Ar + jn, lda, st);
+        }
+      }
     }
-  }
-  finish_info_kernel_launch(dinfo, st);
+    finish_info_kernel_launch(dinfo, st);
+  });
 }
 template void getrf_dev<double>(int, int, double *, long, int *, int *, cudaStream_t, SgemmFn);
 template void getrf_dev<float>(int, int, float *, long, int *, int *, cudaStream_t, SgemmFn);
@@ -432,37 +713,71 @@ namespace {
 
 constexpr int NBD = 128;
 
+// LU without pivoting of one NBD x NBD diagonal block, one CTA: thread
+// (i, g) keeps row i's columns g, g+4, ... in registers.  Each step needs
+// the pivot row and the pivot column; the threads that finish them in step
+// j-1 publish them to a double-buffered shared copy, so a step costs one
+// barrier.
 template <typename T>
 __global__ void __launch_bounds__(512)
 lu_nopiv_diag_kernel(int n, T *A, long lda, int *dinfo, int ioff) {
-  extern __shared__ __align__(16) unsigned char nopiv_smem[];
-  T(*s)[NBD + 1] = reinterpret_cast<T(*)[NBD + 1]>(nopiv_smem);
-  const int tid = threadIdx.x;
-  for (int idx = tid; idx < n * n; idx += blockDim.x) {
-    int i = idx % n, k = idx / n;
-    s[i][k] = A[i + (long)k * lda];
+  static_assert(NBD == 128, "4 threads per row, 32 columns each");
+  __shared__ T prow[2][NBD];
+  __shared__ T pcol[2][NBD];
+  const int tid = threadIdx.x, i = tid % NBD, g = tid / NBD;
+  T a[NBD / 4];
+  const long step4 = 4 * lda;
+  {
+    const T *src = A + (i < n ? i : 0) + (long)g * lda;
+#pragma unroll
+    for (int m = 0; m < NBD / 4; m++) {
+      a[m] = (i < n && g + 4 * m < n) ? src[0] : T(0);
+      src += (g + 4 * m + 4 < n) ? step4 : 0;
+    }
   }
+  if (i == 0) {
+#pragma unroll
+    for (int m = 0; m < NBD / 4; m++) prow[0][g + 4 * m] = a[m];
+  }
+  if (g == 0) pcol[0][i] = a[0];
   __syncthreads();
+#pragma unroll 1
   for (int j = 0; j < n; j++) {
-    const T p = s[j][j];
+    const int b = j & 1;
+    const T p = prow[b][j];
     if (p == T(0)) {
       if (tid == 0) atomicMin(dinfo, ioff + j + 1);
       break;  // uniform: every thread read the same pivot
     }
-    const T r = T(1) / p;
-    for (int i = j + 1 + tid; i < n; i += blockDim.x) s[i][j] *= r;
-    __syncthreads();
-    const int m = n - j - 1;
-    for (int idx = tid; idx < m * m; idx += blockDim.x) {
-      const int i = j + 1 + idx % m, k = j + 1 + idx / m;
-      s[i][k] = fma(-s[i][j], s[j][k], s[i][k]);
+    if (i > j && i < n) {
+      const T l = pcol[b][i] * (T(1) / p);
+#pragma unroll
+      for (int m = 0; m < NBD / 4; m++) {
+        const int k = g + 4 * m;
+        if (k == j) a[m] = l;
+        else if (k > j) a[m] = fma(-l, prow[b][k], a[m]);
+      }
+    }
+    if (i == j + 1) {
+#pragma unroll
+      for (int m = 0; m < NBD / 4; m++) prow[b ^ 1][g + 4 * m] = a[m];
+    }
+    if (g == ((j + 1) & 3) && i > j) {
+      T v = T(0);
+#pragma unroll
+      for (int m = 0; m < NBD / 4; m++)
+        if (g + 4 * m == j + 1) v = a[m];
+      pcol[b ^ 1][i] = v;
     }
     __syncthreads();
   }
-  __syncthreads();
-  for (int idx = tid; idx < n * n; idx += blockDim.x) {
-    int i = idx % n, k = idx / n;
-    A[i + (long)k * lda] = s[i][k];
+  if (i < n) {
+    T *dst = A + i + (long)g * lda;
+#pragma unroll
+    for (int m = 0; m < NBD / 4; m++) {
+      if (g + 4 * m < n) dst[0] = a[m];
+      dst += step4;
+    }
   }
 }
 
@@ -470,26 +785,24 @@ lu_nopiv_diag_kernel(int n, T *A, long lda, int *dinfo, int ioff) {
 
 template <typename T>
 void getrf_nopiv_dev(int N, T *A, long lda, int *dinfo, cudaStream_t st, SgemmFn gemm) {
-  set_info_kernel_launch(dinfo, st);
-  constexpr int smem = NBD * (NBD + 1) * (int)sizeof(T);
-  static bool configured = false;
-  if (!configured) {
-    ATLB_CUDA_CHECK(cudaFuncSetAttribute(lu_nopiv_diag_kernel<T>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    configured = true;
-  }
-  for (int j = 0; j < N; j += NBD) {
-    const int jb = std::min(NBD, N - j), nr = N - j - jb;
-    T *Ad = A + j + (long)j * lda;
-    lu_nopiv_diag_kernel<T><<<1, 512, smem, st>>>(jb, Ad, lda, dinfo, j);
-    ATLB_CUDA_CHECK(cudaGetLastError());
-    if (nr <= 0) break;
-    T *A21 = Ad + jb, *A12 = Ad + (long)jb * lda;
-    trsm_dev<T>(kRight, kUpper, kNoTrans, kNonUnit, nr, jb, T(1), Ad, lda, A21, lda, st, gemm);
-    trsm_dev<T>(kLeft, kLower, kNoTrans, kUnit, jb, nr, T(1), Ad, lda, A12, lda, st, gemm);
-    update_gemm(gemm, nr, nr, jb, A21, A12, A12 + jb, lda, st);
-  }
-  finish_info_kernel_launch(dinfo, st);
+  const std::vector<unsigned long long> key = {11ull + sizeof(T), (unsigned long long)N,
+      (unsigned long long)lda, (unsigned long long)(uintptr_t)A, (unsigned long long)(uintptr_t)dinfo,
+      (unsigned long long)(uintptr_t)gemm, (unsigned long long)(uintptr_t)st};
+  run_graph(key, st, [&]() {
+    set_info_kernel_launch(dinfo, st);
+    for (int j = 0; j < N; j += NBD) {
+      const int jb = std::min(NBD, N - j), nr = N - j - jb;
+      T *Ad = A + j + (long)j * lda;
+      lu_nopiv_diag_kernel<T><<<1, 512, 0, st>>>(jb, Ad, lda, dinfo, j);
+      ATLB_CUDA_CHECK(cudaGetLastError());
+      if (nr <= 0) break;
+      T *A21 = Ad + jb, *A12 = Ad + (long)jb * lda;
+      trsm_dev<T>(kRight, kUpper, kNoTrans, kNonUnit, nr, jb, T(1), Ad, lda, A21, lda, st, gemm);
+      trsm_dev<T>(kLeft, kLower, kNoTrans, kUnit, jb, nr, T(1), Ad, lda, A12, lda, st, gemm);
+      update_gemm(gemm, nr, nr, jb, A21, A12, A12 + jb, lda, st);
+    }
+    finish_info_kernel_launch(dinfo, st);
+  });
 }
 template void getrf_nopiv_dev<double>(int, double *, long, int *, cudaStream_t, SgemmFn);
 template void getrf_nopiv_dev<float>(int, float *, long, int *, cudaStream_t, SgemmFn);

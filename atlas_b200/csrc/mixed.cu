@@ -44,6 +44,17 @@ __global__ void add_s2d_kernel(int M, int N, const float *__restrict__ S, long l
   }
 }
 
+// S(i, j) = (float) R(perm[i], j): the row interchanges fused into the conversion
+__global__ void gather_d2s_kernel(int M, int N, const double *__restrict__ R, long ldr,
+                                  const int *__restrict__ perm, float *__restrict__ S, long lds) {
+  long total = (long)M * N;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    int i = (int)(idx % M), j = (int)(idx / M);
+    S[i + (long)j * lds] = (float)R[perm[i] + (long)j * ldr];
+  }
+}
+
 __global__ void s2d_kernel(int M, int N, const float *__restrict__ S, long lds, double *__restrict__ X,
                            long ldx) {
   long total = (long)M * N;
@@ -216,6 +227,11 @@ void d2s_dev(int M, int N, const double *A, long lda, float *S, long lds, cudaSt
   d2s_kernel<<<grid_for((long)M * N), 256, 0, st>>>(M, N, A, lda, S, lds);
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
+void gather_d2s_dev(int M, int N, const double *R, long ldr, const int *perm, float *S, long lds,
+                    cudaStream_t st) {
+  gather_d2s_kernel<<<grid_for((long)M * N), 256, 0, st>>>(M, N, R, ldr, perm, S, lds);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
 void s2d_dev(int M, int N, const float *S, long lds, double *X, long ldx, cudaStream_t st) {
   s2d_kernel<<<grid_for((long)M * N), 256, 0, st>>>(M, N, S, lds, X, ldx);
   ATLB_CUDA_CHECK(cudaGetLastError());
@@ -323,6 +339,13 @@ int atlb_dsgesv_ex(int N, int NRHS, double *A, int lda, int *ipiv, double *B, in
   float *S = (float *)scratch(kSlotMixedA, sizeof(float) * (size_t)lds * lds);
   float *Rs = (float *)scratch(kSlotMixedX, sizeof(float) * (size_t)lds * NRHS);
   double *rd = pivoting ? (double *)scratch(kSlotTc1, sizeof(double) * 4 * n4) : nullptr;
+  // few right-hand sides: the solves reuse the factors' inverted diagonal
+  // blocks and the net row permutation, computed once after the factorization
+  const bool few = NRHS <= 8;
+  const int nw = few ? (int)lds : 0;
+  float *WL = few ? (float *)scratch(kSlotMixedWL, sizeof(float) * (size_t)cdiv(nw, 64) * 64 * 64) : nullptr;
+  float *WU = few ? (float *)scratch(kSlotMixedWU, sizeof(float) * (size_t)cdiv(nw, 64) * 64 * 64) : nullptr;
+  int *perm = (few && !pivoting) ? (int *)scratch(kSlotMixedPerm, sizeof(int) * (size_t)N) : nullptr;
   auto factor = [&]() {
     if (pivoting) {
       rbt_init_dev(n4, rd, st);
@@ -331,20 +354,30 @@ int atlb_dsgesv_ex(int N, int NRHS, double *A, int lda, int *ipiv, double *B, in
     } else {
       d2s_dev(N, N, dA.d, dA.ld, S, lds, st);
       getrf_dev<float>(N, N, S, lds, dip, dinfo, st, g);
+      if (few) ipiv_to_perm_dev(N, dip, perm, st);
+    }
+    if (few) {
+      trsv_inverse_dev<float>(kLower, kNoTrans, kUnit, nw, S, lds, WL, st);
+      trsv_inverse_dev<float>(kUpper, kNoTrans, kNonUnit, nw, S, lds, WU, st);
     }
     return read_info(dinfo, st);
   };
   auto correct = [&](const double *R, long ldr, double *Xc, long ldxc) {
     if (pivoting) {
       rbt_left_vec_dev(N, NRHS, R, ldr, rd, Rs, st);
-      if (NRHS <= 8) {
-        trsv_dev<float>(kLower, kNoTrans, kUnit, n4, NRHS, S, lds, Rs, n4, st);
-        trsv_dev<float>(kUpper, kNoTrans, kNonUnit, n4, NRHS, S, lds, Rs, n4, st);
+      if (few) {
+        trsv_w_dev<float>(kLower, kNoTrans, n4, NRHS, S, lds, WL, Rs, n4, st);
+        trsv_w_dev<float>(kUpper, kNoTrans, n4, NRHS, S, lds, WU, Rs, n4, st);
       } else {
         trsm_dev<float>(kLeft, kLower, kNoTrans, kUnit, n4, NRHS, 1.f, S, lds, Rs, n4, st, g);
         trsm_dev<float>(kLeft, kUpper, kNoTrans, kNonUnit, n4, NRHS, 1.f, S, lds, Rs, n4, st, g);
       }
       rbt_right_add_dev(N, NRHS, Rs, rd, Xc, ldxc, st);
+    } else if (few) {
+      gather_d2s_dev(N, NRHS, R, ldr, perm, Rs, N, st);
+      trsv_w_dev<float>(kLower, kNoTrans, N, NRHS, S, lds, WL, Rs, N, st);
+      trsv_w_dev<float>(kUpper, kNoTrans, N, NRHS, S, lds, WU, Rs, N, st);
+      add_s2d_dev(N, NRHS, Rs, N, Xc, ldxc, st);
     } else {
       d2s_dev(N, NRHS, R, ldr, Rs, N, st);
       getrs_dev<float>(kNoTrans, N, NRHS, S, lds, dip, Rs, N, st, g);
@@ -406,14 +439,28 @@ int atlb_dsposv(int Uplo, int N, int NRHS, double *A, int lda, double *B, int ld
   symmetrize_dev(Uplo, N, dA.d, dA.ld, Af, N, st);
   float *S = (float *)scratch(kSlotMixedA, sizeof(float) * (size_t)N * N);
   float *Rs = (float *)scratch(kSlotMixedX, sizeof(float) * (size_t)N * NRHS);
+  const bool few = NRHS <= 8;
+  float *W1 = few ? (float *)scratch(kSlotMixedWL, sizeof(float) * (size_t)cdiv(N, 64) * 64 * 64) : nullptr;
+  float *W2 = few ? (float *)scratch(kSlotMixedWU, sizeof(float) * (size_t)cdiv(N, 64) * 64 * 64) : nullptr;
+  // A = U^T U: solve with U^T then U; A = L L^T: with L then L^T
+  const int t1 = Uplo == kUpper ? kTrans : kNoTrans, t2 = Uplo == kUpper ? kNoTrans : kTrans;
   auto factor = [&]() {
     d2s_dev(N, N, Af, N, S, N, st);
     potrf_dev<float>(Uplo, N, S, N, dinfo, st, g);
+    if (few) {
+      trsv_inverse_dev<float>(Uplo, t1, kNonUnit, N, S, N, W1, st);
+      trsv_inverse_dev<float>(Uplo, t2, kNonUnit, N, S, N, W2, st);
+    }
     return read_info(dinfo, st);
   };
   auto correct = [&](const double *R, long ldr, double *Xc, long ldxc) {
     d2s_dev(N, NRHS, R, ldr, Rs, N, st);
-    potrs_dev<float>(Uplo, N, NRHS, S, N, Rs, N, st, g);
+    if (few) {
+      trsv_w_dev<float>(Uplo, t1, N, NRHS, S, N, W1, Rs, N, st);
+      trsv_w_dev<float>(Uplo, t2, N, NRHS, S, N, W2, Rs, N, st);
+    } else {
+      potrs_dev<float>(Uplo, N, NRHS, S, N, Rs, N, st, g);
+    }
     add_s2d_dev(N, NRHS, Rs, N, Xc, ldxc, st);
   };
   bool fell_back = false;

@@ -4,7 +4,9 @@
 // error reporting.
 #include <cstring>
 #include <cstdarg>
+#include <functional>
 #include <mutex>
+#include <vector>
 #include "common.cuh"
 #include "kernels.h"
 #include "../../include/atlas_b200.h"
@@ -19,14 +21,20 @@ struct Buf {
 struct ThreadState {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
-  Buf dev[kNumSlots];
-  Buf host[kNumSlots];
+  cudaStream_t side = nullptr;
+  cudaEvent_t events[4] = {nullptr, nullptr, nullptr, nullptr};
+  Buf dev[2 * kNumSlots];   // second half: buffers of work on the side stream
+  Buf host[2 * kNumSlots];
   ~ThreadState() {
     // buffers are left to process teardown (the CUDA context may already be
     // gone when thread-local destructors run at exit)
   }
 };
 thread_local ThreadState tl;
+thread_local int tl_side = 0;                 // a SideScope is active on this thread
+thread_local bool tl_capturing = false;       // a graph capture is recording on this thread
+thread_local bool tl_capture_failed = false;  // ...and needed a workspace it could not grow
+thread_local unsigned long long tl_scratch_gen = 0;  // bumps whenever a workspace moves
 int g_device = -1;
 int g_sms = 0;
 std::mutex g_init_mu;
@@ -71,13 +79,39 @@ cudaStream_t stream() {
   return tl.stream;
 }
 
+cudaStream_t side_stream() {
+  ensure_device();
+  if (!tl.side) {
+    int least = 0, greatest = 0;
+    ATLB_CUDA_CHECK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    ATLB_CUDA_CHECK(cudaStreamCreateWithPriority(&tl.side, cudaStreamNonBlocking, greatest));
+  }
+  return tl.side;
+}
+
+cudaEvent_t side_event(int i) {
+  if (!tl.events[i]) ATLB_CUDA_CHECK(cudaEventCreateWithFlags(&tl.events[i], cudaEventDisableTiming));
+  return tl.events[i];
+}
+
+SideScope::SideScope() { tl_side = 1; }
+SideScope::~SideScope() { tl_side = 0; }
+
 void *scratch(int slot, size_t bytes) {
-  Buf &b = tl.dev[slot];
+  Buf &b = tl.dev[slot + tl_side * kNumSlots];
   if (bytes == 0) bytes = 16;
+  if (b.n < bytes && tl_capturing) {
+    // cannot allocate while recording a graph: the capture is abandoned and
+    // the work re-run eagerly (the pointer returned here is never executed)
+    tl_capture_failed = true;
+    return b.p ? b.p : (void *)tl.dev;
+  }
   if (b.n < bytes) {
+    tl_scratch_gen++;
     cudaStream_t st = stream();
     if (b.p) {
       ATLB_CUDA_CHECK(cudaStreamSynchronize(st));
+      if (tl.side) ATLB_CUDA_CHECK(cudaStreamSynchronize(tl.side));
       ATLB_CUDA_CHECK(cudaFree(b.p));
     }
     size_t n = (bytes + (1 << 20) - 1) & ~((size_t)(1 << 20) - 1);
@@ -94,12 +128,17 @@ void *scratch(int slot, size_t bytes) {
 }
 
 void *pinned(int slot, size_t bytes) {
-  Buf &b = tl.host[slot];
+  Buf &b = tl.host[slot + tl_side * kNumSlots];
   if (bytes == 0) bytes = 16;
+  if (b.n < bytes && tl_capturing) {
+    tl_capture_failed = true;
+    return b.p ? b.p : (void *)tl.host;
+  }
   if (b.n < bytes) {
     cudaStream_t st = stream();
     if (b.p) {
       ATLB_CUDA_CHECK(cudaStreamSynchronize(st));
+      if (tl.side) ATLB_CUDA_CHECK(cudaStreamSynchronize(tl.side));
       ATLB_CUDA_CHECK(cudaFreeHost(b.p));
     }
     size_t n = (bytes + (1 << 20) - 1) & ~((size_t)(1 << 20) - 1);
@@ -112,6 +151,91 @@ void *pinned(int slot, size_t bytes) {
     b.n = n;
   }
   return b.p;
+}
+
+// ---------------------------------------------------------------- graphs
+namespace {
+struct GraphEntry {
+  std::vector<unsigned long long> key;
+  cudaGraphExec_t exec;
+  unsigned long long gen;
+  unsigned long long last_use;
+};
+thread_local std::vector<GraphEntry> tl_graphs;
+thread_local std::vector<std::vector<unsigned long long>> tl_seen;
+thread_local unsigned long long tl_clock = 0;
+constexpr size_t kMaxGraphs = 24;
+
+bool graphs_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = getenv("ATLAS_B200_GRAPHS");
+    v = (e && e[0] == '0') ? 0 : 1;
+  }
+  return v == 1;
+}
+}  // namespace
+
+void run_graph(const std::vector<unsigned long long> &key, cudaStream_t st,
+               const std::function<void()> &enqueue) {
+  if (!graphs_enabled()) { enqueue(); return; }
+  tl_clock++;
+  for (auto &g : tl_graphs) {
+    if (g.key == key) {
+      if (g.gen == tl_scratch_gen) {
+        g.last_use = tl_clock;
+        ATLB_CUDA_CHECK(cudaGraphLaunch(g.exec, st));
+        return;
+      }
+      cudaGraphExecDestroy(g.exec);  // a workspace moved since the capture
+      g = tl_graphs.back();
+      tl_graphs.pop_back();
+      break;
+    }
+  }
+  bool seen = false;
+  for (auto &k : tl_seen) if (k == key) { seen = true; break; }
+  if (!seen) {  // first call: eager (sizes every workspace, sets kernel attributes)
+    if (tl_seen.size() > 64) tl_seen.erase(tl_seen.begin());
+    tl_seen.push_back(key);
+    enqueue();
+    return;
+  }
+  cudaStreamCaptureStatus cs;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+    cudaGetLastError();
+    enqueue();  // the caller is capturing already: just record into its graph
+    return;
+  }
+  cudaGraph_t graph = nullptr;
+  tl_capturing = true;
+  tl_capture_failed = false;
+  cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    enqueue();
+    e = cudaStreamEndCapture(st, &graph);
+  }
+  tl_capturing = false;
+  cudaGraphExec_t exec = nullptr;
+  if (e == cudaSuccess && !tl_capture_failed && graph)
+    e = cudaGraphInstantiate(&exec, graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  if (e != cudaSuccess || tl_capture_failed || !exec) {
+    cudaGetLastError();
+    if (exec) cudaGraphExecDestroy(exec);
+    enqueue();
+    return;
+  }
+  if (tl_graphs.size() >= kMaxGraphs) {  // evict the least recently used
+    size_t lru = 0;
+    for (size_t i = 1; i < tl_graphs.size(); i++)
+      if (tl_graphs[i].last_use < tl_graphs[lru].last_use) lru = i;
+    cudaGraphExecDestroy(tl_graphs[lru].exec);
+    tl_graphs[lru] = tl_graphs.back();
+    tl_graphs.pop_back();
+  }
+  tl_graphs.push_back({key, exec, tl_scratch_gen, tl_clock});
+  ATLB_CUDA_CHECK(cudaGraphLaunch(exec, st));
 }
 
 int err_mode() {

@@ -33,59 +33,96 @@ constexpr int LEAF = 64;
 
 // Invert the 64x64 (or smaller, last) diagonal blocks of the effective
 // triangle T (T(i,k) = Tp[i*tr + k*tc]) into W: block b is stored dense,
-// column-major 64x64 at W + b*64*64, zero outside its triangle.  One CTA per
-// block, one thread per column of the inverse (forward / backward
-// substitution against the identity, the column held in registers).
+// column-major 64x64 at W + b*64*64, zero outside its triangle (a last block
+// smaller than 64 is padded with the identity).  One CTA per block, by
+// recursive doubling: the eight 8x8 diagonal blocks are inverted by
+// substitution (one thread per column), then the inverse is assembled at
+// block sizes 8 -> 16 -> 32 -> 64 from
+//   lower:  inv([T11 0; T21 T22]) = [W11 0; -W22 T21 W11  W22]
+//   upper:  inv([T11 T12; 0 T22]) = [W11  -W11 T12 W22; 0 W22]
+// (two small matrix products per level, all pairs of a level at once).
 template <typename T>
-__global__ void __launch_bounds__(4 * LEAF)
+__global__ void __launch_bounds__(256)
 trinv_kernel(int n, const T *__restrict__ Tp, long tr, long tc, int lower, int unit, T *__restrict__ W) {
   extern __shared__ __align__(16) unsigned char trinv_smem[];
   T(*sT)[LEAF + 1] = reinterpret_cast<T(*)[LEAF + 1]>(trinv_smem);
   T(*sW)[LEAF + 1] = sT + LEAF;
-  // four threads (consecutive lanes of one warp) per column of the inverse:
-  // column j = tid / 4, the substitution's inner loop split over i mod 4
+  T(*sY)[LEAF + 1] = sW + LEAF;
   const int b = blockIdx.x, r0 = b * LEAF, nb = min(LEAF, n - r0), tid = threadIdx.x;
-  const int j = tid >> 2, part = tid & 3;
   const T *Tb = Tp + r0 * tr + r0 * tc;
-  for (int idx = tid; idx < LEAF * LEAF; idx += 4 * LEAF) {
+  for (int idx = tid; idx < LEAF * LEAF; idx += 256) {
     int i, k;
     if (tr == 1) { i = idx % LEAF; k = idx / LEAF; } else { k = idx % LEAF; i = idx / LEAF; }
-    sT[i][k] = (i < nb && k < nb) ? Tb[i * tr + k * tc] : T(0);
-    sW[i][k] = (i == k) ? T(1) : T(0);
+    T v;
+    if (i < nb && k < nb) {
+      const bool in_tri = lower ? i > k : i < k;
+      v = (i == k) ? (unit ? T(1) : Tb[i * tr + k * tc]) : (in_tri ? Tb[i * tr + k * tc] : T(0));
+    } else {
+      v = (i == k) ? T(1) : T(0);
+    }
+    sT[i][k] = v;
+    sW[i][k] = T(0);
   }
   __syncthreads();
-  const bool active = j < nb;
-  // every lane of a warp runs the same k range (the warp's 8 columns start at
-  // j0 = 8 * warp); for k outside a column's own range the update is zero
-  const int j0 = (tid >> 5) * 8;
-  if (lower) {
-#pragma unroll 1
-    for (int k = j0; k < nb; k++) {
-      const bool on = active && k >= j;
-      T xk = sW[k][j];
-      if (!unit && on) xk = xk / sT[k][k];
-      __syncwarp();
-      if (part == 0 && on) sW[k][j] = xk;
-      if (on)
-        for (int i = k + 1 + part; i < nb; i += 4) sW[i][j] -= sT[i][k] * xk;
-      __syncwarp();
+  // 8x8 diagonal blocks: thread (blk, c) solves for column c of block blk
+  if (tid < LEAF) {
+    const int base = (tid >> 3) * 8, c = tid & 7;
+    T x[8];
+    if (lower) {
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        T s = (k == c) ? T(1) : T(0);
+#pragma unroll
+        for (int m = 0; m < k; m++) s = fma(-sT[base + k][base + m], x[m], s);
+        x[k] = s / sT[base + k][base + k];
+      }
+    } else {
+#pragma unroll
+      for (int k = 7; k >= 0; k--) {
+        T s = (k == c) ? T(1) : T(0);
+#pragma unroll
+        for (int m = k + 1; m < 8; m++) s = fma(-sT[base + k][base + m], x[m], s);
+        x[k] = s / sT[base + k][base + k];
+      }
     }
-  } else {
-#pragma unroll 1
-    for (int k = min(j0 + 7, nb - 1); k >= 0; k--) {
-      const bool on = active && k <= j;
-      T xk = sW[k][j];
-      if (!unit && on) xk = xk / sT[k][k];
-      __syncwarp();
-      if (part == 0 && on) sW[k][j] = xk;
-      if (on)
-        for (int i = part; i < k; i += 4) sW[i][j] -= sT[i][k] * xk;
-      __syncwarp();
-    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) sW[base + k][base + c] = x[k];
   }
   __syncthreads();
+#pragma unroll 1
+  for (int s = 8; s < LEAF; s *= 2) {
+    const int per = s / 8;  // outputs per thread: (LEAF / 2s) pairs x s x s / 256
+    // Y = T21 W11 (lower) or T12 W22 (upper), stored at the off-diagonal block
+    for (int q = 0; q < per; q++) {
+      const int e = tid + q * 256, p = e / (s * s), rem = e % (s * s), i = rem % s, j = rem / s;
+      const int d1 = 2 * p * s, d2 = d1 + s;  // the pair's two diagonal blocks
+      T acc = T(0);
+      if (lower) {
+        for (int k = 0; k < s; k++) acc = fma(sT[d2 + i][d1 + k], sW[d1 + k][d1 + j], acc);
+        sY[d2 + i][d1 + j] = acc;
+      } else {
+        for (int k = 0; k < s; k++) acc = fma(sT[d1 + i][d2 + k], sW[d2 + k][d2 + j], acc);
+        sY[d1 + i][d2 + j] = acc;
+      }
+    }
+    __syncthreads();
+    // off-diagonal block of the inverse = -W22 Y (lower) or -W11 Y (upper)
+    for (int q = 0; q < per; q++) {
+      const int e = tid + q * 256, p = e / (s * s), rem = e % (s * s), i = rem % s, j = rem / s;
+      const int d1 = 2 * p * s, d2 = d1 + s;
+      T acc = T(0);
+      if (lower) {
+        for (int k = 0; k < s; k++) acc = fma(sW[d2 + i][d2 + k], sY[d2 + k][d1 + j], acc);
+        sW[d2 + i][d1 + j] = -acc;
+      } else {
+        for (int k = 0; k < s; k++) acc = fma(sW[d1 + i][d1 + k], sY[d1 + k][d2 + j], acc);
+        sW[d1 + i][d2 + j] = -acc;
+      }
+    }
+    __syncthreads();
+  }
   T *Wb = W + (long)b * LEAF * LEAF;
-  for (int idx = tid; idx < LEAF * LEAF; idx += 4 * LEAF) Wb[idx] = sW[idx % LEAF][idx / LEAF];
+  for (int idx = tid; idx < LEAF * LEAF; idx += 256) Wb[idx] = sW[idx % LEAF][idx / LEAF];
 }
 
 // B_blk (nb x m, effective strides) = W_b (nb x nb) * B_blk, in place: one
@@ -343,13 +380,13 @@ __global__ void finish_info_kernel(int *d) { if (*d == 0x7fffffff) *d = 0; }
 
 template <typename T>
 void trinv_dev(int n, const T *Tp, long tr, long tc, int lower, int unit, T *W, cudaStream_t st) {
-  constexpr int smem = 2 * LEAF * (LEAF + 1) * (int)sizeof(T);
+  constexpr int smem = 3 * LEAF * (LEAF + 1) * (int)sizeof(T);
   static bool configured = false;
   if (!configured) {
     ATLB_CUDA_CHECK(cudaFuncSetAttribute(trinv_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     configured = true;
   }
-  trinv_kernel<T><<<cdiv(n, LEAF), 4 * LEAF, smem, st>>>(n, Tp, tr, tc, lower, unit, W);
+  trinv_kernel<T><<<cdiv(n, LEAF), 256, smem, st>>>(n, Tp, tr, tc, lower, unit, W);
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
 template void trinv_dev<double>(int, const double *, long, long, int, int, double *, cudaStream_t);
@@ -452,6 +489,46 @@ void laswp_dev(int ncols, T *A, long lda, int k1, int k2, const int *ipiv, int i
   }
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
+
+namespace {
+// One thread replays the n interchanges on an index vector (the chain is
+// sequential); the vector sits in shared memory when it fits.
+__global__ void ipiv_perm_kernel(int n, const int *__restrict__ ipiv, int *__restrict__ perm, int use_smem) {
+  extern __shared__ int sp[];
+  int *pv = use_smem ? sp : perm;
+  int *ip = use_smem ? sp + n : nullptr;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    pv[i] = i;
+    if (use_smem) ip[i] = ipiv[i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < n; k++) {
+      const int b = use_smem ? ip[k] : ipiv[k];
+      const int t = pv[k];
+      pv[k] = pv[b];
+      pv[b] = t;
+    }
+  }
+  __syncthreads();
+  if (use_smem)
+    for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = pv[i];
+}
+}  // namespace
+
+void ipiv_to_perm_dev(int n, const int *ipiv, int *perm, cudaStream_t st) {
+  if (n <= 0) return;
+  const size_t bytes = sizeof(int) * 2 * (size_t)n;
+  const int use_smem = bytes <= 200 * 1024;
+  static bool configured = false;
+  if (!configured) {
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(ipiv_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    configured = true;
+  }
+  ipiv_perm_kernel<<<1, 1024, use_smem ? bytes : 0, st>>>(n, ipiv, perm, use_smem);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
+
 template void laswp_dev<double>(int, double *, long, int, int, const int *, int, cudaStream_t);
 template void laswp_dev<float>(int, float *, long, int, int, const int *, int, cudaStream_t);
 
