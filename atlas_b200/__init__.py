@@ -59,6 +59,7 @@ _SIGS = {
     "atlb_sgemm_dev": (_I, [_I, _I, _I, _I, _I, _F, _P, _I, _P, _I, _F, _P, _I]),
     "atlb_sgemm_tc_dev": (_I, [_I, _I, _I, _I, _I, _I, _F, _P, _I, _P, _I, _F, _P, _I]),
     "atlb_dtrsm_dev": (_I, [_I, _I, _I, _I, _I, _I, _D, _P, _I, _P, _I]),
+    "atlb_dtrsm_dev_noalloc": (_I, [_I, _I, _I, _I, _I, _I, _D, _P, _I, _P, _I]),
     "atlb_dsyrk_dev": (_I, [_I, _I, _I, _I, _D, _P, _I, _D, _P, _I]),
     "atlb_dgetrf_dev": (_I, [_I, _I, _P, _I, _P, _P]),
     "atlb_dgetrs_dev": (_I, [_I, _I, _I, _P, _I, _P, _P, _I]),
