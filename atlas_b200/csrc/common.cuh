@@ -45,12 +45,20 @@ struct SideScope {
   SideScope();
   ~SideScope();
 };
+// While a NoAllocScope is alive on a thread, scratch() and pinned() never
+// allocate (they return nullptr instead of growing a buffer) and the GEMM
+// driver does not take its split-K path, which needs a workspace.
+struct NoAllocScope {
+  NoAllocScope();
+  ~NoAllocScope();
+};
+bool no_alloc_active();
 enum ScratchSlot {
   kSlotA = 0, kSlotB, kSlotC, kSlotIpiv, kSlotTau, kSlotWork, kSlotWork2,
   kSlotInfo, kSlotMixedA, kSlotMixedR, kSlotMixedX, kSlotMixedD,
   kSlotOzA, kSlotOzB, kSlotOzScale, kSlotBatch0, kSlotBatch1, kSlotBatch2,
   kSlotBatch3, kSlotAdj0, kSlotAdj1, kSlotAdj2, kSlotTc0, kSlotTc1, kSlotTrsmW, kSlotTrsvCtl, kSlotLaswp,
-  kSlotMixedWL, kSlotMixedWU, kSlotMixedPerm,
+  kSlotMixedWL, kSlotMixedWU, kSlotMixedPerm, kSlotGemmSplit,
   kNumSlots
 };
 

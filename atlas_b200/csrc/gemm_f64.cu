@@ -225,6 +225,41 @@ dgemm_grouped_kernel(const GemmProb *__restrict__ probs, const int *__restrict__
   }
 }
 
+// Split-K for GEMMs with too few output tiles to fill the GPU (the small
+// updates inside the factorizations): CTA (tile, s) multiplies over the s-th
+// K range into its own dense partial P_s (ld = M); a second kernel sums the
+// partials in a fixed order (deterministic) and applies alpha, beta and tri.
+template <bool TA, bool TB, int VEC>
+__global__ void __launch_bounds__(THREADS, 1)
+dgemm_splitk_kernel(int M, int N, int K, int kc, const double *__restrict__ A, long lda,
+                    const double *__restrict__ B, long ldb, double *__restrict__ P) {
+  extern __shared__ __align__(16) double smem[];
+  const int tiles_m = (M + BM - 1) / BM;
+  const int tm = blockIdx.x % tiles_m, tn = blockIdx.x / tiles_m, s = blockIdx.y;
+  const int k0 = s * kc, kl = min(kc, K - k0);
+  const double *As = TA ? A + k0 : A + (long)k0 * lda;
+  const double *Bs = TB ? B + (long)k0 * ldb : B + k0;
+  dgemm_tile<TA, TB, VEC>(M, N, kl, 1.0, As, lda, Bs, ldb, 0.0, P + (long)s * M * N, M, 0, tm * BM,
+                          tn * BN, smem);
+}
+
+__global__ void splitk_reduce_kernel(int M, int N, int S, double alpha, const double *__restrict__ P,
+                                     double beta, double *__restrict__ C, long ldc, int tri) {
+  const long total = (long)M * N, mn = total;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    const int r = (int)(idx % M), c = (int)(idx / M);
+    if (tri == 1 && r < c) continue;
+    if (tri == 2 && r > c) continue;
+    double acc = 0.0;
+    for (int s = 0; s < S; s++) acc += P[idx + s * mn];
+    double *p = C + r + (long)c * ldc;
+    double v = alpha * acc;
+    if (beta != 0.0) v = fma(beta, *p, v);
+    *p = v;
+  }
+}
+
 __global__ void scale_kernel(int M, int N, double beta, double *C, long ldc, int tri) {
   long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
   long total = (long)M * N;
@@ -248,6 +283,29 @@ void launch(int M, int N, int K, double alpha, const double *A, long lda, const 
     configured = true;
   }
   int tiles = cdiv(M, BM) * cdiv(N, BN);
+  // too few tiles for the 148 SMs and a long K: split K (partials + reduction)
+  const int nsm = num_sms();
+  int S = 1;
+  if (tiles * 2 <= nsm && K >= 4 * BK && !no_alloc_active()) S = std::min(cdiv(nsm, tiles), K / (2 * BK));
+  if (S > 1) {
+    const int kc = cdiv(cdiv(K, S), BK) * BK;
+    S = cdiv(K, kc);
+    double *P = (double *)scratch(kSlotGemmSplit, sizeof(double) * (size_t)S * M * N);
+    if (P) {
+      static bool configured_s = false;
+      if (!configured_s) {
+        ATLB_CUDA_CHECK(cudaFuncSetAttribute(dgemm_splitk_kernel<TA, TB, VEC>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        configured_s = true;
+      }
+      dgemm_splitk_kernel<TA, TB, VEC><<<dim3(tiles, S), THREADS, smem, st>>>(M, N, K, kc, A, lda, B, ldb, P);
+      const long total = (long)M * N;
+      splitk_reduce_kernel<<<(int)std::min<long>((total + 255) / 256, 148L * 8), 256, 0, st>>>(
+          M, N, S, alpha, P, beta, C, ldc, tri);
+      ATLB_CUDA_CHECK(cudaGetLastError());
+      return;
+    }
+  }
   dgemm_dmma_kernel<TA, TB, VEC><<<tiles, THREADS, smem, st>>>(M, N, K, alpha, A, lda, B, ldb,
                                                               beta, C, ldc, tri);
   ATLB_CUDA_CHECK(cudaGetLastError());

@@ -188,33 +188,41 @@ getf2_cluster_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restr
   cl.sync();  // keep this CTA's shared memory alive until every peer is done
 }
 
-// Panel kernel for up to 32 columns and up to 512 rows per CTA (one row per
-// thread), organised so that a column costs one CTA barrier and one cluster
-// barrier and no runtime-indexed register access:
-//   * each thread keeps its row SHIFTED: a[0] always holds the current
-//     column, so the rank-1 update of column j is a[k-1] = a[k] - l * u[k]
-//     over fixed register indices (the shift is free: each FMA writes the
-//     register the previous column just vacated);
-//   * the finished part of each row goes to shared memory (L multipliers as
-//     they are produced; the U part of a pivot row when it is chosen) and is
-//     written to its final row position at the end;
-//   * per column: warp arg-max -> CTA arg-max (one __syncthreads); the CTA's
-//     winner publishes (|value|, position, row) in its shared memory; one
-//     cluster barrier; every warp then reads the C candidates over
-//     distributed shared memory (one load per lane), reduces them to the
-//     same global winner, and fetches that row (one load per lane) into a
-//     per-warp buffer from which all lanes read the update row.
+// Leaf panel kernel: LU with partial pivoting of an M x ncols panel (ncols
+// <= 32, M <= 512 x cluster size), fused with the two operations that
+// follow it inside a block column of the factorization:
+//   * the panel's row interchanges applied to the block's other columns
+//     (nleft columns left of the panel, nright right of it), and
+//   * the triangular solve U12 = L11^-1 A12 of the right columns' top rows.
+// One thread holds one row, SHIFTED: a[0] is always the current column, so
+// the rank-1 update is a[k-1] = a[k] - l*u[k] over fixed register indices.
+// Finished parts of rows go to shared memory (L multipliers as produced, the
+// U part of a pivot row when chosen) and reach their final row at the end.
+//
+// Per column, one cluster barrier and no remote reads: each CTA reduces its
+// candidates (warp arg-max, then one __syncthreads), the CTA winner first
+// completes its own row update, and its warp PUSHES (|value|, position, row)
+// into a slot of every CTA's shared memory; after the barrier every warp
+// reduces the C local slots to the same global winner.  The rest of the
+// rank-1 update runs between the barrier's arrive and wait, so the barrier
+// latency hides behind it.  Slots are double-buffered by column parity.
 // Pivot order: largest |value|, lowest current row position on ties (the
 // first maximum, like cblas_idamax); a NaN entry ranks below every number.
 template <typename T, int NB>
-struct ShiftPub {
+struct PanelSlot {
   T row[NB];
   T val;
   int pos;
 };
 
 template <typename T>
-__device__ __forceinline__ void argmax_step(T &v, int &p, int &w, int o) {
+__device__ __forceinline__ void argmax2(T &v, int &p, int o) {
+  const T ov = __shfl_xor_sync(0xffffffffu, v, o);
+  const int op = __shfl_xor_sync(0xffffffffu, p, o);
+  if (ov > v || (ov == v && op < p)) { v = ov; p = op; }
+}
+template <typename T>
+__device__ __forceinline__ void argmax3(T &v, int &p, int &w, int o) {
   const T ov = __shfl_xor_sync(0xffffffffu, v, o);
   const int op = __shfl_xor_sync(0xffffffffu, p, o);
   const int ow = __shfl_xor_sync(0xffffffffu, w, o);
@@ -228,23 +236,56 @@ __device__ __forceinline__ void cluster_wait() {
   asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
 }
 
+// U12 = L11^-1 A12 for the fused panel kernel (one CTA; L11 = the unit
+// lower MN x MN top of the factored panel, A12 its right columns' top rows).
+// Kept out of line so its registers do not add to the panel loop's.
+template <typename T, int NB>
+__device__ __noinline__ void panel_u12_solve(int MN, int ncols, int nright, T *A, long lda, unsigned char *smem) {
+  const int tid = threadIdx.x;
+  T(*sL)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem);
+  for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
+    const int i = idx % NB, k = idx / NB;
+    sL[i][k] = (i < MN && k < i) ? __ldcg(A + i + (long)k * lda) : T(0);
+  }
+  __syncthreads();
+  for (int c = tid; c < nright; c += blockDim.x) {
+    T *col = A + (long)(ncols + c) * lda;
+    T x[NB];
+#pragma unroll
+    for (int i = 0; i < NB; i++) x[i] = i < MN ? __ldcg(col + i) : T(0);
+#pragma unroll
+    for (int i = 1; i < NB; i++) {
+      T s = x[i];
+#pragma unroll
+      for (int k = 0; k < i; k++) s = fma(-sL[i][k], x[k], s);
+      x[i] = s;
+    }
+#pragma unroll
+    for (int i = 0; i < NB; i++)
+      if (i < MN) col[i] = x[i];
+  }
+}
+
+constexpr int kMaxPanelCluster = 16;
+
 template <typename T, int NB>
 __global__ void __launch_bounds__(PT, 1)
-getf2_shift_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restrict__ ipiv,
-                   int roff, int *__restrict__ dinfo) {
+getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restrict__ ipiv, int roff,
+                   int *__restrict__ dinfo, int nleft, int nright) {
   static_assert(NB == 32, "one pivot-row element per lane");
   cg::cluster_group cl = cg::this_cluster();
   const int C = (int)cl.num_blocks(), crank = (int)cl.block_rank();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int MN = min(M, ncols);
-  extern __shared__ __align__(16) unsigned char shift_smem[];
-  T *Lsm = reinterpret_cast<T *>(shift_smem);  // [NB][PT]: finished row parts
-  __shared__ ShiftPub<T, NB> pub[2];
+  extern __shared__ __align__(16) unsigned char fused_smem[];
+  T *Lsm = reinterpret_cast<T *>(fused_smem);  // [NB][PT]: finished row parts
+  __shared__ PanelSlot<T, NB> slot[2][kMaxPanelCluster];
   __shared__ __align__(16) T wu[PT / 32][NB];  // per-warp copy of the pivot row
+  __shared__ __align__(16) T stage[NB];        // the CTA winner's row, for the push
+  __shared__ T zrow[NB];
   __shared__ T wv[PT / 32];
   __shared__ int wp[PT / 32];
-  __shared__ T zrow[NB];
-  if (tid < NB) zrow[tid] = T(0);  // ordered before its first use by publish's barriers
+  if (tid < NB) zrow[tid] = T(0);  // ordered before first use by the first barrier
 
   const int r = crank * PT + tid;
   bool act = r < M;
@@ -258,59 +299,79 @@ getf2_shift_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
       if (k + 1 < ncols) src += lda;
     }
   }
+  T lm = T(0);
+  const T *u = zrow;
 
-  // CTA-level candidate for the current column (a[0]); publishes into pub[b]
-  auto publish = [&](int b) {
+  // Reduce this CTA's candidates (|a[0]| of active rows), let the winner
+  // finish its row (tail() when it still owes the update), push to all CTAs.
+  auto push = [&](int b, bool owes_tail) {
     T v = T(-1);
-    int p = INT_MAX, w = 0;
+    int p = INT_MAX;
     if (act) {
       const T t = fabs(a[0]);
-      v = t >= T(0) ? t : T(-0.5);  // NaN ranks below every number
+      v = t >= T(0) ? t : T(-0.5);
       p = pos;
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) argmax_step(v, p, w, o);
+    for (int o = 16; o > 0; o >>= 1) argmax2(v, p, o);
     if (lane == 0) { wv[warp] = v; wp[warp] = p; }
     __syncthreads();
     v = lane < PT / 32 ? wv[lane] : T(-1);
     p = lane < PT / 32 ? wp[lane] : INT_MAX;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) argmax_step(v, p, w, o);
-    if (tid == 0) { pub[b].val = v; pub[b].pos = p; }
-    if (act && pos == p) {
+    for (int o = 16; o > 0; o >>= 1) argmax2(v, p, o);
+    const bool owner = act && pos == p;
+    bool done = false;
+    if (owner) {
+      if (owes_tail) {
 #pragma unroll
-      for (int k = 0; k < NB; k++) pub[b].row[k] = a[k];
+        for (int k = 2; k < NB; k++) a[k - 1] = fma(-lm, u[k], a[k]);
+        a[NB - 1] = T(0);
+        done = true;
+      }
+#pragma unroll
+      for (int k = 0; k < NB; k++) stage[k] = a[k];
+    }
+    const bool mine = __any_sync(0xffffffffu, owner) || (p == INT_MAX && warp == 0);
+    if (mine) {
+      __syncwarp();
+      const T e = stage[lane];
+      for (int q = 0; q < C; q++) {
+        PanelSlot<T, NB> *rs = cl.map_shared_rank(&slot[b][crank], q);
+        rs->row[lane] = e;
+      }
+      if (lane < C) {
+        PanelSlot<T, NB> *rs = cl.map_shared_rank(&slot[b][crank], lane);
+        rs->val = v;
+        rs->pos = p;
+      }
     }
     __syncwarp();
     cluster_arrive();
-    cluster_wait();
+    return done;
   };
 
-  if (MN > 0) publish(0);
+  if (MN > 0) {
+    push(0, false);
+    cluster_wait();
+  }
 #pragma unroll 1
   for (int j = 0; j < MN; j++) {
     const int b = j & 1;
-    // every warp reduces the C published candidates to the same winner
-    T v = T(-1);
-    int p = INT_MAX, w = 0;
-    if (lane < C) {
-      const ShiftPub<T, NB> *rp = cl.map_shared_rank(&pub[b], lane);
-      v = rp->val;
-      p = rp->pos;
-      w = lane;
-    }
+    // the global winner from the C local slots (every warp computes it)
+    T v = lane < C ? slot[b][lane].val : T(-1);
+    int p = lane < C ? slot[b][lane].pos : INT_MAX, w = lane;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) argmax_step(v, p, w, o);
-    {
-      const ShiftPub<T, NB> *rp = cl.map_shared_rank(&pub[b], w);
-      wu[warp][lane] = rp->row[lane];
-    }
+    for (int o = 16; o > 0; o >>= 1) argmax3(v, p, w, o);
+    __syncwarp();
+    wu[warp][lane] = slot[b][w].row[lane];
     __syncwarp();
     const T piv = wu[warp][0];
     if (crank == 0 && tid == 0) {
       ipiv[j] = roff + p;
       if (piv == T(0)) atomicMin(dinfo, roff + j + 1);
     }
+    bool owes = false;
     if (act) {
       if (pos == p) {  // this row becomes row j of U: its remaining part is final
         act = false;
@@ -325,24 +386,57 @@ getf2_shift_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
         // update then runs with l = 0 against a zero row (exact: a - 0*0 = a)
         const bool nz = piv != T(0);
         const T l = !nz ? a[0] : (fabs(piv) >= safmin<T>() ? a[0] * (T(1) / piv) : a[0] / piv);
-        const T lm = nz ? l : T(0);
-        const T *u = nz ? wu[warp] : zrow;
+        lm = nz ? l : T(0);
+        u = nz ? wu[warp] : zrow;
         Lsm[j * PT + tid] = l;
-#pragma unroll
-        for (int k = 1; k < NB; k++) a[k - 1] = fma(-lm, u[k], a[k]);
-        a[NB - 1] = T(0);
+        a[0] = fma(-lm, u[1], a[1]);  // the next column first: it decides the next pivot
+        owes = j + 1 < MN;
       }
     }
-    if (j + 1 < MN) publish(b ^ 1);
+    if (j + 1 < MN) {
+      const bool done = push(b ^ 1, owes);
+      if (owes && !done) {
+#pragma unroll
+        for (int k = 2; k < NB; k++) a[k - 1] = fma(-lm, u[k], a[k]);
+        a[NB - 1] = T(0);
+      }
+      cluster_wait();
+    }
   }
 
-  if (r < M) {
+  // rows to their final positions: the panel's columns from shared memory,
+  // then the block's other columns (through shared memory, 32 at a time, a
+  // cluster barrier between reading all moving rows and writing them)
+  const bool in = r < M;
+  if (in) {
 #pragma unroll 4
     for (int k = 0; k < ncols; k++) A[pos + (long)k * lda] = Lsm[k * PT + tid];
   }
+  const bool moved = in && pos != r;
+  const int nother = nleft + nright;
+  for (int c0 = 0; c0 < nother; c0 += NB) {
+    const int nc = min(NB, nother - c0);
+    if (moved) {
+      for (int k = 0; k < nc; k++) {
+        const int c = c0 + k, col = c < nleft ? c - nleft : ncols + (c - nleft);
+        Lsm[k * PT + tid] = __ldcg(A + r + (long)col * lda);
+      }
+    }
+    __syncwarp();
+    cluster_arrive();
+    cluster_wait();
+    if (moved) {
+      for (int k = 0; k < nc; k++) {
+        const int c = c0 + k, col = c < nleft ? c - nleft : ncols + (c - nleft);
+        A[pos + (long)col * lda] = Lsm[k * PT + tid];
+      }
+    }
+  }
   __syncwarp();
-  cluster_arrive();  // peers may still be reading this CTA's last candidate
+  cluster_arrive();  // every row is in place (and no CTA still pushes to this one)
   cluster_wait();
+  // U12 = L11^-1 A12 on the right columns' top MN rows (L11 unit lower)
+  if (crank == 0 && nright > 0 && MN > 1) panel_u12_solve<T, NB>(MN, ncols, nright, A, lda, fused_smem);
 }
 
 // Fallback for panels taller than a cluster can hold: one CTA, global memory.
@@ -458,27 +552,27 @@ void init_max_cluster() {
 }
 
 template <typename T>
-constexpr int shift_smem_bytes() { return 32 * PT * (int)sizeof(T); }
+constexpr int fused_smem_bytes() { return 32 * PT * (int)sizeof(T); }
 
-// Largest cluster of the shift kernel (<= 16 CTAs, ~130 KB shared memory
-// each) the device can co-schedule; 0 when none.
+// Largest cluster of the fused panel kernel (<= 16 CTAs, ~140 KB shared
+// memory each) the device can co-schedule; 0 when none.
 template <typename T>
-int max_cluster_shift() {
+int max_cluster_fused() {
   static int cached = -1;
   if (cached >= 0) return cached;
-  auto kern = getf2_shift_kernel<T, 32>;
+  auto kern = getf2_fused_kernel<T, 32>;
   cached = 0;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, shift_smem_bytes<T>()) !=
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, fused_smem_bytes<T>()) !=
           cudaSuccess) {
     cudaGetLastError();
     return cached;
   }
-  for (int c : {16, 8}) {
+  for (int c : {kMaxPanelCluster, 8}) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(c, 1, 1);
     cfg.blockDim = dim3(PT, 1, 1);
-    cfg.dynamicSmemBytes = shift_smem_bytes<T>();
+    cfg.dynamicSmemBytes = fused_smem_bytes<T>();
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = c;
@@ -493,16 +587,19 @@ int max_cluster_shift() {
   return cached;
 }
 
+// Factor the M x ncols panel at A (rows 0.., ipiv + roff numbering) and, when
+// nleft / nright > 0, interchange the rows of the block columns beside it and
+// solve its right columns' top rows (see getf2_fused_kernel).
 template <typename T>
-bool launch_shift_panel(int M, int ncols, T *A, long lda, int *ipiv, int roff, int *dinfo,
-                        cudaStream_t st) {
+bool launch_fused_panel(int M, int ncols, T *A, long lda, int *ipiv, int roff, int *dinfo, int nleft,
+                        int nright, cudaStream_t st) {
   if (ncols > 32) return false;
   const int C = cdiv(M, PT);
-  if (C > max_cluster_shift<T>()) return false;
+  if (C > max_cluster_fused<T>()) return false;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(C, 1, 1);
   cfg.blockDim = dim3(PT, 1, 1);
-  cfg.dynamicSmemBytes = shift_smem_bytes<T>();
+  cfg.dynamicSmemBytes = fused_smem_bytes<T>();
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -511,11 +608,12 @@ bool launch_shift_panel(int M, int ncols, T *A, long lda, int *ipiv, int roff, i
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  ATLB_CUDA_CHECK(cudaLaunchKernelEx(&cfg, getf2_shift_kernel<T, 32>, M, ncols, A, lda, ipiv, roff, dinfo));
+  ATLB_CUDA_CHECK(cudaLaunchKernelEx(&cfg, getf2_fused_kernel<T, 32>, M, ncols, A, lda, ipiv, roff, dinfo,
+                                     nleft, nright));
   return true;
 }
 
-bool shift_panel_disabled() {
+bool fused_panel_disabled() {
   static int v = -1;
   if (v < 0) {
     const char *e = getenv("ATLAS_B200_PANEL");
@@ -535,7 +633,7 @@ int panel_nb(int M) {
 
 template <typename T>
 void panel(int M, int ncols, T *A, long lda, int *ipiv, int roff, int *dinfo, cudaStream_t st) {
-  bool ok = !shift_panel_disabled() && launch_shift_panel<T>(M, ncols, A, lda, ipiv, roff, dinfo, st);
+  bool ok = !fused_panel_disabled() && launch_fused_panel<T>(M, ncols, A, lda, ipiv, roff, dinfo, 0, 0, st);
   if (ok) return;
   if (ncols <= 32 && M <= g_max_cluster * PT) ok = launch_cluster_panel<T, 32, 1>(M, ncols, A, lda, ipiv, roff, dinfo, st);
   else if (ncols <= 16 && M <= g_max_cluster * PT * 2) ok = launch_cluster_panel<T, 16, 2>(M, ncols, A, lda, ipiv, roff, dinfo, st);
@@ -583,6 +681,28 @@ void getrf_rec(int off, int M, int N, T *A, long lda, int *ipiv, int *dinfo, cud
   laswp_dev<T>(Nl, A + (long)off * lda, lda, off + Nl, off + MN, ipiv, 1, st);
 }
 
+// Block column [j, j + jb) of the factorization, rows j..M-1, as 32-column
+// leaves: each leaf is one fused panel launch (factor + interchanges across
+// the block + U12 solve) followed by one GEMM updating the block's columns
+// right of the leaf.  The pivots are those of the reference's recursion
+// (partial pivoting does not depend on the blocking).  Returns false when
+// the rows do not fit one cluster (the caller then uses the recursion).
+template <typename T>
+bool getrf_block(int j, int M, int jb, T *A, long lda, int *ipiv, int *dinfo, cudaStream_t st,
+                 SgemmFn gemm) {
+  if (fused_panel_disabled() || cdiv(M - j, PT) > max_cluster_fused<T>()) return false;
+  for (int l = 0; l < jb; l += 32) {
+    const int c = j + l, w = std::min(32, jb - l), m = M - c;
+    if (m <= 0) break;
+    const int nright = jb - l - w;
+    T *Ac = A + c + (long)c * lda;
+    launch_fused_panel<T>(m, w, Ac, lda, ipiv + c, c, dinfo, l, nright, st);
+    if (nright > 0 && m - w > 0)
+      update_gemm(gemm, m - w, nright, w, Ac + w, Ac + (long)w * lda, Ac + w + (long)w * lda, lda, st);
+  }
+  return true;
+}
+
 }  // namespace
 
 bool lookahead_enabled() {
@@ -616,7 +736,8 @@ void getrf_dev(int M, int N, T *A, long lda, int *ipiv, int *dinfo, cudaStream_t
       for (int j = 0; j < MN; j += NBO) {
         const int jb = std::min(NBO, MN - j);
         T *Ad = A + j + (long)j * lda;
-        getrf_rec<T>(j, M - j, jb, A, lda, ipiv, dinfo, st, gemm);   // panel: rows j.., columns j..j+jb
+        if (!getrf_block<T>(j, M, jb, A, lda, ipiv, dinfo, st, gemm))   // panel: rows j.., columns j..j+jb
+          getrf_rec<T>(j, M - j, jb, A, lda, ipiv, dinfo, st, gemm);
         if (j > 0) laswp_dev<T>(j, A, lda, j, j + jb, ipiv, 1, st);  // left of the panel
         const int nr = N - j - jb;
         if (nr > 0) {
@@ -635,7 +756,8 @@ void getrf_dev(int M, int N, T *A, long lda, int *ipiv, int *dinfo, cudaStream_t
       // next block column, the main stream everything to its right and the
       // interchanges on the left.
       cudaStream_t s1 = side_stream();
-      getrf_rec<T>(0, M, std::min(NBO, MN), A, lda, ipiv, dinfo, st, gemm);
+      if (!getrf_block<T>(0, M, std::min(NBO, MN), A, lda, ipiv, dinfo, st, gemm))
+        getrf_rec<T>(0, M, std::min(NBO, MN), A, lda, ipiv, dinfo, st, gemm);
       for (int k = 0; k < nblk; k++) {
         const int j = k * NBO, jb = std::min(NBO, MN - j), jn = j + jb;
         const int jbn = k + 1 < nblk ? std::min(NBO, MN - jn) : 0;
@@ -649,7 +771,8 @@ void getrf_dev(int M, int N, T *A, long lda, int *ipiv, int *dinfo, cudaStream_t
           laswp_dev<T>(jbn, An, lda, j, jn, ipiv, 1, s1);
           trsm_dev<T>(kLeft, kLower, kNoTrans, kUnit, jb, jbn, T(1), Ad, lda, An + j, lda, s1, gemm);
           if (M - jn > 0) update_gemm(gemm, M - jn, jbn, jb, Ad + jb, An + j, An + jn, lda, s1);
-          getrf_rec<T>(jn, M - jn, jbn, A, lda, ipiv, dinfo, s1, gemm);
+          if (!getrf_block<T>(jn, M, jbn, A, lda, ipiv, dinfo, s1, gemm))
+            getrf_rec<T>(jn, M - jn, jbn, A, lda, ipiv, dinfo, s1, gemm);
           ATLB_CUDA_CHECK(cudaEventRecord(side_event(2 + ((k + 1) & 1)), s1));
         }
         if (j > 0) laswp_dev<T>(j, A, lda, j, jn, ipiv, 1, st);

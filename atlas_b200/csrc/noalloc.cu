@@ -84,6 +84,7 @@ extern "C" int atlb_dtrsm_dev_noalloc(int Side, int Uplo, int TA, int Diag, int 
   if (M == 0 || N == 0) return 0;
   double *W = workspace_address();
   if (!W) return -100;
+  NoAllocScope guard;  // the GEMMs inside the solve must not take a workspace either
   trsm_impl<double>(Side, Uplo, TA == kNoTrans ? kNoTrans : kTrans, Diag, M, N, alpha, A, lda, B, ldb,
                     stream(), nullptr, W);
   return 0;

@@ -97,9 +97,17 @@ cudaEvent_t side_event(int i) {
 SideScope::SideScope() { tl_side = 1; }
 SideScope::~SideScope() { tl_side = 0; }
 
+namespace {
+thread_local int tl_no_alloc = 0;
+}
+NoAllocScope::NoAllocScope() { tl_no_alloc++; }
+NoAllocScope::~NoAllocScope() { tl_no_alloc--; }
+bool no_alloc_active() { return tl_no_alloc > 0; }
+
 void *scratch(int slot, size_t bytes) {
   Buf &b = tl.dev[slot + tl_side * kNumSlots];
   if (bytes == 0) bytes = 16;
+  if (b.n < bytes && no_alloc_active()) return nullptr;
   if (b.n < bytes && tl_capturing) {
     // cannot allocate while recording a graph: the capture is abandoned and
     // the work re-run eagerly (the pointer returned here is never executed)
@@ -130,6 +138,7 @@ void *scratch(int slot, size_t bytes) {
 void *pinned(int slot, size_t bytes) {
   Buf &b = tl.host[slot + tl_side * kNumSlots];
   if (bytes == 0) bytes = 16;
+  if (b.n < bytes && no_alloc_active()) return nullptr;
   if (b.n < bytes && tl_capturing) {
     tl_capture_failed = true;
     return b.p ? b.p : (void *)tl.host;
