@@ -156,25 +156,38 @@ __device__ __forceinline__ void dgemm_tile(int M, int N, int K, double alpha, co
   }
   cp_async_wait<0>();
 
-  // epilogue: C fragment row = lane>>2, cols = 2*(lane&3) + {0,1}
+  // epilogue: C fragment row = lane>>2, cols = 2*(lane&3) + {0,1}.  The old
+  // C values of fragment row i+1 are loaded before row i is stored, so the
+  // loads' latencies overlap instead of adding up.
+  auto ok = [&](int r, int c) {
+    return r < M && c < N && !(tri == 1 && r < c) && !(tri == 2 && r > c);
+  };
+  double cv[2][4][2];
+  auto load_c = [&](int i, double (&d)[4][2]) {
+    const int r = m0 + wm + i * 8 + fr;
 #pragma unroll
-  for (int i = 0; i < 8; i++) {
-    int r = m0 + wm + i * 8 + fr;
-    if (r >= M) continue;
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
+    for (int j = 0; j < 4; j++)
 #pragma unroll
       for (int h = 0; h < 2; h++) {
-        int c = n0 + wn + j * 8 + fk * 2 + h;
-        if (c >= N) continue;
-        if (tri == 1 && r < c) continue;
-        if (tri == 2 && r > c) continue;
-        double *p = C + r + (long)c * ldc;
-        double v = alpha * acc[i][j][h];
-        if (beta != 0.0) v = fma(beta, *p, v);
-        *p = v;
+        const int c = n0 + wn + j * 8 + fk * 2 + h;
+        d[j][h] = (beta != 0.0 && ok(r, c)) ? C[r + (long)c * ldc] : 0.0;
       }
-    }
+  };
+  load_c(0, cv[0]);
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    if (i + 1 < 8) load_c(i + 1, cv[(i + 1) & 1]);
+    const int r = m0 + wm + i * 8 + fr;
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int c = n0 + wn + j * 8 + fk * 2 + h;
+        if (!ok(r, c)) continue;
+        double v = alpha * acc[i][j][h];
+        if (beta != 0.0) v = fma(beta, cv[i & 1][j][h], v);
+        C[r + (long)c * ldc] = v;
+      }
   }
 }
 

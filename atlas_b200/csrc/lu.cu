@@ -211,22 +211,29 @@ getf2_cluster_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restr
 template <typename T, int NB>
 struct PanelSlot {
   T row[NB];
-  T val;
+  unsigned long long key;  // pivot_key of the candidate
+  T rcp;                   // 1 / row[0], computed by the sender off the critical path
   int pos;
 };
 
+// Candidates are compared through one integer key: |value|'s bit pattern + 1
+// (non-negative IEEE values order like their bit patterns), 0 for a NaN or
+// for "no candidate"; ties go to the lowest row position.  A warp's arg-max
+// is then three redux instructions instead of a shuffle tree.
 template <typename T>
-__device__ __forceinline__ void argmax2(T &v, int &p, int o) {
-  const T ov = __shfl_xor_sync(0xffffffffu, v, o);
-  const int op = __shfl_xor_sync(0xffffffffu, p, o);
-  if (ov > v || (ov == v && op < p)) { v = ov; p = op; }
+__device__ __forceinline__ unsigned long long pivot_key(T v) {
+  const T t = fabs(v);
+  if (!(t >= T(0))) return 0ull;
+  if (sizeof(T) == 8) return (unsigned long long)__double_as_longlong((double)t) + 1ull;
+  return (unsigned long long)__float_as_uint((float)t) + 1ull;
 }
-template <typename T>
-__device__ __forceinline__ void argmax3(T &v, int &p, int &w, int o) {
-  const T ov = __shfl_xor_sync(0xffffffffu, v, o);
-  const int op = __shfl_xor_sync(0xffffffffu, p, o);
-  const int ow = __shfl_xor_sync(0xffffffffu, w, o);
-  if (ov > v || (ov == v && op < p)) { v = ov; p = op; w = ow; }
+__device__ __forceinline__ void warp_argmax_key(unsigned long long &key, unsigned &pos) {
+  const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+  const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+  const bool eq = hi == mhi && lo == mlo;
+  pos = __reduce_min_sync(0xffffffffu, eq ? pos : 0xffffffffu);
+  key = ((unsigned long long)mhi << 32) | mlo;
 }
 
 __device__ __forceinline__ void cluster_arrive() {
@@ -234,6 +241,35 @@ __device__ __forceinline__ void cluster_arrive() {
 }
 __device__ __forceinline__ void cluster_wait() {
   asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ uint32_t mapa_u32(uint32_t a, int rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+  return r;
+}
+// one-way store into another CTA's shared memory that completes a
+// transaction on that CTA's mbarrier (no fence, no round trip)
+__device__ __forceinline__ void st_async(uint32_t addr, double v, uint32_t mbar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b64 [%0], %1, [%2];"
+               ::"r"(addr), "l"(__double_as_longlong(v)), "r"(mbar) : "memory");
+}
+__device__ __forceinline__ void st_async(uint32_t addr, float v, uint32_t mbar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b32 [%0], %1, [%2];"
+               ::"r"(addr), "r"(__float_as_uint(v)), "r"(mbar) : "memory");
+}
+__device__ __forceinline__ void st_async(uint32_t addr, unsigned long long v, uint32_t mbar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b64 [%0], %1, [%2];"
+               ::"r"(addr), "l"(v), "r"(mbar) : "memory");
+}
+__device__ __forceinline__ void st_async(uint32_t addr, int v, uint32_t mbar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b32 [%0], %1, [%2];"
+               ::"r"(addr), "r"(v), "r"(mbar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t a, uint32_t parity) {
+  uint32_t ok;
+  asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+               " selp.u32 %0, 1, 0, p;\n}" : "=r"(ok) : "r"(a), "r"(parity) : "memory");
+  return ok != 0;
 }
 
 // U12 = L11^-1 A12 for the fused panel kernel (one CTA; L11 = the unit
@@ -267,12 +303,14 @@ __device__ __noinline__ void panel_u12_solve(int MN, int ncols, int nright, T *A
 }
 
 constexpr int kMaxPanelCluster = 16;
+__device__ int g_panel_timeout = 0;  // set if a panel wait ever gives up (1 s)
 
 template <typename T, int NB>
 __global__ void __launch_bounds__(PT, 1)
 getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restrict__ ipiv, int roff,
                    int *__restrict__ dinfo, int nleft, int nright) {
   static_assert(NB == 32, "one pivot-row element per lane");
+  constexpr uint32_t kMsg = NB * sizeof(T) + 8 + sizeof(T) + sizeof(int);  // bytes one CTA sends one CTA
   cg::cluster_group cl = cg::this_cluster();
   const int C = (int)cl.num_blocks(), crank = (int)cl.block_rank();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -280,12 +318,25 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
   extern __shared__ __align__(16) unsigned char fused_smem[];
   T *Lsm = reinterpret_cast<T *>(fused_smem);  // [NB][PT]: finished row parts
   __shared__ PanelSlot<T, NB> slot[2][kMaxPanelCluster];
+  __shared__ __align__(8) unsigned long long mbar[2];
   __shared__ __align__(16) T wu[PT / 32][NB];  // per-warp copy of the pivot row
-  __shared__ __align__(16) T stage[NB];        // the CTA winner's row, for the push
+  __shared__ __align__(16) T stage[NB + 1];    // the CTA winner's row and 1/row[0], for the push
   __shared__ T zrow[NB];
-  __shared__ T wv[PT / 32];
-  __shared__ int wp[PT / 32];
-  if (tid < NB) zrow[tid] = T(0);  // ordered before first use by the first barrier
+  __shared__ unsigned long long wv[2][PT / 32];   // per-warp candidates, by column parity
+  __shared__ unsigned wp[2][PT / 32];
+  __shared__ int s_nmoved;
+  __shared__ int s_from[2 * NB], s_to[2 * NB];  // rows that move: from (old) -> to (final)
+  const uint32_t mb0 = smem_u32(&mbar[0]), mb1 = smem_u32(&mbar[1]);
+  if (tid < NB) zrow[tid] = T(0);
+  if (tid == 0) {
+    s_nmoved = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb0));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb1));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  cluster_arrive();  // every CTA's barriers exist before anyone sends
+  cluster_wait();
 
   const int r = crank * PT + tid;
   bool act = r < M;
@@ -302,25 +353,23 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
   T lm = T(0);
   const T *u = zrow;
 
-  // Reduce this CTA's candidates (|a[0]| of active rows), let the winner
-  // finish its row (tail() when it still owes the update), push to all CTAs.
-  auto push = [&](int b, bool owes_tail) {
-    T v = T(-1);
-    int p = INT_MAX;
-    if (act) {
-      const T t = fabs(a[0]);
-      v = t >= T(0) ? t : T(-0.5);
-      p = pos;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) argmax2(v, p, o);
-    if (lane == 0) { wv[warp] = v; wp[warp] = p; }
+  // Reduce this CTA's candidates (|a[0]| of active rows); the winner first
+  // finishes its row (when it still owes the update), then its warp sends
+  // (row, |value|, position) for column c to every CTA's slot.
+  auto push = [&](int c, bool owes_tail) {
+    const int b = c & 1;
+    const uint32_t mb = b ? mb1 : mb0;
+    if (tid == 0)
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(kMsg * C) : "memory");
+    unsigned long long v = act ? pivot_key(a[0]) : 0ull;
+    unsigned p = act ? (unsigned)pos : 0xffffffffu;
+    warp_argmax_key(v, p);
+    if (lane == 0) { wv[b][warp] = v; wp[b][warp] = p; }
     __syncthreads();
-    v = lane < PT / 32 ? wv[lane] : T(-1);
-    p = lane < PT / 32 ? wp[lane] : INT_MAX;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) argmax2(v, p, o);
-    const bool owner = act && pos == p;
+    v = lane < PT / 32 ? wv[b][lane] : 0ull;
+    p = lane < PT / 32 ? wp[b][lane] : 0xffffffffu;
+    warp_argmax_key(v, p);
+    const bool owner = act && (unsigned)pos == p;
     bool done = false;
     if (owner) {
       if (owes_tail) {
@@ -331,42 +380,60 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
       }
 #pragma unroll
       for (int k = 0; k < NB; k++) stage[k] = a[k];
+      stage[NB] = T(1) / a[0];
     }
-    const bool mine = __any_sync(0xffffffffu, owner) || (p == INT_MAX && warp == 0);
+    const bool mine = __any_sync(0xffffffffu, owner) || (p == 0xffffffffu && warp == 0);
     if (mine) {
       __syncwarp();
       const T e = stage[lane];
-      for (int q = 0; q < C; q++) {
-        PanelSlot<T, NB> *rs = cl.map_shared_rank(&slot[b][crank], q);
-        rs->row[lane] = e;
-      }
-      if (lane < C) {
-        PanelSlot<T, NB> *rs = cl.map_shared_rank(&slot[b][crank], lane);
-        rs->val = v;
-        rs->pos = p;
+      const uint32_t srow = smem_u32(&slot[b][crank].row[lane]);
+      for (int q = 0; q < C; q++) st_async(mapa_u32(srow, q), e, mapa_u32(mb, q));
+      if (lane == 0) {
+        const uint32_t sv = smem_u32(&slot[b][crank].key), sp = smem_u32(&slot[b][crank].pos),
+                       sr = smem_u32(&slot[b][crank].rcp);
+        const T rc = stage[NB];
+        for (int q = 0; q < C; q++) {
+          const uint32_t rm = mapa_u32(mb, q);
+          st_async(mapa_u32(sv, q), v, rm);
+          st_async(mapa_u32(sp, q), (int)p, rm);
+          st_async(mapa_u32(sr, q), rc, rm);
+        }
       }
     }
-    __syncwarp();
-    cluster_arrive();
     return done;
+  };
+  // wait until column c's C messages are in this CTA's slots
+  auto receive = [&](int c) {
+    const uint32_t mb = (c & 1) ? mb1 : mb0, parity = (c >> 1) & 1;
+    if (!mbar_try_wait(mb, parity)) {
+      uint64_t t0, t;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+      while (!mbar_try_wait(mb, parity)) {
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        if (t - t0 > 1000000000ull) { atomicExch(&g_panel_timeout, 1); break; }
+      }
+    }
   };
 
   if (MN > 0) {
     push(0, false);
-    cluster_wait();
+    receive(0);
   }
 #pragma unroll 1
   for (int j = 0; j < MN; j++) {
     const int b = j & 1;
     // the global winner from the C local slots (every warp computes it)
-    T v = lane < C ? slot[b][lane].val : T(-1);
-    int p = lane < C ? slot[b][lane].pos : INT_MAX, w = lane;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) argmax3(v, p, w, o);
+    unsigned long long kv = lane < C ? slot[b][lane].key : 0ull;
+    const unsigned mypos = lane < C ? (unsigned)slot[b][lane].pos : 0xffffffffu;
+    unsigned pu = mypos;
+    const unsigned long long mykey = kv;
+    warp_argmax_key(kv, pu);
+    const int p = (int)pu;
+    const int w = __ffs(__ballot_sync(0xffffffffu, lane < C && mykey == kv && mypos == pu)) - 1;
     __syncwarp();
     wu[warp][lane] = slot[b][w].row[lane];
     __syncwarp();
-    const T piv = wu[warp][0];
+    const T piv = wu[warp][0], prcp = slot[b][w].rcp;
     if (crank == 0 && tid == 0) {
       ipiv[j] = roff + p;
       if (piv == T(0)) atomicMin(dinfo, roff + j + 1);
@@ -385,7 +452,7 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
         // a zero pivot leaves the column unscaled and the row unchanged: the
         // update then runs with l = 0 against a zero row (exact: a - 0*0 = a)
         const bool nz = piv != T(0);
-        const T l = !nz ? a[0] : (fabs(piv) >= safmin<T>() ? a[0] * (T(1) / piv) : a[0] / piv);
+        const T l = !nz ? a[0] : (fabs(piv) >= safmin<T>() ? a[0] * prcp : a[0] / piv);
         lm = nz ? l : T(0);
         u = nz ? wu[warp] : zrow;
         Lsm[j * PT + tid] = l;
@@ -394,46 +461,50 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
       }
     }
     if (j + 1 < MN) {
-      const bool done = push(b ^ 1, owes);
-      if (owes && !done) {
+      const bool done = push(j + 1, owes);
+      if (owes && !done) {  // the rest of the update runs while the messages travel
 #pragma unroll
         for (int k = 2; k < NB; k++) a[k - 1] = fma(-lm, u[k], a[k]);
         a[NB - 1] = T(0);
       }
-      cluster_wait();
+      receive(j + 1);
     }
   }
 
-  // rows to their final positions: the panel's columns from shared memory,
-  // then the block's other columns (through shared memory, 32 at a time, a
-  // cluster barrier between reading all moving rows and writing them)
+  // rows to their final positions: the panel's columns from shared memory;
+  // the block's other columns of the rows that move (at most 2*MN rows) are
+  // staged in shared memory, then written after one cluster barrier
   const bool in = r < M;
   if (in) {
 #pragma unroll 4
     for (int k = 0; k < ncols; k++) A[pos + (long)k * lda] = Lsm[k * PT + tid];
   }
-  const bool moved = in && pos != r;
   const int nother = nleft + nright;
-  for (int c0 = 0; c0 < nother; c0 += NB) {
-    const int nc = min(NB, nother - c0);
-    if (moved) {
-      for (int k = 0; k < nc; k++) {
-        const int c = c0 + k, col = c < nleft ? c - nleft : ncols + (c - nleft);
-        Lsm[k * PT + tid] = __ldcg(A + r + (long)col * lda);
-      }
-    }
-    __syncwarp();
-    cluster_arrive();
-    cluster_wait();
-    if (moved) {
-      for (int k = 0; k < nc; k++) {
-        const int c = c0 + k, col = c < nleft ? c - nleft : ncols + (c - nleft);
-        A[pos + (long)col * lda] = Lsm[k * PT + tid];
-      }
-    }
+  const bool moved = in && pos != r && nother > 0;
+  __syncthreads();  // Lsm is free from here on
+  if (moved) {
+    const int i = atomicAdd(&s_nmoved, 1);
+    if (i < 2 * NB) { s_from[i] = r; s_to[i] = pos; }
+  }
+  __syncthreads();
+  // all threads copy (row, column) pairs of the moving rows: independent
+  // loads, so their latencies overlap
+  const int nm = min(s_nmoved, 2 * NB), total = nm * nother;
+  for (int idx = tid; idx < total; idx += PT) {
+    const int i = idx / nother, c = idx - i * nother;
+    const int col = c < nleft ? c - nleft : ncols + (c - nleft);
+    Lsm[idx] = __ldcg(A + s_from[i] + (long)col * lda);
   }
   __syncwarp();
-  cluster_arrive();  // every row is in place (and no CTA still pushes to this one)
+  cluster_arrive();
+  cluster_wait();
+  for (int idx = tid; idx < total; idx += PT) {
+    const int i = idx / nother, c = idx - i * nother;
+    const int col = c < nleft ? c - nleft : ncols + (c - nleft);
+    A[s_to[i] + (long)col * lda] = Lsm[idx];
+  }
+  __syncwarp();
+  cluster_arrive();  // every row is in place
   cluster_wait();
   // U12 = L11^-1 A12 on the right columns' top MN rows (L11 unit lower)
   if (crank == 0 && nright > 0 && MN > 1) panel_u12_solve<T, NB>(MN, ncols, nright, A, lda, fused_smem);
@@ -593,7 +664,7 @@ int max_cluster_fused() {
 template <typename T>
 bool launch_fused_panel(int M, int ncols, T *A, long lda, int *ipiv, int roff, int *dinfo, int nleft,
                         int nright, cudaStream_t st) {
-  if (ncols > 32) return false;
+  if (ncols > 32 || nleft + nright > 256) return false;  // the interchange staging holds 64 x 256
   const int C = cdiv(M, PT);
   if (C > max_cluster_fused<T>()) return false;
   cudaLaunchConfig_t cfg = {};

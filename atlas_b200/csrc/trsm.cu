@@ -31,6 +31,49 @@ namespace {
 
 constexpr int LEAF = 64;
 
+// One doubling level of the triangular inverse below: for each pair of
+// s x s diagonal blocks (already inverted in sW), the off-diagonal block of
+// the inverse of the 2s x 2s block.
+template <typename T, int s>
+__device__ __forceinline__ void trinv_level(T (*sT)[LEAF + 1], T (*sW)[LEAF + 1], T (*sY)[LEAF + 1],
+                                            int lower, int tid) {
+  constexpr int per = s / 8;  // outputs per thread: (LEAF / 2s) pairs x s x s / 256
+  // Y = T21 W11 (lower) or T12 W22 (upper), stored at the off-diagonal block
+#pragma unroll
+  for (int q = 0; q < per; q++) {
+    const int e = tid + q * 256, p = e / (s * s), rem = e % (s * s), i = rem % s, j = rem / s;
+    const int d1 = 2 * p * s, d2 = d1 + s;  // the pair's two diagonal blocks
+    T acc = T(0);
+    if (lower) {
+#pragma unroll
+      for (int k = 0; k < s; k++) acc = fma(sT[d2 + i][d1 + k], sW[d1 + k][d1 + j], acc);
+      sY[d2 + i][d1 + j] = acc;
+    } else {
+#pragma unroll
+      for (int k = 0; k < s; k++) acc = fma(sT[d1 + i][d2 + k], sW[d2 + k][d2 + j], acc);
+      sY[d1 + i][d2 + j] = acc;
+    }
+  }
+  __syncthreads();
+  // off-diagonal block of the inverse = -W22 Y (lower) or -W11 Y (upper)
+#pragma unroll
+  for (int q = 0; q < per; q++) {
+    const int e = tid + q * 256, p = e / (s * s), rem = e % (s * s), i = rem % s, j = rem / s;
+    const int d1 = 2 * p * s, d2 = d1 + s;
+    T acc = T(0);
+    if (lower) {
+#pragma unroll
+      for (int k = 0; k < s; k++) acc = fma(sW[d2 + i][d2 + k], sY[d2 + k][d1 + j], acc);
+      sW[d2 + i][d1 + j] = -acc;
+    } else {
+#pragma unroll
+      for (int k = 0; k < s; k++) acc = fma(sW[d1 + i][d1 + k], sY[d1 + k][d2 + j], acc);
+      sW[d1 + i][d2 + j] = -acc;
+    }
+  }
+  __syncthreads();
+}
+
 // Invert the 64x64 (or smaller, last) diagonal blocks of the effective
 // triangle T (T(i,k) = Tp[i*tr + k*tc]) into W: block b is stored dense,
 // column-major 64x64 at W + b*64*64, zero outside its triangle (a last block
@@ -50,18 +93,30 @@ trinv_kernel(int n, const T *__restrict__ Tp, long tr, long tc, int lower, int u
   T(*sY)[LEAF + 1] = sW + LEAF;
   const int b = blockIdx.x, r0 = b * LEAF, nb = min(LEAF, n - r0), tid = threadIdx.x;
   const T *Tb = Tp + r0 * tr + r0 * tc;
-  for (int idx = tid; idx < LEAF * LEAF; idx += 256) {
-    int i, k;
-    if (tr == 1) { i = idx % LEAF; k = idx / LEAF; } else { k = idx % LEAF; i = idx / LEAF; }
-    T v;
-    if (i < nb && k < nb) {
-      const bool in_tri = lower ? i > k : i < k;
-      v = (i == k) ? (unit ? T(1) : Tb[i * tr + k * tc]) : (in_tri ? Tb[i * tr + k * tc] : T(0));
-    } else {
-      v = (i == k) ? T(1) : T(0);
+  {
+    T tv[LEAF * LEAF / 256];  // unrolled: all loads of a thread in flight at once
+#pragma unroll
+    for (int q = 0; q < LEAF * LEAF / 256; q++) {
+      const int idx = tid + 256 * q;
+      int i, k;
+      if (tr == 1) { i = idx % LEAF; k = idx / LEAF; } else { k = idx % LEAF; i = idx / LEAF; }
+      T v;
+      if (i < nb && k < nb) {
+        const bool in_tri = lower ? i > k : i < k;
+        v = (i == k) ? (unit ? T(1) : Tb[i * tr + k * tc]) : (in_tri ? Tb[i * tr + k * tc] : T(0));
+      } else {
+        v = (i == k) ? T(1) : T(0);
+      }
+      tv[q] = v;
     }
-    sT[i][k] = v;
-    sW[i][k] = T(0);
+#pragma unroll
+    for (int q = 0; q < LEAF * LEAF / 256; q++) {
+      const int idx = tid + 256 * q;
+      int i, k;
+      if (tr == 1) { i = idx % LEAF; k = idx / LEAF; } else { k = idx % LEAF; i = idx / LEAF; }
+      sT[i][k] = tv[q];
+      sW[i][k] = T(0);
+    }
   }
   __syncthreads();
   // 8x8 diagonal blocks: thread (blk, c) solves for column c of block blk
@@ -89,40 +144,15 @@ trinv_kernel(int n, const T *__restrict__ Tp, long tr, long tc, int lower, int u
     for (int k = 0; k < 8; k++) sW[base + k][base + c] = x[k];
   }
   __syncthreads();
-#pragma unroll 1
-  for (int s = 8; s < LEAF; s *= 2) {
-    const int per = s / 8;  // outputs per thread: (LEAF / 2s) pairs x s x s / 256
-    // Y = T21 W11 (lower) or T12 W22 (upper), stored at the off-diagonal block
-    for (int q = 0; q < per; q++) {
-      const int e = tid + q * 256, p = e / (s * s), rem = e % (s * s), i = rem % s, j = rem / s;
-      const int d1 = 2 * p * s, d2 = d1 + s;  // the pair's two diagonal blocks
-      T acc = T(0);
-      if (lower) {
-        for (int k = 0; k < s; k++) acc = fma(sT[d2 + i][d1 + k], sW[d1 + k][d1 + j], acc);
-        sY[d2 + i][d1 + j] = acc;
-      } else {
-        for (int k = 0; k < s; k++) acc = fma(sT[d1 + i][d2 + k], sW[d2 + k][d2 + j], acc);
-        sY[d1 + i][d2 + j] = acc;
-      }
-    }
-    __syncthreads();
-    // off-diagonal block of the inverse = -W22 Y (lower) or -W11 Y (upper)
-    for (int q = 0; q < per; q++) {
-      const int e = tid + q * 256, p = e / (s * s), rem = e % (s * s), i = rem % s, j = rem / s;
-      const int d1 = 2 * p * s, d2 = d1 + s;
-      T acc = T(0);
-      if (lower) {
-        for (int k = 0; k < s; k++) acc = fma(sW[d2 + i][d2 + k], sY[d2 + k][d1 + j], acc);
-        sW[d2 + i][d1 + j] = -acc;
-      } else {
-        for (int k = 0; k < s; k++) acc = fma(sW[d1 + i][d1 + k], sY[d1 + k][d2 + j], acc);
-        sW[d1 + i][d2 + j] = -acc;
-      }
-    }
-    __syncthreads();
-  }
+  trinv_level<T, 8>(sT, sW, sY, lower, tid);
+  trinv_level<T, 16>(sT, sW, sY, lower, tid);
+  trinv_level<T, 32>(sT, sW, sY, lower, tid);
   T *Wb = W + (long)b * LEAF * LEAF;
-  for (int idx = tid; idx < LEAF * LEAF; idx += 256) Wb[idx] = sW[idx % LEAF][idx / LEAF];
+#pragma unroll
+  for (int q = 0; q < LEAF * LEAF / 256; q++) {
+    const int idx = tid + 256 * q;
+    Wb[idx] = sW[idx % LEAF][idx / LEAF];
+  }
 }
 
 // B_blk (nb x m, effective strides) = W_b (nb x nb) * B_blk, in place: one
@@ -135,14 +165,27 @@ tri_apply_kernel(int nb, int m, const T *__restrict__ Wb, T *__restrict__ Bp, lo
   T(*sB)[LEAF + 1] = sW + LEAF;
   const int j0 = blockIdx.x * LEAF, tid = threadIdx.x;
   const int mcols = min(LEAF, m - j0);
-  for (int idx = tid; idx < LEAF * LEAF; idx += 256) {
-    int i = idx % LEAF, k = idx / LEAF;
-    sW[i][k] = (i < nb && k < nb) ? Wb[i + (long)k * LEAF] : T(0);
+  // fixed trip counts, unrolled: all 32 loads of a thread are in flight at once
+  T wv[LEAF * LEAF / 256], bv[LEAF * LEAF / 256];
+#pragma unroll
+  for (int q = 0; q < LEAF * LEAF / 256; q++) {
+    const int idx = tid + 256 * q, i = idx % LEAF, k = idx / LEAF;
+    wv[q] = (i < nb && k < nb) ? Wb[i + (long)k * LEAF] : T(0);
   }
-  for (int idx = tid; idx < LEAF * LEAF; idx += 256) {
+#pragma unroll
+  for (int q = 0; q < LEAF * LEAF / 256; q++) {
+    const int idx = tid + 256 * q;
     int i, j;
     if (br == 1) { i = idx % LEAF; j = idx / LEAF; } else { j = idx % LEAF; i = idx / LEAF; }
-    sB[i][j] = (i < nb && j < mcols) ? Bp[i * br + (long)(j0 + j) * bc] : T(0);
+    bv[q] = (i < nb && j < mcols) ? Bp[i * br + (long)(j0 + j) * bc] : T(0);
+  }
+#pragma unroll
+  for (int q = 0; q < LEAF * LEAF / 256; q++) {
+    const int idx = tid + 256 * q;
+    sW[idx % LEAF][idx / LEAF] = wv[q];
+    int i, j;
+    if (br == 1) { i = idx % LEAF; j = idx / LEAF; } else { j = idx % LEAF; i = idx / LEAF; }
+    sB[i][j] = bv[q];
   }
   __syncthreads();
   const int r = tid % LEAF, cg = tid / LEAF;  // 4 column groups
