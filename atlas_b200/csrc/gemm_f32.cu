@@ -4,6 +4,7 @@
 // k-major (m / n contiguous) by a 3-stage cp.async pipeline, whatever their
 // global layout, so the inner loop reads 128-bit vectors.
 // Reference semantics: src/blas/reference/level3/ATL_srefgemm.c.
+#include <cstdint>
 #include "common.cuh"
 #include "kernels.h"
 
@@ -87,20 +88,64 @@ sgemm_simt_kernel(int M, int N, int K, float alpha, const float *__restrict__ A,
     }
   }
   cp_async_wait<0>();
+  // epilogue: each thread owns rows {ty*4 .. +3, 64 + ty*4 .. +3} x columns
+  // {tx*4 .. +3, 64 + tx*4 .. +3}; a row quad of one column is contiguous in C.
+  // All old C values are loaded before any store, so the loads overlap.
+  const bool vec = tri == 0 && ((uintptr_t)C % 16 == 0) && (ldc % 4 == 0) && m0 + BM <= M && n0 + BN <= N;
+  if (vec) {
 #pragma unroll
-  for (int i = 0; i < 8; i++) {
-    int r = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + i - 4);
-    if (r >= M) continue;
+    for (int jh = 0; jh < 8; jh += 4) {  // two rounds of 8 float4 loads, then their stores
+      float4 cv[4][2];
 #pragma unroll
-    for (int j = 0; j < 8; j++) {
-      int c = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + j - 4);
-      if (c >= N) continue;
+      for (int jj = 0; jj < 4; jj++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int j = jh + jj;
+          const int c = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + j - 4), r = m0 + h * 64 + ty * 4;
+          cv[jj][h] = beta != 0.f ? *reinterpret_cast<const float4 *>(C + r + (long)c * ldc)
+                                  : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+      for (int jj = 0; jj < 4; jj++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int j = jh + jj;
+          const int c = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + j - 4), r = m0 + h * 64 + ty * 4;
+          float4 o;
+          o.x = alpha * acc[h * 4 + 0][j];
+          o.y = alpha * acc[h * 4 + 1][j];
+          o.z = alpha * acc[h * 4 + 2][j];
+          o.w = alpha * acc[h * 4 + 3][j];
+          if (beta != 0.f) {
+            o.x = fmaf(beta, cv[jj][h].x, o.x);
+            o.y = fmaf(beta, cv[jj][h].y, o.y);
+            o.z = fmaf(beta, cv[jj][h].z, o.z);
+            o.w = fmaf(beta, cv[jj][h].w, o.w);
+          }
+          *reinterpret_cast<float4 *>(C + r + (long)c * ldc) = o;
+        }
+    }
+    return;
+  }
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    const int c = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + j - 4);
+    float cv[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int r = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + i - 4);
+      const bool ok = r < M && c < N && !(tri == 1 && r < c) && !(tri == 2 && r > c);
+      cv[i] = (ok && beta != 0.f) ? C[r + (long)c * ldc] : 0.f;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int r = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + i - 4);
+      if (r >= M || c >= N) continue;
       if (tri == 1 && r < c) continue;
       if (tri == 2 && r > c) continue;
-      float *p = C + r + (long)c * ldc;
       float v = alpha * acc[i][j];
-      if (beta != 0.f) v = fmaf(beta, *p, v);
-      *p = v;
+      if (beta != 0.f) v = fmaf(beta, cv[i], v);
+      C[r + (long)c * ldc] = v;
     }
   }
 }

@@ -212,7 +212,8 @@ template <typename T, int NB>
 struct PanelSlot {
   T row[NB];
   unsigned long long key;  // pivot_key of the candidate
-  T rcp;                   // 1 / row[0], computed by the sender off the critical path
+  T rcp;                   // 1 / (candidate value), computed by the sender off the critical path
+  T lm;                    // the sender's pending multiplier: the row is row - lm * u (see below)
   int pos;
 };
 
@@ -310,7 +311,7 @@ __global__ void __launch_bounds__(PT, 1)
 getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restrict__ ipiv, int roff,
                    int *__restrict__ dinfo, int nleft, int nright) {
   static_assert(NB == 32, "one pivot-row element per lane");
-  constexpr uint32_t kMsg = NB * sizeof(T) + 8 + sizeof(T) + sizeof(int);  // bytes one CTA sends one CTA
+  constexpr uint32_t kMsg = NB * sizeof(T) + 8 + 2 * sizeof(T) + sizeof(int);  // bytes one CTA sends one CTA
   cg::cluster_group cl = cg::this_cluster();
   const int C = (int)cl.num_blocks(), crank = (int)cl.block_rank();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -320,7 +321,7 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
   __shared__ PanelSlot<T, NB> slot[2][kMaxPanelCluster];
   __shared__ __align__(8) unsigned long long mbar[2];
   __shared__ __align__(16) T wu[PT / 32][NB];  // per-warp copy of the pivot row
-  __shared__ __align__(16) T stage[NB + 1];    // the CTA winner's row and 1/row[0], for the push
+  __shared__ __align__(16) T stage[NB + 2];    // the CTA winner's message: row, 1/value, lm
   __shared__ T zrow[NB];
   __shared__ unsigned long long wv[2][PT / 32];   // per-warp candidates, by column parity
   __shared__ unsigned wp[2][PT / 32];
@@ -353,14 +354,18 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
   T lm = T(0);
   const T *u = zrow;
 
-  // Reduce this CTA's candidates (|a[0]| of active rows); the winner first
-  // finishes its row (when it still owes the update), then its warp sends
-  // (row, |value|, position) for column c to every CTA's slot.
-  auto push = [&](int c, bool owes_tail) {
+  // Reduce this CTA's candidates (|a[0]| of active rows) and let the
+  // winner's warp send its row for column c to every CTA's slot.  Inside the
+  // column loop the winner has updated only a[0] (the candidate itself): it
+  // sends its other entries as they are, shifted, with its multiplier lm, and
+  // the receivers finish the update (row[k] - lm * u[k+1]) themselves, so the
+  // message leaves before the sender's own row update.
+  auto push = [&](int c, bool shifted) {
     const int b = c & 1;
     const uint32_t mb = b ? mb1 : mb0;
     if (tid == 0)
       asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(kMsg * C) : "memory");
+    const T rc = act ? T(1) / a[0] : T(0);  // needed only by the winner; overlaps the reductions
     unsigned long long v = act ? pivot_key(a[0]) : 0ull;
     unsigned p = act ? (unsigned)pos : 0xffffffffu;
     warp_argmax_key(v, p);
@@ -370,17 +375,18 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
     p = lane < PT / 32 ? wp[b][lane] : 0xffffffffu;
     warp_argmax_key(v, p);
     const bool owner = act && (unsigned)pos == p;
-    bool done = false;
     if (owner) {
-      if (owes_tail) {
+      if (shifted) {
 #pragma unroll
-        for (int k = 2; k < NB; k++) a[k - 1] = fma(-lm, u[k], a[k]);
-        a[NB - 1] = T(0);
-        done = true;
+        for (int k = 0; k < NB - 1; k++) stage[k] = a[k + 1];
+        stage[NB - 1] = T(0);
+        stage[NB + 1] = lm;
+      } else {
+#pragma unroll
+        for (int k = 0; k < NB; k++) stage[k] = a[k];
+        stage[NB + 1] = T(0);
       }
-#pragma unroll
-      for (int k = 0; k < NB; k++) stage[k] = a[k];
-      stage[NB] = T(1) / a[0];
+      stage[NB] = rc;
     }
     const bool mine = __any_sync(0xffffffffu, owner) || (p == 0xffffffffu && warp == 0);
     if (mine) {
@@ -390,17 +396,17 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
       for (int q = 0; q < C; q++) st_async(mapa_u32(srow, q), e, mapa_u32(mb, q));
       if (lane == 0) {
         const uint32_t sv = smem_u32(&slot[b][crank].key), sp = smem_u32(&slot[b][crank].pos),
-                       sr = smem_u32(&slot[b][crank].rcp);
-        const T rc = stage[NB];
+                       sr = smem_u32(&slot[b][crank].rcp), sl = smem_u32(&slot[b][crank].lm);
+        const T rcs = stage[NB], lms = stage[NB + 1];
         for (int q = 0; q < C; q++) {
           const uint32_t rm = mapa_u32(mb, q);
           st_async(mapa_u32(sv, q), v, rm);
           st_async(mapa_u32(sp, q), (int)p, rm);
-          st_async(mapa_u32(sr, q), rc, rm);
+          st_async(mapa_u32(sr, q), rcs, rm);
+          st_async(mapa_u32(sl, q), lms, rm);
         }
       }
     }
-    return done;
   };
   // wait until column c's C messages are in this CTA's slots
   auto receive = [&](int c) {
@@ -419,6 +425,7 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
     push(0, false);
     receive(0);
   }
+  bool nz_prev = false;  // pivot of the previous column non-zero (its row is then the update row)
 #pragma unroll 1
   for (int j = 0; j < MN; j++) {
     const int b = j & 1;
@@ -430,15 +437,21 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
     warp_argmax_key(kv, pu);
     const int p = (int)pu;
     const int w = __ffs(__ballot_sync(0xffffffffu, lane < C && mykey == kv && mypos == pu)) - 1;
-    __syncwarp();
-    wu[warp][lane] = slot[b][w].row[lane];
-    __syncwarp();
+    {
+      // finish the winner's update with the previous column's pivot row
+      const T *uprev = nz_prev ? wu[warp] : zrow;
+      const T up = lane < NB - 1 ? uprev[lane + 1] : T(0);
+      const T nv = fma(-slot[b][w].lm, up, slot[b][w].row[lane]);
+      __syncwarp();
+      wu[warp][lane] = nv;
+      __syncwarp();
+    }
     const T piv = wu[warp][0], prcp = slot[b][w].rcp;
+    nz_prev = piv != T(0);
     if (crank == 0 && tid == 0) {
       ipiv[j] = roff + p;
       if (piv == T(0)) atomicMin(dinfo, roff + j + 1);
     }
-    bool owes = false;
     if (act) {
       if (pos == p) {  // this row becomes row j of U: its remaining part is final
         act = false;
@@ -457,12 +470,12 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
         u = nz ? wu[warp] : zrow;
         Lsm[j * PT + tid] = l;
         a[0] = fma(-lm, u[1], a[1]);  // the next column first: it decides the next pivot
-        owes = j + 1 < MN;
       }
     }
     if (j + 1 < MN) {
-      const bool done = push(j + 1, owes);
-      if (owes && !done) {  // the rest of the update runs while the messages travel
+      const bool upd = act;  // active rows (the pivot row has just left) owe the rest of the update
+      push(j + 1, true);
+      if (upd) {  // it runs while the messages travel
 #pragma unroll
         for (int k = 2; k < NB; k++) a[k - 1] = fma(-lm, u[k], a[k]);
         a[NB - 1] = T(0);
@@ -479,29 +492,55 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
 #pragma unroll 4
     for (int k = 0; k < ncols; k++) A[pos + (long)k * lda] = Lsm[k * PT + tid];
   }
+  // The block's other columns of the rows that moved (at most 2*MN rows,
+  // most of them in CTA 0, whose rows include the top of the panel): the
+  // list of moves is gathered in CTA 0, and every CTA copies an equal share
+  // of the (move, column) pairs through its shared memory, with a cluster
+  // barrier between all reads and all writes.
   const int nother = nleft + nright;
-  const bool moved = in && pos != r && nother > 0;
   __syncthreads();  // Lsm is free from here on
-  if (moved) {
-    const int i = atomicAdd(&s_nmoved, 1);
-    if (i < 2 * NB) { s_from[i] = r; s_to[i] = pos; }
-  }
-  __syncthreads();
-  // all threads copy (row, column) pairs of the moving rows: independent
-  // loads, so their latencies overlap
-  const int nm = min(s_nmoved, 2 * NB), total = nm * nother;
-  for (int idx = tid; idx < total; idx += PT) {
-    const int i = idx / nother, c = idx - i * nother;
-    const int col = c < nleft ? c - nleft : ncols + (c - nleft);
-    Lsm[idx] = __ldcg(A + s_from[i] + (long)col * lda);
+  if (nother > 0 && in && pos != r) {
+    int *cnt0 = cl.map_shared_rank(&s_nmoved, 0);
+    const int i = atomicAdd(cnt0, 1);
+    if (i < 2 * NB) {
+      cl.map_shared_rank(s_from, 0)[i] = r;
+      cl.map_shared_rank(s_to, 0)[i] = pos;
+    }
   }
   __syncwarp();
   cluster_arrive();
   cluster_wait();
-  for (int idx = tid; idx < total; idx += PT) {
-    const int i = idx / nother, c = idx - i * nother;
+  __shared__ int l_from[2 * NB], l_to[2 * NB];
+  const int nm = nother > 0 ? min(*cl.map_shared_rank(&s_nmoved, 0), 2 * NB) : 0;
+  if (tid < nm) {
+    l_from[tid] = cl.map_shared_rank(s_from, 0)[tid];
+    l_to[tid] = cl.map_shared_rank(s_to, 0)[tid];
+  }
+  __syncthreads();
+  const int total = nm * nother, per = (total + C - 1) / C;
+  const int g0 = crank * per, g1 = min(total, g0 + per);
+  for (int base = g0 + tid; base < g1; base += 4 * PT) {
+    T v[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int g = base + q * PT;
+      if (g < g1) {
+        const int i = g / nother, c = g - i * nother;
+        const int col = c < nleft ? c - nleft : ncols + (c - nleft);
+        v[q] = __ldcg(A + l_from[i] + (long)col * lda);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      if (base + q * PT < g1) Lsm[base + q * PT - g0] = v[q];
+  }
+  __syncwarp();
+  cluster_arrive();
+  cluster_wait();
+  for (int g = g0 + tid; g < g1; g += PT) {
+    const int i = g / nother, c = g - i * nother;
     const int col = c < nleft ? c - nleft : ncols + (c - nleft);
-    A[s_to[i] + (long)col * lda] = Lsm[idx];
+    A[l_to[i] + (long)col * lda] = Lsm[g - g0];
   }
   __syncwarp();
   cluster_arrive();  // every row is in place

@@ -186,10 +186,26 @@ void symmetrize_dev(int uplo, int N, const double *A, long lda, double *F, long 
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
 
+// The factorization's GEMMs: the tensor-core paths pay an operand
+// conversion pass per call, which only large updates (the block trailing
+// updates, K >= 256) amortize; the small updates inside a block column run
+// as plain FP32 FMA GEMMs (more accurate than the tensor-core formats, so the
+// factorization is at least as accurate as with the tensor cores alone).
+constexpr long kTcMinWork = 1L << 31;  // M*N*K below which FP32 FMA is used
+template <void (*TC)(int, int, int, int, int, float, const float *, long, const float *, long, float,
+                     float *, long, cudaStream_t, int)>
+void sgemm_by_size(int ta, int tb, int M, int N, int K, float alpha, const float *A, long lda,
+                   const float *B, long ldb, float beta, float *C, long ldc, cudaStream_t st, int tri) {
+  if (K < 128 || (long)M * N * K < kTcMinWork)
+    sgemm_dev(ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, st, tri);
+  else
+    TC(ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, st, tri);
+}
+
 SgemmFn factor_gemm(int prec) {
-  if (prec == kPrecTF32) return sgemm_tf32_dev;
-  if (prec == kPrecBF16) return sgemm_bf16_dev;
-  if (prec == kPrecTF32x3) return sgemm_tf32x3_dev;
+  if (prec == kPrecTF32) return sgemm_by_size<sgemm_tf32_dev>;
+  if (prec == kPrecBF16) return sgemm_by_size<sgemm_bf16_dev>;
+  if (prec == kPrecTF32x3) return sgemm_by_size<sgemm_tf32x3_dev>;
   return sgemm_dev;
 }
 
