@@ -209,21 +209,38 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       uint32_t r[32];
       tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + c * 32, r);
       if (m < M) {
+        // all 32 old values of C first (independent loads, latencies overlap),
+        // then the 32 results: the loads are not serialized behind the stores
+        const int n1 = n0 + c * 32;
+        if (EPI == kEpiF32) {
+          float old[32];
 #pragma unroll
-        for (int i = 0; i < 32; i++) {
-          const int n = n0 + c * 32 + i;
-          if (n >= N) break;
-          if (EPI == kEpiF32) {
-            if (ep.tri == 1 && m < n) continue;
-            if (ep.tri == 2 && m > n) continue;
-            float *p = ep.Cf + m + (long)n * ep.ldc;
+          for (int i = 0; i < 32; i++) {
+            const int n = n1 + i;
+            const bool ok = n < N && !(ep.tri == 1 && m < n) && !(ep.tri == 2 && m > n);
+            old[i] = (ok && ep.beta != 0.f) ? ep.Cf[m + (long)n * ep.ldc] : 0.f;
+          }
+#pragma unroll
+          for (int i = 0; i < 32; i++) {
+            const int n = n1 + i;
+            const bool ok = n < N && !(ep.tri == 1 && m < n) && !(ep.tri == 2 && m > n);
+            if (!ok) continue;
             float v = ep.alpha * __uint_as_float(r[i]);
-            if (ep.beta != 0.f) v = fmaf(ep.beta, *p, v);
-            *p = v;
-          } else {
-            double *p = ep.Cd + m + (long)n * ep.ldc;
-            const double w = ep.w * ep.rs[m] * ep.cs[n];
-            *p = fma(w, (double)(int)r[i], *p);
+            if (ep.beta != 0.f) v = fmaf(ep.beta, old[i], v);
+            ep.Cf[m + (long)n * ep.ldc] = v;
+          }
+        } else {
+          const double wr = ep.w * ep.rs[m];
+          double old[32];
+#pragma unroll
+          for (int i = 0; i < 32; i++) {
+            const int n = n1 + i;
+            old[i] = n < N ? ep.Cd[m + (long)n * ep.ldc] : 0.0;
+          }
+#pragma unroll
+          for (int i = 0; i < 32; i++) {
+            const int n = n1 + i;
+            if (n < N) ep.Cd[m + (long)n * ep.ldc] = fma(wr * ep.cs[n], (double)(int)r[i], old[i]);
           }
         }
       }

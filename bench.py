@@ -32,6 +32,8 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -189,6 +191,272 @@ def timed(torch, stream, fn, reps):
     e1.record(stream)
     torch.cuda.synchronize()
     return e0.elapsed_time(e1) / reps
+
+
+def extra_factorizations(torch, AB, dev, stream):
+    """The FP64 factorization configurations: dgetrf+dgetrs N=8192 with 16
+    right-hand sides on A = G/sqrt(N) + 4I, dpotrf+dpotrs N=8192 on
+    A = G G^T/N + I, dgeqrf on a 16384 x 8192 Gaussian matrix."""
+    f64 = torch.float64
+    res = {}
+    n, nrhs = 8192, 16
+    g = torch.Generator(device=dev)
+    g.manual_seed(11)
+    a0 = torch.randn(n, n, dtype=f64, device=dev, generator=g) / n ** 0.5
+    a0 += 4.0 * torch.eye(n, dtype=f64, device=dev)
+    b0 = torch.rand(nrhs, n, dtype=f64, device=dev, generator=g) * 2 - 1    # column-major n x nrhs
+    A, B = torch.empty_like(a0), torch.empty_like(b0)
+    ipiv = torch.zeros(n, dtype=torch.int32, device=dev)
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def lu():
+        A.copy_(a0)
+        B.copy_(b0)
+        AB.atlb_dgetrf_dev(n, n, A, n, ipiv, info)
+        AB.atlb_dgetrs_dev(111, n, nrhs, A, n, ipiv, B, n)
+    lu()
+    lu()
+    ms = timed(torch, stream, lu, 3)
+    flop = 2.0 / 3.0 * n ** 3 + 2.0 * n ** 2 * nrhs
+    x = B.T                                   # logical n x nrhs
+    r = b0.T - a0.T @ x
+    resid = (r.abs().max() / (a0.abs().sum(0).max() * x.abs().max() * n * 2.0 ** -53)).item()
+    res["dgetrf_dgetrs_8192_16rhs"] = {
+        "ms": ms, "gflops": flop / ms / 1e6, "info": int(info.item()),
+        "ipiv_identity": bool((ipiv == torch.arange(n, device=dev, dtype=torch.int32)).all().item()),
+        "solve_residual_over_n_eps": resid}
+    # Cholesky
+    gm = torch.randn(n, n, dtype=f64, device=dev, generator=g)
+    s0 = gm @ gm.T / n + torch.eye(n, dtype=f64, device=dev)
+    del gm
+
+    def ch():
+        A.copy_(s0)
+        B.copy_(b0)
+        AB.atlb_dpotrf_dev(122, n, A, n, info)
+        AB.atlb_dpotrs_dev(122, n, nrhs, A, n, B, n)
+    ch()
+    ch()
+    ms = timed(torch, stream, ch, 3)
+    flop = n ** 3 / 3.0 + 2.0 * n ** 2 * nrhs
+    x = B.T
+    r = b0.T - s0 @ x
+    resid = (r.abs().max() / (s0.abs().sum(0).max() * x.abs().max() * n * 2.0 ** -53)).item()
+    res["dpotrf_dpotrs_8192_16rhs"] = {"ms": ms, "gflops": flop / ms / 1e6, "info": int(info.item()),
+                                       "solve_residual_over_n_eps": resid}
+    del s0, A, B, a0, b0
+    # QR
+    m, nq = 16384, 8192
+    q0 = torch.randn(nq, m, dtype=f64, device=dev, generator=g)             # column-major m x n
+    Q = torch.empty_like(q0)
+    tau = torch.empty(nq, dtype=f64, device=dev)
+
+    def qr():
+        Q.copy_(q0)
+        AB.atlb_dgeqrf_dev(m, nq, Q, m, tau)
+    qr()
+    ms = timed(torch, stream, qr, 2)
+    flop = 2.0 * m * nq ** 2 - 2.0 / 3.0 * nq ** 3
+    res["dgeqrf_16384x8192"] = {"ms": ms, "gflops": flop / ms / 1e6}
+    del q0, Q
+    torch.cuda.empty_cache()
+    return res
+
+
+def extra_kappa(torch, AB, dev, stream, n):
+    """Mixed solver at kappa = 1e6: iterations (or FP64 fallback) per precision."""
+    acol, b = make_system(torch, n, 1e6, 4321, dev)
+    a0 = acol.clone()
+    x = torch.empty_like(b)
+    ipiv = torch.empty(n, dtype=torch.int32, device=dev)
+    it = np.zeros(1, dtype=np.int32)
+    res = {}
+    for name, prec in (("fp32", 0), ("tf32x3", 3), ("bf16", 2)):
+        def call():
+            AB.atlb_dsgesv_ex(n, 1, acol, n, ipiv, b, n, x, n, prec, 0, it)
+            if it[0] < 0:
+                acol.copy_(a0)
+        call()
+        ms = timed(torch, stream, call, 2)
+        res[name] = {"ms": ms, "iter": int(it[0]), "backward_error": backward_error(torch, a0, x, b)}
+    del acol, a0
+    return res
+
+
+def extra_batched(torch, AB, dev, stream):
+    """10,000 SPD systems (n in [8,256], 4 RHS), 10,000 LU solves, 50,000 uneven
+    DGEMMs (M,N,K in [16,512]): one launch per batch, against a per-instance
+    loop of the plain kernels on a sample of the same problems."""
+    import ctypes
+    f64 = torch.float64
+    rng = np.random.default_rng(2024)
+    res = {}
+
+    def ptrs(ts):
+        return (ctypes.c_void_p * len(ts))(*[t.data_ptr() for t in ts])
+
+    count = 10000
+    ns = rng.integers(8, 257, count).astype(np.int32)
+    g = torch.Generator(device=dev)
+    g.manual_seed(5)
+    # SPD A = B B^T + n I, generated per distinct size in batches
+    As, Bs, A0s = [None] * count, [None] * count, [None] * count
+    for n in np.unique(ns):
+        idx = np.nonzero(ns == n)[0]
+        gb = torch.randn(len(idx), n, n, dtype=f64, device=dev, generator=g)
+        sp = gb @ gb.transpose(1, 2) + n * torch.eye(n, dtype=f64, device=dev)
+        rh = torch.rand(len(idx), 4, n, dtype=f64, device=dev, generator=g) * 2 - 1
+        for j, i in enumerate(idx):
+            A0s[i] = sp[j]
+            Bs[i] = rh[j]
+    nr = np.full(count, 4, dtype=np.int32)
+    info = np.zeros(count, dtype=np.int32)
+    work = [a.clone() for a in A0s]
+    rhs0 = [b.clone() for b in Bs]
+
+    def posv():
+        return AB.atlb_dposv_batched(count, ns, ptrs(work), ns, ptrs(Bs), ns, nr, info)
+    # restore inputs outside the timed region, one timed launch at a time
+    ts = []
+    for rep in range(3):
+        for w, a in zip(work, A0s):
+            w.copy_(a)
+        for b, b0 in zip(Bs, rhs0):
+            b.copy_(b0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        assert posv() == 0
+        torch.cuda.synchronize()
+        ts.append(time.perf_counter() - t0)
+    flop = float(np.sum(ns.astype(np.float64) ** 3 / 3 + 2.0 * ns.astype(np.float64) ** 2 * 4))
+    batch_ms = min(ts[1:]) * 1e3
+    sample = 300
+    info_d = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def loop():
+        for i in range(sample):
+            n = int(ns[i])
+            AB.atlb_dpotrf_dev(122, n, work[i], n, info_d)
+            AB.atlb_dpotrs_dev(122, n, 4, work[i], n, Bs[i], n)
+    for w, a in zip(work[:sample], A0s[:sample]):
+        w.copy_(a)
+    loop()
+    loop_ms = timed(torch, stream, loop, 1) * count / sample
+    res["posv_10k"] = {"ms_one_launch": batch_ms, "gflops": flop / batch_ms / 1e6, "all_info_zero": bool((info == 0).all()),
+                       "ms_per_instance_loop_scaled": loop_ms, "loop_sample": sample,
+                       "speedup_vs_loop": loop_ms / batch_ms, "timing": "wall clock around the synchronous call"}
+    del work, rhs0, A0s
+    # LU solves: A = G/sqrt(n) + 4I, 1 RHS
+    A0s, work = [None] * count, [None] * count
+    for n in np.unique(ns):
+        idx = np.nonzero(ns == n)[0]
+        ga = torch.randn(len(idx), n, n, dtype=f64, device=dev, generator=g) / float(n) ** 0.5
+        ga += 4.0 * torch.eye(n, dtype=f64, device=dev)
+        for j, i in enumerate(idx):
+            A0s[i] = ga[j]
+    work = [a.clone() for a in A0s]
+    rh = [torch.ones(1, int(n), dtype=f64, device=dev) for n in ns]
+    piv = [torch.zeros(int(n), dtype=torch.int32, device=dev) for n in ns]
+    one = np.ones(count, dtype=np.int32)
+    ts = []
+    for rep in range(3):
+        for w, a in zip(work, A0s):
+            w.copy_(a)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        assert AB.atlb_dgesv_batched(count, ns, ptrs(work), ns, ptrs(piv), ptrs(rh), ns, one, info) == 0
+        torch.cuda.synchronize()
+        ts.append(time.perf_counter() - t0)
+    batch_ms = min(ts[1:]) * 1e3
+    flop = float(np.sum(2.0 / 3.0 * ns.astype(np.float64) ** 3 + 2.0 * ns.astype(np.float64) ** 2))
+
+    def loop2():
+        for i in range(sample):
+            n = int(ns[i])
+            AB.atlb_dgetrf_dev(n, n, work[i], n, piv[i], info_d)
+            AB.atlb_dgetrs_dev(111, n, 1, work[i], n, piv[i], rh[i], n)
+    loop2()
+    loop_ms = timed(torch, stream, loop2, 1) * count / sample
+    res["gesv_10k"] = {"ms_one_launch": batch_ms, "gflops": flop / batch_ms / 1e6, "all_info_zero": bool((info == 0).all()),
+                       "ms_per_instance_loop_scaled": loop_ms, "loop_sample": sample,
+                       "speedup_vs_loop": loop_ms / batch_ms, "timing": "wall clock around the synchronous call"}
+    del work, A0s, rh, piv
+    torch.cuda.empty_cache()
+    # 50,000 uneven DGEMMs: operands are sub-blocks of two shared 512 x 512 matrices, C distinct
+    cnt = 50000
+    M = rng.integers(16, 513, cnt).astype(np.int32)
+    N = rng.integers(16, 513, cnt).astype(np.int32)
+    K = rng.integers(16, 513, cnt).astype(np.int32)
+    abig = torch.rand(512, 512, dtype=f64, device=dev, generator=g) * 2 - 1
+    bbig = torch.rand(512, 512, dtype=f64, device=dev, generator=g) * 2 - 1
+    sizes = M.astype(np.int64) * N.astype(np.int64)
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    cbuf = torch.zeros(int(offs[-1]), dtype=f64, device=dev)
+    base = cbuf.data_ptr()
+    cp = (ctypes.c_void_p * cnt)(*[base + 8 * int(o) for o in offs[:-1]])
+    ap = (ctypes.c_void_p * cnt)(*([abig.data_ptr()] * cnt))
+    bp = (ctypes.c_void_p * cnt)(*([bbig.data_ptr()] * cnt))
+    ld = np.full(cnt, 512, dtype=np.int32)
+
+    def grouped():
+        return AB.atlb_dgemm_batched_dev(111, 111, cnt, M, N, K, 1.0, ap, ld, bp, ld, 0.0, cp, M)
+    grouped()
+    torch.cuda.synchronize()
+    ts = []
+    for rep in range(3):
+        t0 = time.perf_counter()
+        grouped()
+        torch.cuda.synchronize()
+        ts.append(time.perf_counter() - t0)
+    batch_ms = min(ts) * 1e3
+    flop = float(np.sum(2.0 * M.astype(np.float64) * N * K))
+    sample = 2000
+
+    def loop3():
+        for i in range(sample):
+            AB.atlb_dgemm_dev(111, 111, int(M[i]), int(N[i]), int(K[i]), 1.0, abig, 512, bbig, 512, 0.0,
+                              base + 8 * int(offs[i]), int(M[i]))
+    loop3()
+    loop_ms = timed(torch, stream, loop3, 1) * cnt / sample
+    res["dgemm_50k"] = {"ms_one_launch": batch_ms, "gflops": flop / batch_ms / 1e6,
+                        "ms_per_instance_loop_scaled": loop_ms, "loop_sample": sample,
+                        "speedup_vs_loop": loop_ms / batch_ms, "timing": "wall clock around the synchronous call"}
+    del cbuf, abig, bbig
+    torch.cuda.empty_cache()
+    return res
+
+
+def extra_adjoints(torch, AB, dev, stream):
+    """Gaussian-likelihood loss adjoint at N=4096 (potrf/potrs adjoints) and
+    the getrs adjoint, FP64; time of forward + adjoint."""
+    f64 = torch.float64
+    n = 4096
+    g = torch.Generator(device=dev)
+    g.manual_seed(3)
+    bm = torch.randn(n, n, dtype=f64, device=dev, generator=g)
+    a = bm @ bm.T / n + torch.eye(n, dtype=f64, device=dev)
+    del bm
+    y = torch.rand(n, dtype=f64, device=dev, generator=g) * 2 - 1
+    L, x = torch.empty_like(a), torch.empty_like(y)
+    Lbar, Abar, Bbar = torch.zeros_like(a), torch.zeros_like(a), torch.empty_like(y)
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def fwd_bwd():
+        L.copy_(a)
+        x.copy_(y)
+        AB.atlb_dpotrf_dev(122, n, L, n, info)
+        AB.atlb_dpotrs_dev(122, n, 1, L, n, x, n)
+        Lbar.zero_()
+        Lbar.view(-1)[:: n + 1] = 2.0 / L.view(-1)[:: n + 1]
+        AB.atlb_dpotrf_adjoint_dev(n, L, n, Lbar, n, Abar, n)
+        AB.atlb_dpotrs_adjoint_dev(n, 1, L, n, x, n, y, n, Bbar, n, Abar, n)
+    fwd_bwd()
+    ms = timed(torch, stream, fwd_bwd, 3)
+    ainv = torch.linalg.inv(a)
+    av = ainv @ y
+    closed = ainv - torch.outer(av, av)
+    err = ((Abar - closed).abs().max() / closed.abs().max()).item()
+    return {"gaussian_loss_4096": {"ms_forward_plus_adjoint": ms, "rel_err_vs_closed_form": err}}
 
 
 def main():
@@ -359,6 +627,11 @@ def main():
                                  "speedup_vs_dmma_dgemm": dgemm_ms / t_ms}
         out["ozaki_8192"] = oz
         del gc, oa, ob
+        torch.cuda.empty_cache()
+        out["fp64_factorizations"] = extra_factorizations(torch, AB, dev, stream)
+        out["mixed_kappa_1e6"] = extra_kappa(torch, AB, dev, stream, n)
+        out["batched"] = extra_batched(torch, AB, dev, stream)
+        out["adjoints"] = extra_adjoints(torch, AB, dev, stream)
 
     # ---- end to end through the C ABI with pinned host buffers (H2D of A and b,
     # D2H of x inside the timed region)
