@@ -31,6 +31,7 @@ PREC_FP32, PREC_TF32, PREC_BF16, PREC_TF32X3 = 0, 1, 2, 3
 _lib = None
 
 _I, _D, _F, _P = ctypes.c_int, ctypes.c_double, ctypes.c_float, ctypes.c_void_p
+_S = ctypes.c_char_p
 
 # name -> (restype, argtypes)
 _SIGS = {
@@ -60,6 +61,11 @@ _SIGS = {
     "atlb_sgemm_tc_dev": (_I, [_I, _I, _I, _I, _I, _I, _F, _P, _I, _P, _I, _F, _P, _I]),
     "atlb_dtrsm_dev": (_I, [_I, _I, _I, _I, _I, _I, _D, _P, _I, _P, _I]),
     "atlb_dtrsm_dev_noalloc": (_I, [_I, _I, _I, _I, _I, _I, _D, _P, _I, _P, _I]),
+    "atlb_tune_get": (_I, [_S]),
+    "atlb_tune_set": (_I, [_S, _I]),
+    "atlb_tune_load": (_I, [_S]),
+    "atlb_tune_count": (_I, []),
+    "atlb_tune_name": (_S, [_I]),
     "atlb_dsyrk_dev": (_I, [_I, _I, _I, _I, _D, _P, _I, _D, _P, _I]),
     "atlb_dgetrf_dev": (_I, [_I, _I, _P, _I, _P, _P]),
     "atlb_dgetrs_dev": (_I, [_I, _I, _I, _P, _I, _P, _P, _I]),
@@ -118,7 +124,11 @@ def _wrap(name):
         f = getattr(lib(), name)
         conv = []
         for a, t in zip(args, f.argtypes):
-            conv.append(ptr(a) if t is _P else a)
+            if t is _P:
+                a = ptr(a)
+            elif t is _S and isinstance(a, str):
+                a = a.encode()
+            conv.append(a)
         return f(*conv)
     call.__name__ = name
     call.__doc__ = f"ctypes call of {name} (see include/atlas_b200.h)"

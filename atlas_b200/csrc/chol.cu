@@ -128,11 +128,12 @@ void potrf_rec(int upper, int off, int N, T *A, long lda, int *dinfo, cudaStream
 // Outer loop: NBO-wide diagonal blocks factored by the recursion above, then
 // one TRSM for the block column below (right of) the diagonal block and one
 // SYRK for the trailing matrix.
-constexpr int NBO = 256;
 
 template <typename T>
 void potrf_dev(int uplo, int N, T *A, long lda, int *dinfo, cudaStream_t st, SgemmFn gemm) {
-  const std::vector<unsigned long long> key = {21ull + sizeof(T), (unsigned long long)uplo,
+  const int NBO = tune(kTunePotrfNB);  // multiple of 64
+  const std::vector<unsigned long long> key = {21ull + sizeof(T), (unsigned long long)tune_generation(),
+      (unsigned long long)uplo,
       (unsigned long long)N, (unsigned long long)lda, (unsigned long long)(uintptr_t)A,
       (unsigned long long)(uintptr_t)dinfo, (unsigned long long)(uintptr_t)gemm,
       (unsigned long long)(uintptr_t)st};

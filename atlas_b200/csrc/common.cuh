@@ -64,6 +64,14 @@ enum ScratchSlot {
 
 inline int cdiv(long a, long b) { return (int)((a + b - 1) / b); }
 
+// Tunable driver parameters (tuning.cu; chosen by atlas_b200/tune.py).
+enum TuneParam {
+  kTuneGetrfNB = 0, kTunePotrfNB, kTuneGemmGroup, kTuneSplitK, kTuneLookahead, kTuneTcMinWorkLog2,
+  kNumTune
+};
+int tune(int p);
+int tune_generation();  // bumps whenever a parameter changes (part of graph keys)
+
 // Replay cache for launch sequences that depend only on their arguments
 // (sizes, pointers, stream): the first call with a key runs `enqueue`
 // eagerly (sizing every workspace), the second captures it into a CUDA graph,

@@ -195,11 +195,11 @@ template <bool TA, bool TB, int VEC>
 __global__ void __launch_bounds__(THREADS, 1)
 dgemm_dmma_kernel(int M, int N, int K, double alpha, const double *__restrict__ A, long lda,
                   const double *__restrict__ B, long ldb, double beta, double *__restrict__ C,
-                  long ldc, int tri) {
+                  long ldc, int tri, int G) {
   extern __shared__ __align__(16) double smem[];
   const int tiles_m = (M + BM - 1) / BM, tiles_n = (N + BN - 1) / BN;
-  // grouped rasterisation: 8 tile-rows share B panels in L2
-  const int bid = blockIdx.x, G = 8;
+  // grouped rasterisation: G tile-rows share B panels in L2
+  const int bid = blockIdx.x;
   const int per_group = G * tiles_n, group = bid / per_group;
   const int first_m = group * G, gsz = min(tiles_m - first_m, G);
   const int tm = first_m + (bid % per_group) % gsz, tn = (bid % per_group) / gsz;
@@ -299,7 +299,7 @@ void launch(int M, int N, int K, double alpha, const double *A, long lda, const 
   // too few tiles for the 148 SMs and a long K: split K (partials + reduction)
   const int nsm = num_sms();
   int S = 1;
-  if (tiles * 2 <= nsm && K >= 4 * BK && !no_alloc_active()) S = std::min(cdiv(nsm, tiles), K / (2 * BK));
+  if (tune(kTuneSplitK) && tiles * 2 <= nsm && K >= 4 * BK && !no_alloc_active()) S = std::min(cdiv(nsm, tiles), K / (2 * BK));
   if (S > 1) {
     const int kc = cdiv(cdiv(K, S), BK) * BK;
     S = cdiv(K, kc);
@@ -320,7 +320,7 @@ void launch(int M, int N, int K, double alpha, const double *A, long lda, const 
     }
   }
   dgemm_dmma_kernel<TA, TB, VEC><<<tiles, THREADS, smem, st>>>(M, N, K, alpha, A, lda, B, ldb,
-                                                              beta, C, ldc, tri);
+                                                              beta, C, ldc, tri, tune(kTuneGemmGroup));
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
 

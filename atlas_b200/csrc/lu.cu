@@ -1182,27 +1182,20 @@ bool getrf_block(int j, int M, int jb, T *A, long lda, int *ipiv, int *dinfo, cu
 
 }  // namespace
 
-bool lookahead_enabled() {
-  static int v = -1;
-  if (v < 0) {
-    const char *e = getenv("ATLAS_B200_LOOKAHEAD");
-    v = (e && e[0] == '0') ? 0 : 1;
-  }
-  return v == 1;
-}
+bool lookahead_enabled() { return tune(kTuneLookahead) != 0; }
 
-// Outer loop: NBO-column block panels, each factored by the recursion above
+// Outer loop: NBO-column block panels (NBO tunable, 256 by default), each factored by the recursion above
 // (restricted to the panel's columns); the panel's row interchanges are then
 // applied to the columns on both sides and the trailing matrix is updated with
 // one TRSM and one large GEMM (the reference's recursion would issue the same
 // updates as a cascade of smaller ones; the pivots are the same).
-constexpr int NBO = 256;
-
 template <typename T>
 void getrf_dev(int M, int N, T *A, long lda, int *ipiv, int *dinfo, cudaStream_t st,
                SgemmFn gemm) {
   // the launch sequence depends only on (M, N, lda, pointers): replayed as a graph
-  const std::vector<unsigned long long> key = {1ull + sizeof(T), (unsigned long long)M,
+  const int NBO = tune(kTuneGetrfNB);  // multiple of 32, <= 256 (the fused panel's limit)
+  const std::vector<unsigned long long> key = {1ull + sizeof(T), (unsigned long long)tune_generation(),
+      (unsigned long long)M,
       (unsigned long long)N, (unsigned long long)lda, (unsigned long long)(uintptr_t)A,
       (unsigned long long)(uintptr_t)ipiv, (unsigned long long)(uintptr_t)dinfo,
       (unsigned long long)(uintptr_t)gemm, (unsigned long long)(uintptr_t)st};

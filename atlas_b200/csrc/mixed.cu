@@ -191,12 +191,11 @@ void symmetrize_dev(int uplo, int N, const double *A, long lda, double *F, long 
 // updates, K >= 256) amortize; the small updates inside a block column run
 // as plain FP32 FMA GEMMs (more accurate than the tensor-core formats, so the
 // factorization is at least as accurate as with the tensor cores alone).
-constexpr long kTcMinWork = 1L << 31;  // M*N*K below which FP32 FMA is used
 template <void (*TC)(int, int, int, int, int, float, const float *, long, const float *, long, float,
                      float *, long, cudaStream_t, int)>
 void sgemm_by_size(int ta, int tb, int M, int N, int K, float alpha, const float *A, long lda,
                    const float *B, long ldb, float beta, float *C, long ldc, cudaStream_t st, int tri) {
-  if (K < 128 || (long)M * N * K < kTcMinWork)
+  if (K < 128 || (long)M * N * K < (1L << tune(kTuneTcMinWorkLog2)))
     sgemm_dev(ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, st, tri);
   else
     TC(ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, st, tri);

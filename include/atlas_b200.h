@@ -124,6 +124,21 @@ int atlb_dtrsm_dev(int Side, int Uplo, int TransA, int Diag, int M, int N, doubl
                    const double *A, int lda, double *B, int ldb);
 int atlb_dsyrk_dev(int Uplo, int Trans, int N, int K, double alpha, const double *A, int lda,
                    double beta, double *C, int ldc);
+/* Tunable driver parameters.  Stand-in for the reference's install-time
+ * tuning output (tune/blas/gemm/gmmsearch.c:3604-3634 writes the chosen
+ * kernels and blockings into generated headers): atlas_b200/tune.py times the
+ * candidates on the GPU and writes tuning.conf beside the library, which is
+ * read on first use (ATLAS_B200_TUNE_FILE overrides the path, "none" skips
+ * it).  Names: getrf_nb, potrf_nb, dgemm_group, dgemm_splitk, lookahead,
+ * mixed_tc_min_work_log2.  get returns INT_MIN for an unknown name; set
+ * returns the stored (clamped) value or -1; load returns the number of values
+ * read or -1. */
+int atlb_tune_get(const char *name);
+int atlb_tune_set(const char *name, int value);
+int atlb_tune_load(const char *path);
+int atlb_tune_count(void);
+const char *atlb_tune_name(int i);
+
 /* atlb_dtrsm_dev without any device allocation.  No counterpart in the
  * reference.  For callers that cannot let the library call cudaMalloc:
  * code running during a CUDA graph capture, applications whose device memory
