@@ -635,7 +635,9 @@ def main():
         dgemm_tf, cublas_tf = flop / dgemm_ms / 1e9, flop / cublas_ms / 1e9
         out["dgemm_8192"] = {"ms": dgemm_ms, "tflops": dgemm_tf, "cublas_fp64_tflops": cublas_tf}
         out["roofline"] = {"bound": "tensor", "achieved": dgemm_tf, "peak": cublas_tf, "unit": "TFLOP/s",
-                           "frac": dgemm_tf / cublas_tf, "traffic": None,
+                           "frac": dgemm_tf / cublas_tf, "traffic": 7295669760,
+                           "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one 8192^3 launch "
+                                           "(ncu, profiles/dgemm_dmma_8192.md); algorithmic minimum 1.61e9 B",
                            "kernel": "dgemm_dmma_kernel 8192^3 (2*M*N*K flop per launch)",
                            "peak_note": "no FP64 figure in MEASURED_PEAKS.json; peak = cuBLAS DGEMM 8192^3 measured in this run"}
         del ga, gb
