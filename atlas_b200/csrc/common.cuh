@@ -53,6 +53,14 @@ struct NoAllocScope {
   ~NoAllocScope();
 };
 bool no_alloc_active();
+// While a GemmCtaCap is alive on a thread, large DGEMMs run on at most that
+// many CTAs (0: no cap).
+struct GemmCtaCap {
+  explicit GemmCtaCap(int ctas);
+  ~GemmCtaCap();
+  int prev;
+};
+int gemm_cta_cap();
 enum ScratchSlot {
   kSlotA = 0, kSlotB, kSlotC, kSlotIpiv, kSlotTau, kSlotWork, kSlotWork2,
   kSlotInfo, kSlotMixedA, kSlotMixedR, kSlotMixedX, kSlotMixedD,
@@ -67,7 +75,7 @@ inline int cdiv(long a, long b) { return (int)((a + b - 1) / b); }
 // Tunable driver parameters (tuning.cu; chosen by atlas_b200/tune.py).
 enum TuneParam {
   kTuneGetrfNB = 0, kTunePotrfNB, kTuneGemmGroup, kTuneSplitK, kTuneLookahead, kTuneTcMinWorkLog2,
-  kNumTune
+  kTuneLookaheadReserve, kNumTune
 };
 int tune(int p);
 int tune_generation();  // bumps whenever a parameter changes (part of graph keys)

@@ -209,6 +209,28 @@ dgemm_dmma_kernel(int M, int N, int K, double alpha, const double *__restrict__ 
   dgemm_tile<TA, TB, VEC>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, tri, m0, n0, smem);
 }
 
+// The same GEMM on a capped number of CTAs, each walking tiles t, t + grid,
+// ... (same rasterisation): leaves SMs free for work on another stream
+// (the factorizations' look-ahead panels).
+template <bool TA, bool TB, int VEC>
+__global__ void __launch_bounds__(THREADS, 1)
+dgemm_capped_kernel(int M, int N, int K, double alpha, const double *__restrict__ A, long lda,
+                    const double *__restrict__ B, long ldb, double beta, double *__restrict__ C,
+                    long ldc, int tri, int G) {
+  extern __shared__ __align__(16) double smem[];
+  const int tiles_m = (M + BM - 1) / BM, tiles_n = (N + BN - 1) / BN, tiles = tiles_m * tiles_n;
+  for (int bid = blockIdx.x; bid < tiles; bid += gridDim.x) {
+    const int per_group = G * tiles_n, group = bid / per_group;
+    const int first_m = group * G, gsz = min(tiles_m - first_m, G);
+    const int tm = first_m + (bid % per_group) % gsz, tn = (bid % per_group) / gsz;
+    const int m0 = tm * BM, n0 = tn * BN;
+    if (tri == 1 && m0 + BM - 1 < n0) continue;
+    if (tri == 2 && m0 > n0 + BN - 1) continue;
+    dgemm_tile<TA, TB, VEC>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, tri, m0, n0, smem);
+    __syncthreads();  // shared memory is reused by the next tile
+  }
+}
+
 // Grouped (batched, uneven) GEMM: a persistent grid walks the 128x128 tiles
 // of all problems; tile t belongs to problem order[p] where tile_start[p] <= t
 // < tile_start[p+1] (problems sorted by decreasing size on the host).
@@ -318,6 +340,19 @@ void launch(int M, int N, int K, double alpha, const double *A, long lda, const 
       ATLB_CUDA_CHECK(cudaGetLastError());
       return;
     }
+  }
+  const int cap = gemm_cta_cap();
+  if (cap > 0 && tiles > cap) {
+    static bool configured_c = false;
+    if (!configured_c) {
+      ATLB_CUDA_CHECK(cudaFuncSetAttribute(dgemm_capped_kernel<TA, TB, VEC>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      configured_c = true;
+    }
+    dgemm_capped_kernel<TA, TB, VEC><<<cap, THREADS, smem, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C,
+                                                                 ldc, tri, tune(kTuneGemmGroup));
+    ATLB_CUDA_CHECK(cudaGetLastError());
+    return;
   }
   dgemm_dmma_kernel<TA, TB, VEC><<<tiles, THREADS, smem, st>>>(M, N, K, alpha, A, lda, B, ldb,
                                                               beta, C, ldc, tri, tune(kTuneGemmGroup));

@@ -336,6 +336,30 @@ __device__ __forceinline__ void shift_update(T (&a)[NB], T l, const T *u, int kf
   a[NB - 1] = T(0);
 }
 
+// stage[k] = a[k + off] (k < NB, zero past the row), 16 bytes per store
+template <typename T, int NB>
+__device__ __forceinline__ void stage_row(T *stage, const T (&a)[NB], int off) {
+  if (sizeof(T) == 4) {
+#pragma unroll
+    for (int q = 0; q < NB / 4; q++) {
+      float4 v;
+      v.x = (float)(4 * q + 0 + off < NB ? a[(4 * q + 0 + off) % NB] : T(0));
+      v.y = (float)(4 * q + 1 + off < NB ? a[(4 * q + 1 + off) % NB] : T(0));
+      v.z = (float)(4 * q + 2 + off < NB ? a[(4 * q + 2 + off) % NB] : T(0));
+      v.w = (float)(4 * q + 3 + off < NB ? a[(4 * q + 3 + off) % NB] : T(0));
+      reinterpret_cast<float4 *>(stage)[q] = v;
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < NB / 2; q++) {
+      double2 v;
+      v.x = (double)(2 * q + 0 + off < NB ? a[(2 * q + 0 + off) % NB] : T(0));
+      v.y = (double)(2 * q + 1 + off < NB ? a[(2 * q + 1 + off) % NB] : T(0));
+      reinterpret_cast<double2 *>(stage)[q] = v;
+    }
+  }
+}
+
 constexpr int kMaxPanelCluster = 16;
 __device__ int g_panel_timeout = 0;  // set if a panel wait ever gives up (1 s)
 
@@ -410,13 +434,10 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
     const bool owner = act && (unsigned)pos == p;
     if (owner) {
       if (shifted) {
-#pragma unroll
-        for (int k = 0; k < NB - 1; k++) stage[k] = a[k + 1];
-        stage[NB - 1] = T(0);
+        stage_row<T, NB>(stage, a, 1);
         stage[NB + 1] = lm;
       } else {
-#pragma unroll
-        for (int k = 0; k < NB; k++) stage[k] = a[k];
+        stage_row<T, NB>(stage, a, 0);
         stage[NB + 1] = T(0);
       }
       stage[NB] = rc;
@@ -471,16 +492,22 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
     warp_argmax_key(kv, pu);
     const int p = (int)pu;
     const int w = __ffs(__ballot_sync(0xffffffffu, lane < C && mykey == kv && mypos == pu)) - 1;
+    T piv_s, u1_s;
     {
       // finish the winner's update with the previous column's pivot row
       const T *uprev = nz_prev ? wu[warp] : zrow;
       const T up = lane < NB - 1 ? uprev[lane + 1] : T(0);
       const T nv = fma(-slot[b][w].lm, up, slot[b][w].row[lane]);
+      // the pivot and the next column's update coefficient come straight from
+      // the lanes that computed them; the full row goes to shared memory for
+      // the rest of the update
+      piv_s = __shfl_sync(0xffffffffu, nv, 0);
+      u1_s = __shfl_sync(0xffffffffu, nv, 1);
       __syncwarp();
       wu[warp][lane] = nv;
       __syncwarp();
     }
-    const T piv = wu[warp][0], prcp = slot[b][w].rcp;
+    const T piv = piv_s, prcp = slot[b][w].rcp;
     nz_prev = piv != T(0);
     if (crank == 0 && tid == 0) {
       ipiv[j] = roff + p;
@@ -500,7 +527,7 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
         lm = nz ? l : T(0);
         u = nz ? wu[warp] : zrow;
         Lsm[j * PT + tid] = l;
-        a[0] = fma(-lm, u[1], a[1]);  // the next column first: it decides the next pivot
+        a[0] = fma(-lm, nz ? u1_s : T(0), a[1]);  // the next column first: it decides the next pivot
       }
     }
     if (j + 1 < MN) {
@@ -1156,6 +1183,84 @@ void getrf_rec(int off, int M, int N, T *A, long lda, int *ipiv, int *dinfo, cud
   laswp_dev<T>(Nl, A + (long)off * lda, lda, off + Nl, off + MN, ipiv, 1, st);
 }
 
+// C (m x nr) -= A (m x k) * B (k x nr), k <= 32, nr <= 256, one leading
+// dimension: the update of a block column's remaining columns by one leaf
+// panel.  Small and skinny, so a plain GEMM pays its K-loop pipeline and
+// tiling for a single 32-deep step; here one CTA loads all of B and a
+// 16*RT-row slice of A into shared memory once, every thread computes RT
+// rows x up to 16 columns, and the old C values are loaded before any
+// result is stored.
+template <typename T, int RT>
+__global__ void __launch_bounds__(256)
+rank_update_kernel(int m, int nr, int k, const T *__restrict__ A, const T *__restrict__ B, T *__restrict__ C,
+                   long lda) {
+  constexpr int BR = 16 * RT;
+  __shared__ __align__(16) T sA[32][BR];
+  extern __shared__ __align__(16) unsigned char ru_smem[];
+  T *sB = reinterpret_cast<T *>(ru_smem);  // [32][nrp]
+  const int nrp = (nr + 15) / 16 * 16;
+  const int tid = threadIdx.x, r0 = blockIdx.x * BR;
+  for (int idx = tid; idx < 32 * BR; idx += 256) {
+    const int r = idx % BR, i = idx / BR;
+    sA[i][r] = (i < k && r0 + r < m) ? A[r0 + r + (long)i * lda] : T(0);
+  }
+  for (int idx = tid; idx < 32 * nrp; idx += 256) {
+    const int i = idx % 32, c = idx / 32;
+    sB[i * nrp + c] = (i < k && c < nr) ? B[i + (long)c * lda] : T(0);
+  }
+  __syncthreads();
+  const int tr = tid % 16, tc = tid / 16;  // rows tr*RT .. +RT-1, columns tc + 16 q
+  const int nq = (nr - tc + 15) / 16;      // this thread's columns (<= 16)
+  T acc[RT][16];
+#pragma unroll
+  for (int a = 0; a < RT; a++)
+#pragma unroll
+    for (int q = 0; q < 16; q++) acc[a][q] = T(0);
+#pragma unroll 4
+  for (int i = 0; i < 32; i++) {
+    T av[RT];
+#pragma unroll
+    for (int a = 0; a < RT; a++) av[a] = sA[i][tr * RT + a];
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      if (q < nq) {  // sB holds nrp columns only
+        const T bv = sB[i * nrp + tc + 16 * q];
+#pragma unroll
+        for (int a = 0; a < RT; a++) acc[a][q] = fma(av[a], bv, acc[a][q]);
+      }
+    }
+  }
+  T old[RT][16];
+#pragma unroll
+  for (int q = 0; q < 16; q++)
+#pragma unroll
+    for (int a = 0; a < RT; a++) {
+      const int r = r0 + tr * RT + a, c = tc + 16 * q;
+      old[a][q] = (q < nq && r < m) ? C[r + (long)c * lda] : T(0);
+    }
+#pragma unroll
+  for (int q = 0; q < 16; q++)
+#pragma unroll
+    for (int a = 0; a < RT; a++) {
+      const int r = r0 + tr * RT + a, c = tc + 16 * q;
+      if (q < nq && r < m) C[r + (long)c * lda] = old[a][q] - acc[a][q];
+    }
+}
+
+template <typename T>
+void rank_update(int m, int nr, int k, const T *A, const T *B, T *C, long lda, cudaStream_t st) {
+  constexpr int RT = sizeof(T) == 8 ? 2 : 4;
+  const int nrp = (nr + 15) / 16 * 16, smem = 32 * nrp * (int)sizeof(T);
+  static bool configured = false;
+  if (!configured) {
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(rank_update_kernel<T, RT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         32 * 256 * (int)sizeof(T)));
+    configured = true;
+  }
+  rank_update_kernel<T, RT><<<cdiv(m, 16 * RT), 256, smem, st>>>(m, nr, k, A, B, C, lda);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
+
 // Block column [j, j + jb) of the factorization, rows j..M-1, as 32-column
 // leaves: each leaf is one fused panel launch (factor + interchanges across
 // the block + U12 solve) followed by one GEMM updating the block's columns
@@ -1174,8 +1279,8 @@ bool getrf_block(int j, int M, int jb, T *A, long lda, int *ipiv, int *dinfo, cu
     if (!(sizeof(T) == 4 && tournament_enabled() &&
           launch_tournament_panel((int)m, w, (float *)Ac, lda, ipiv + c, c, dinfo, l, nright, st)))
       launch_fused_panel<T>(m, w, Ac, lda, ipiv + c, c, dinfo, l, nright, st);
-    if (nright > 0 && m - w > 0)
-      update_gemm(gemm, m - w, nright, w, Ac + w, Ac + (long)w * lda, Ac + w + (long)w * lda, lda, st);
+    if (nright > 0 && m - w > 0)  // rank-w update of the block's columns right of the leaf
+      rank_update<T>(m - w, nright, w, Ac + w, Ac + (long)w * lda, Ac + w + (long)w * lda, lda, st);
   }
   return true;
 }
@@ -1251,6 +1356,9 @@ void getrf_dev(int M, int N, T *A, long lda, int *ipiv, int *dinfo, cudaStream_t
           T *Ar = A + (long)c0 * lda;
           laswp_dev<T>(nr, Ar, lda, j, jn, ipiv, 1, st);
           trsm_dev<T>(kLeft, kLower, kNoTrans, kUnit, jb, nr, T(1), Ad, lda, Ar + j, lda, st, gemm);
+          // the trailing update may leave SMs to the side stream's panel
+          const int reserve = jbn > 0 ? tune(kTuneLookaheadReserve) : 0;
+          GemmCtaCap cap(reserve > 0 ? std::max(1, num_sms() - reserve) : 0);
           if (M - jn > 0) update_gemm(gemm, M - jn, nr, jb, Ad + jb, Ar + j, Ar + jn, lda, st);
         }
       }

@@ -104,6 +104,13 @@ NoAllocScope::NoAllocScope() { tl_no_alloc++; }
 NoAllocScope::~NoAllocScope() { tl_no_alloc--; }
 bool no_alloc_active() { return tl_no_alloc > 0; }
 
+namespace {
+thread_local int tl_gemm_cap = 0;
+}
+GemmCtaCap::GemmCtaCap(int ctas) : prev(tl_gemm_cap) { tl_gemm_cap = ctas; }
+GemmCtaCap::~GemmCtaCap() { tl_gemm_cap = prev; }
+int gemm_cta_cap() { return tl_gemm_cap; }
+
 void *scratch(int slot, size_t bytes) {
   Buf &b = tl.dev[slot + tl_side * kNumSlots];
   if (bytes == 0) bytes = 16;
@@ -227,7 +234,8 @@ void run_graph(const std::vector<unsigned long long> &key, cudaStream_t st,
   tl_capturing = false;
   cudaGraphExec_t exec = nullptr;
   if (e == cudaSuccess && !tl_capture_failed && graph)
-    e = cudaGraphInstantiate(&exec, graph, 0);
+    // keep the side stream's priority inside the graph (look-ahead panels)
+    e = cudaGraphInstantiateWithFlags(&exec, graph, cudaGraphInstantiateFlagUseNodePriority);
   if (graph) cudaGraphDestroy(graph);
   if (e != cudaSuccess || tl_capture_failed || !exec) {
     cudaGetLastError();

@@ -33,6 +33,7 @@ const TuneDef kDefs[kNumTune] = {
     {"dgemm_splitk", 1, 0, 1, 1},             // split K when the output has too few tiles
     {"lookahead", 1, 0, 1, 1},                // depth-one look-ahead in getrf / potrf
     {"mixed_tc_min_work_log2", 31, 16, 40, 1},  // mixed solvers: M*N*K below 2^x runs on FP32 FMA
+    {"lookahead_reserve_sms", 0, 0, 96, 1},   // SMs the trailing-update DGEMM leaves to the look-ahead panel
 };
 
 std::atomic<int> g_val[kNumTune];
