@@ -15,6 +15,7 @@
 // panel: each row carries its current position and the final permutation is
 // applied when the rows are written back.
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 #include <cfloat>
 #include <climits>
@@ -208,13 +209,17 @@ getf2_cluster_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restr
 // latency hides behind it.  Slots are double-buffered by column parity.
 // Pivot order: largest |value|, lowest current row position on ties (the
 // first maximum, like cblas_idamax); a NaN entry ranks below every number.
+// One CTA's candidate for one column as it lands in every CTA's shared
+// memory: a whole number of 16-byte units, each sent by one st.async.
+template <typename T>
+using PivKey = typename std::conditional<sizeof(T) == 8, unsigned long long, unsigned>::type;
 template <typename T, int NB>
-struct PanelSlot {
+struct __align__(16) PanelSlot {
   T row[NB];
-  unsigned long long key;  // pivot_key of the candidate
-  T rcp;                   // 1 / (candidate value), computed by the sender off the critical path
-  T lm;                    // the sender's pending multiplier: the row is row - lm * u (see below)
-  int pos;
+  PivKey<T> key;  // pivot_key of the candidate
+  typename std::conditional<sizeof(T) == 8, long long, int>::type pos;
+  T rcp;          // 1 / (candidate value), computed by the sender off the critical path
+  T lm;           // the sender's pending multiplier: the row is row - lm * u (see below)
 };
 
 // Candidates are compared through one integer key: |value|'s bit pattern + 1
@@ -228,6 +233,11 @@ __device__ __forceinline__ unsigned long long pivot_key(T v) {
   if (sizeof(T) == 8) return (unsigned long long)__double_as_longlong((double)t) + 1ull;
   return (unsigned long long)__float_as_uint((float)t) + 1ull;
 }
+__device__ __forceinline__ void warp_argmax_key(unsigned &key, unsigned &pos) {  // FP32 keys fit 32 bits
+  const unsigned m = __reduce_max_sync(0xffffffffu, key);
+  pos = __reduce_min_sync(0xffffffffu, key == m ? pos : 0xffffffffu);
+  key = m;
+}
 __device__ __forceinline__ void warp_argmax_key(unsigned long long &key, unsigned &pos) {
   const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
   const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
@@ -235,6 +245,21 @@ __device__ __forceinline__ void warp_argmax_key(unsigned long long &key, unsigne
   const bool eq = hi == mhi && lo == mlo;
   pos = __reduce_min_sync(0xffffffffu, eq ? pos : 0xffffffffu);
   key = ((unsigned long long)mhi << 32) | mlo;
+}
+
+// Lane of the warp's largest key (lowest pos among equal keys).  Usually
+// the high 32 bits of the largest key occur in one lane only: one redux and
+// one ballot then settle it.
+template <typename K>
+__device__ __forceinline__ int warp_argmax_lane(K key, unsigned pos) {
+  const unsigned hi = sizeof(K) == 8 ? (unsigned)((unsigned long long)key >> 32) : (unsigned)key;
+  const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned m = __ballot_sync(0xffffffffu, hi == mhi);
+  if ((m & (m - 1)) == 0) return __ffs(m) - 1;
+  K k = key;
+  unsigned p = pos;
+  warp_argmax_key(k, p);
+  return __ffs(__ballot_sync(0xffffffffu, key == k && pos == p)) - 1;
 }
 
 __device__ __forceinline__ void cluster_arrive() {
@@ -248,23 +273,11 @@ __device__ __forceinline__ uint32_t mapa_u32(uint32_t a, int rank) {
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
   return r;
 }
-// one-way store into another CTA's shared memory that completes a
+// one-way 16-byte store into another CTA's shared memory that completes a
 // transaction on that CTA's mbarrier (no fence, no round trip)
-__device__ __forceinline__ void st_async(uint32_t addr, double v, uint32_t mbar) {
-  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b64 [%0], %1, [%2];"
-               ::"r"(addr), "l"(__double_as_longlong(v)), "r"(mbar) : "memory");
-}
-__device__ __forceinline__ void st_async(uint32_t addr, float v, uint32_t mbar) {
-  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b32 [%0], %1, [%2];"
-               ::"r"(addr), "r"(__float_as_uint(v)), "r"(mbar) : "memory");
-}
-__device__ __forceinline__ void st_async(uint32_t addr, unsigned long long v, uint32_t mbar) {
-  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b64 [%0], %1, [%2];"
-               ::"r"(addr), "l"(v), "r"(mbar) : "memory");
-}
-__device__ __forceinline__ void st_async(uint32_t addr, int v, uint32_t mbar) {
-  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b32 [%0], %1, [%2];"
-               ::"r"(addr), "r"(v), "r"(mbar) : "memory");
+__device__ __forceinline__ void st_async16(uint32_t addr, uint4 v, uint32_t mbar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.b32 [%0], {%1, %2, %3, %4}, [%5];"
+               ::"r"(addr), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w), "r"(mbar) : "memory");
 }
 __device__ __forceinline__ bool mbar_try_wait(uint32_t a, uint32_t parity) {
   uint32_t ok;
@@ -273,33 +286,35 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t a, uint32_t parity) {
   return ok != 0;
 }
 
-// U12 = L11^-1 A12 for the fused panel kernel (one CTA; L11 = the unit
-// lower MN x MN top of the factored panel, A12 its right columns' top rows).
-// Kept out of line so its registers do not add to the panel loop's.
+// U12 = L11^-1 A12 for the panel kernels: L11 = the unit lower MN x MN top
+// of the factored panel, A12 the top MN rows of the right columns.  Warp gw
+// of GW solves columns 4 gw .. 4 gw + 3, 4 (gw + GW) .. and so on: lane i
+// holds row i of four columns and row i of L11, and x_i -= L[i][k] x_k runs
+// for k = 0, 1, .. in order (forward substitution, x_k by shuffle), four
+// independent chains at a time.  Out of line so its registers do not add to
+// the panel loop's.
 template <typename T, int NB>
-__device__ __noinline__ void panel_u12_solve(int MN, int ncols, int nright, T *A, long lda, unsigned char *smem) {
-  const int tid = threadIdx.x;
-  T(*sL)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem);
-  for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
-    const int i = idx % NB, k = idx / NB;
-    sL[i][k] = (i < MN && k < i) ? __ldcg(A + i + (long)k * lda) : T(0);
-  }
-  __syncthreads();
-  for (int c = tid; c < nright; c += blockDim.x) {
-    T *col = A + (long)(ncols + c) * lda;
-    T x[NB];
+__device__ __noinline__ void panel_u12_solve(int MN, int ncols, int nright, int gw, int GW, T *A, long lda) {
+  const int lane = threadIdx.x & 31;
+  T L[NB - 1];
 #pragma unroll
-    for (int i = 0; i < NB; i++) x[i] = i < MN ? __ldcg(col + i) : T(0);
+  for (int k = 0; k < NB - 1; k++) L[k] = (k < lane && lane < MN) ? __ldcg(A + lane + (long)k * lda) : T(0);
+  for (int c0 = 4 * gw; c0 < nright; c0 += 4 * GW) {
+    T x[4];
 #pragma unroll
-    for (int i = 1; i < NB; i++) {
-      T s = x[i];
+    for (int q = 0; q < 4; q++)
+      x[q] = (c0 + q < nright && lane < MN) ? __ldcg(A + lane + (long)(ncols + c0 + q) * lda) : T(0);
 #pragma unroll
-      for (int k = 0; k < i; k++) s = fma(-sL[i][k], x[k], s);
-      x[i] = s;
+    for (int k = 0; k < NB - 1; k++) {
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const T xk = __shfl_sync(0xffffffffu, x[q], k);
+        if (lane > k) x[q] = fma(-L[k], xk, x[q]);
+      }
     }
 #pragma unroll
-    for (int i = 0; i < NB; i++)
-      if (i < MN) col[i] = x[i];
+    for (int q = 0; q < 4; q++)
+      if (c0 + q < nright && lane < MN) A[lane + (long)(ncols + c0 + q) * lda] = x[q];
   }
 }
 
@@ -368,19 +383,23 @@ __global__ void __launch_bounds__(PT, 1)
 getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restrict__ ipiv, int roff,
                    int *__restrict__ dinfo, int nleft, int nright) {
   static_assert(NB == 32, "one pivot-row element per lane");
-  constexpr uint32_t kMsg = NB * sizeof(T) + 8 + 2 * sizeof(T) + sizeof(int);  // bytes one CTA sends one CTA
+  using Slot = PanelSlot<T, NB>;
+  using K = PivKey<T>;
+  constexpr int kUnits = (int)sizeof(Slot) / 16;  // 16-byte messages one CTA sends one CTA
+  static_assert(sizeof(Slot) % 16 == 0, "slots travel as 16-byte units");
+  constexpr uint32_t kMsg = sizeof(Slot);
   cg::cluster_group cl = cg::this_cluster();
   const int C = (int)cl.num_blocks(), crank = (int)cl.block_rank();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int MN = min(M, ncols);
   extern __shared__ __align__(16) unsigned char fused_smem[];
   T *Lsm = reinterpret_cast<T *>(fused_smem);  // [NB][PT]: finished row parts
-  __shared__ PanelSlot<T, NB> slot[2][kMaxPanelCluster];
+  __shared__ Slot slot[2][kMaxPanelCluster];
   __shared__ __align__(8) unsigned long long mbar[2];
-  __shared__ __align__(16) T wu[PT / 32][NB];  // per-warp copy of the pivot row
-  __shared__ __align__(16) T stage[NB + 2];    // the CTA winner's message: row, 1/value, lm
+  __shared__ __align__(16) T wu[2][PT / 32][NB];  // per-warp copy of the pivot row, by column parity
+  __shared__ Slot stage;                       // the CTA winner's message
   __shared__ __align__(16) T zrow[NB];
-  __shared__ unsigned long long wv[2][PT / 32];   // per-warp candidates, by column parity
+  __shared__ K wv[2][PT / 32];                 // per-warp candidates, by column parity
   __shared__ unsigned wp[2][PT / 32];
   __shared__ int s_nmoved;
   __shared__ int s_from[2 * NB], s_to[2 * NB];  // rows that move: from (old) -> to (final)
@@ -414,50 +433,58 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
   // Reduce this CTA's candidates (|a[0]| of active rows) and let the
   // winner's warp send its row for column c to every CTA's slot.  Inside the
   // column loop the winner has updated only a[0] (the candidate itself): it
-  // sends its other entries as they are, shifted, with its multiplier lm, and
-  // the receivers finish the update (row[k] - lm * u[k+1]) themselves, so the
-  // message leaves before the sender's own row update.
-  auto push = [&](int c, bool shifted) {
+  // sends row[0] = a[0] and row[1] (the next column, finished here with the
+  // pivot row's u2) ready to use, its other entries as they are, shifted,
+  // with its multiplier lm, and the receivers finish the update
+  // (row[k] - lm * u[k+1], k >= 2) themselves, so the message leaves before
+  // the sender's own row update.
+  auto push = [&](int c, bool shifted, T u2) {
     const int b = c & 1;
     const uint32_t mb = b ? mb1 : mb0;
     if (tid == 0)
       asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(kMsg * C) : "memory");
-    const T rc = act ? T(1) / a[0] : T(0);  // needed only by the winner; overlaps the reductions
-    unsigned long long v = act ? pivot_key(a[0]) : 0ull;
-    unsigned p = act ? (unsigned)pos : 0xffffffffu;
-    warp_argmax_key(v, p);
-    if (lane == 0) { wv[b][warp] = v; wp[b][warp] = p; }
+    const K v = act ? (K)pivot_key(a[0]) : K(0);
+    const unsigned p = act ? (unsigned)pos : 0xffffffffu;
+    const int wl = warp_argmax_lane(v, p);
+    if (lane == wl) { wv[b][warp] = v; wp[b][warp] = p; }
     __syncthreads();
-    v = lane < PT / 32 ? wv[b][lane] : 0ull;
-    p = lane < PT / 32 ? wp[b][lane] : 0xffffffffu;
-    warp_argmax_key(v, p);
-    const bool owner = act && (unsigned)pos == p;
-    if (owner) {
-      if (shifted) {
-        stage_row<T, NB>(stage, a, 1);
-        stage[NB + 1] = lm;
-      } else {
-        stage_row<T, NB>(stage, a, 0);
-        stage[NB + 1] = T(0);
+    const int wc = warp_argmax_lane(lane < PT / 32 ? wv[b][lane] : K(0),
+                                    lane < PT / 32 ? wp[b][lane] : 0xffffffffu);
+    if (warp == wc) {  // the warp of the CTA's candidate (or, without one, of a key that never wins)
+      const bool owner = act && lane == wl;
+      if (owner) {
+        stage_row<T, NB>(stage.row, a, shifted ? 1 : 0);
+        if (shifted) {
+          stage.row[0] = a[0];
+          stage.row[1] = fma(-lm, u2, a[2]);
+        }
+        stage.key = v;
+        stage.pos = (int)p;
+        stage.rcp = T(1) / a[0];
+        stage.lm = shifted ? lm : T(0);
       }
-      stage[NB] = rc;
-    }
-    const bool mine = __any_sync(0xffffffffu, owner) || (p == 0xffffffffu && warp == 0);
-    if (mine) {
+      if (!__any_sync(0xffffffffu, owner) && lane == 0) {
+        stage.key = K(0);
+        stage.pos = -1;
+      }
+      // kUnits x C messages spread over the warp's lanes, 16 bytes each
       __syncwarp();
-      const T e = stage[lane];
-      const uint32_t srow = smem_u32(&slot[b][crank].row[lane]);
-      for (int q = 0; q < C; q++) st_async(mapa_u32(srow, q), e, mapa_u32(mb, q));
-      if (lane == 0) {
-        const uint32_t sv = smem_u32(&slot[b][crank].key), sp = smem_u32(&slot[b][crank].pos),
-                       sr = smem_u32(&slot[b][crank].rcp), sl = smem_u32(&slot[b][crank].lm);
-        const T rcs = stage[NB], lms = stage[NB + 1];
-        for (int q = 0; q < C; q++) {
-          const uint32_t rm = mapa_u32(mb, q);
-          st_async(mapa_u32(sv, q), v, rm);
-          st_async(mapa_u32(sp, q), (int)p, rm);
-          st_async(mapa_u32(sr, q), rcs, rm);
-          st_async(mapa_u32(sl, q), lms, rm);
+      const uint4 *src = reinterpret_cast<const uint4 *>(&stage);
+      const uint32_t dst = smem_u32(&slot[b][crank]);
+      if (sizeof(T) == 4) {
+        constexpr int kItems = (kUnits * kMaxPanelCluster + 31) / 32;
+#pragma unroll
+        for (int i = 0; i < kItems; i++) {
+          const int it = lane + 32 * i;
+          if (it < kUnits * C) {
+            const int q = it / kUnits, unit = it - q * kUnits;
+            st_async16(mapa_u32(dst + 16 * unit, q), src[unit], mapa_u32(mb, q));
+          }
+        }
+      } else {
+        for (int it = lane; it < kUnits * C; it += 32) {
+          const int q = it / kUnits, unit = it - q * kUnits;
+          st_async16(mapa_u32(dst + 16 * unit, q), src[unit], mapa_u32(mb, q));
         }
       }
     }
@@ -476,7 +503,7 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
   };
 
   if (MN > 0) {
-    push(0, false);
+    push(0, false, T(0));
     receive(0);
   }
   bool nz_prev = false;  // pivot of the previous column non-zero (its row is then the update row)
@@ -485,55 +512,54 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
   for (int j = 0; j < MN; j++) {
     const int b = j & 1;
     // the global winner from the C local slots (every warp computes it)
-    unsigned long long kv = lane < C ? slot[b][lane].key : 0ull;
     const unsigned mypos = lane < C ? (unsigned)slot[b][lane].pos : 0xffffffffu;
-    unsigned pu = mypos;
-    const unsigned long long mykey = kv;
-    warp_argmax_key(kv, pu);
-    const int p = (int)pu;
-    const int w = __ffs(__ballot_sync(0xffffffffu, lane < C && mykey == kv && mypos == pu)) - 1;
-    T piv_s, u1_s;
+    const int w = warp_argmax_lane(lane < C ? slot[b][lane].key : K(0), mypos);
+    const int p = (int)__shfl_sync(0xffffffffu, mypos, w);
+    // the pivot, the next column's update coefficient and 1/pivot come ready
+    // in the winner's slot; u2 (the pivot row's next entry) is for the next
+    // sender
+    const T *uprev = nz_prev ? wu[b ^ 1][warp] : zrow;
+    const T piv = slot[b][w].row[0], u1 = slot[b][w].row[1], prcp = slot[b][w].rcp;
+    const T lmw = slot[b][w].lm;
+    const T u2 = fma(-lmw, uprev[3], slot[b][w].row[2]);
     {
-      // finish the winner's update with the previous column's pivot row
-      const T *uprev = nz_prev ? wu[warp] : zrow;
-      const T up = lane < NB - 1 ? uprev[lane + 1] : T(0);
-      const T nv = fma(-slot[b][w].lm, up, slot[b][w].row[lane]);
-      // the pivot and the next column's update coefficient come straight from
-      // the lanes that computed them; the full row goes to shared memory for
-      // the rest of the update
-      piv_s = __shfl_sync(0xffffffffu, nv, 0);
-      u1_s = __shfl_sync(0xffffffffu, nv, 1);
-      __syncwarp();
-      wu[warp][lane] = nv;
-      __syncwarp();
+      // the winner's full row for the rest of the update (lanes 0 and 1 came
+      // finished), taken out of the slot before this column's message goes
+      // out (after it, a CTA that has all of it may send column j + 2 here)
+      const T rw = slot[b][w].row[lane];
+      const T up = (lane >= 2 && lane < NB - 1) ? uprev[lane + 1] : T(0);
+      wu[b][warp][lane] = lane < 2 ? rw : fma(-lmw, up, rw);
     }
-    const T piv = piv_s, prcp = slot[b][w].rcp;
-    nz_prev = piv != T(0);
+    const bool nz = piv != T(0);
     if (crank == 0 && tid == 0) {
       ipiv[j] = roff + p;
-      if (piv == T(0)) atomicMin(dinfo, roff + j + 1);
+      if (!nz) atomicMin(dinfo, roff + j + 1);
     }
     if (act) {
       if (pos == p) {  // this row becomes row j of U: its remaining part is final
-        act = false;     // (stored to Lsm after the loop, off the critical path)
+        act = false;     // (stored after the loop, off the critical path)
         piv_row = true;
         pos = j;
       } else {
         if (pos == j) pos = p;  // the row displaced by the interchange
         // a zero pivot leaves the column unscaled and the row unchanged: the
         // update then runs with l = 0 against a zero row (exact: a - 0*0 = a)
-        const bool nz = piv != T(0);
-        const T l = !nz ? a[0] : (fabs(piv) >= safmin<T>() ? a[0] * prcp : a[0] / piv);
+        T l;
+        if (!nz) l = a[0];
+        else if (fabs(piv) >= safmin<T>()) l = a[0] * prcp;
+        else l = a[0] / piv;
         lm = nz ? l : T(0);
-        u = nz ? wu[warp] : zrow;
+        a[0] = fma(-lm, nz ? u1 : T(0), a[1]);  // the next column first: it decides the next pivot
         Lsm[j * PT + tid] = l;
-        a[0] = fma(-lm, nz ? u1_s : T(0), a[1]);  // the next column first: it decides the next pivot
+        A[r + (long)j * lda] = l;  // at the row's original place (moved rows are rewritten at the end)
       }
     }
+    if (j + 1 < MN) push(j + 1, true, nz ? u2 : T(0));
+    __syncwarp();
+    nz_prev = nz;
+    u = nz ? wu[b][warp] : zrow;
     if (j + 1 < MN) {
-      const bool upd = act;  // active rows (the pivot row has just left) owe the rest of the update
-      push(j + 1, true);
-      if (upd) shift_update<T, NB>(a, lm, u, 2);  // it runs while the messages travel
+      if (act) shift_update<T, NB>(a, lm, u, 2);  // it runs while the messages travel
       receive(j + 1);
     }
   }
@@ -544,21 +570,13 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
     for (int k = 0; k < NB; k++)
       if (pos + k < ncols) dst[k * PT] = a[k];
   }
-  // rows to their final positions: the panel's columns from shared memory;
-  // the block's other columns of the rows that move (at most 2*MN rows) are
-  // staged in shared memory, then written after one cluster barrier
+  // Rows that moved register (from, to) in CTA 0's list, for the block's
+  // other columns.  After one cluster barrier (which also orders the
+  // multipliers stored during the loop before what follows), a row that
+  // moved writes its whole panel row at its final place, a pivot row that
+  // stayed its U part.
   const bool in = r < M;
-  if (in) {
-#pragma unroll 4
-    for (int k = 0; k < ncols; k++) A[pos + (long)k * lda] = Lsm[k * PT + tid];
-  }
-  // The block's other columns of the rows that moved (at most 2*MN rows,
-  // most of them in CTA 0, whose rows include the top of the panel): the
-  // list of moves is gathered in CTA 0, and every CTA copies an equal share
-  // of the (move, column) pairs through its shared memory, with a cluster
-  // barrier between all reads and all writes.
   const int nother = nleft + nright;
-  __syncthreads();  // Lsm is free from here on
   if (nother > 0 && in && pos != r) {
     int *cnt0 = cl.map_shared_rank(&s_nmoved, 0);
     const int i = atomicAdd(cnt0, 1);
@@ -570,43 +588,57 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
   __syncwarp();
   cluster_arrive();
   cluster_wait();
+  if (in && (pos != r || piv_row)) {
+    const int k0 = pos != r ? 0 : pos;
+    for (int k = k0; k < ncols; k++) A[pos + (long)k * lda] = Lsm[k * PT + tid];
+  }
+  if (nother == 0) return;
+  // The block's other columns of the rows that moved (at most 2*MN rows):
+  // CTA q takes an equal share of the columns, reads the moved rows' old
+  // values into shared memory and writes them to their final rows.
   __shared__ int l_from[2 * NB], l_to[2 * NB];
-  const int nm = nother > 0 ? min(*cl.map_shared_rank(&s_nmoved, 0), 2 * NB) : 0;
+  const int nm = min(*cl.map_shared_rank(&s_nmoved, 0), 2 * NB);
   if (tid < nm) {
     l_from[tid] = cl.map_shared_rank(s_from, 0)[tid];
     l_to[tid] = cl.map_shared_rank(s_to, 0)[tid];
   }
-  __syncthreads();
-  const int total = nm * nother, per = (total + C - 1) / C;
-  const int g0 = crank * per, g1 = min(total, g0 + per);
-  for (int base = g0 + tid; base < g1; base += 4 * PT) {
+  __syncthreads();  // the list is here and Lsm is free
+  // CTA 0's shared memory must outlive the other CTAs' reads of its list: a
+  // cluster barrier follows them before any CTA exits
+  const bool u12 = nright > 0 && MN > 1;
+  if (!u12) cluster_arrive();
+  const int per = (nother + C - 1) / C, g0 = crank * per, ncol = max(0, min(nother, g0 + per) - g0);
+  const int total = nm * ncol;  // <= 2 NB x NB*PT/(2 NB): fits Lsm
+  for (int base = tid; base < total; base += 4 * PT) {
     T v[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const int g = base + q * PT;
-      if (g < g1) {
-        const int i = g / nother, c = g - i * nother;
+      if (g < total) {
+        const int i = g % nm, c = g0 + g / nm;
         const int col = c < nleft ? c - nleft : ncols + (c - nleft);
         v[q] = __ldcg(A + l_from[i] + (long)col * lda);
       }
     }
 #pragma unroll
     for (int q = 0; q < 4; q++)
-      if (base + q * PT < g1) Lsm[base + q * PT - g0] = v[q];
+      if (base + q * PT < total) Lsm[base + q * PT] = v[q];
   }
-  __syncwarp();
-  cluster_arrive();
-  cluster_wait();
-  for (int g = g0 + tid; g < g1; g += PT) {
-    const int i = g / nother, c = g - i * nother;
+  __syncthreads();
+  for (int g = tid; g < total; g += PT) {
+    const int i = g % nm, c = g0 + g / nm;
     const int col = c < nleft ? c - nleft : ncols + (c - nleft);
-    A[l_to[i] + (long)col * lda] = Lsm[g - g0];
+    A[l_to[i] + (long)col * lda] = Lsm[g];
+  }
+  if (!u12) {
+    cluster_wait();
+    return;
   }
   __syncwarp();
   cluster_arrive();  // every row is in place
   cluster_wait();
-  // U12 = L11^-1 A12 on the right columns' top MN rows (L11 unit lower)
-  if (crank == 0 && nright > 0 && MN > 1) panel_u12_solve<T, NB>(MN, ncols, nright, A, lda, fused_smem);
+  // U12 = L11^-1 A12 on the right columns' top MN rows, over all the cluster's warps
+  panel_u12_solve<T, NB>(MN, ncols, nright, crank * (PT / 32) + warp, C * (PT / 32), A, lda);
 }
 
 // Tournament-pivoting panel for the FP32 factorization inside the
@@ -871,7 +903,7 @@ getf2_tournament_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__re
   __syncwarp();
   cluster_arrive();  // every row is in place
   cluster_wait();
-  if (crank == 0 && nright > 0 && MN > 1) panel_u12_solve<T, NB>(MN, ncols, nright, A, lda, tourn_smem);
+  if (crank == 0 && nright > 0 && MN > 1) panel_u12_solve<T, NB>(MN, ncols, nright, warp, PT / 32, A, lda);
 }
 
 // Fallback for panels taller than a cluster can hold: one CTA, global memory.
