@@ -467,26 +467,14 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
         stage.key = K(0);
         stage.pos = -1;
       }
-      // kUnits x C messages spread over the warp's lanes, 16 bytes each
-      __syncwarp();
-      const uint4 *src = reinterpret_cast<const uint4 *>(&stage);
-      const uint32_t dst = smem_u32(&slot[b][crank]);
-      if (sizeof(T) == 4) {
-        constexpr int kItems = (kUnits * kMaxPanelCluster + 31) / 32;
-#pragma unroll
-        for (int i = 0; i < kItems; i++) {
-          const int it = lane + 32 * i;
-          if (it < kUnits * C) {
-            const int q = it / kUnits, unit = it - q * kUnits;
-            st_async16(mapa_u32(dst + 16 * unit, q), src[unit], mapa_u32(mb, q));
-          }
-        }
-      } else {
-        for (int it = lane; it < kUnits * C; it += 32) {
-          const int q = it / kUnits, unit = it - q * kUnits;
-          st_async16(mapa_u32(dst + 16 * unit, q), src[unit], mapa_u32(mb, q));
-        }
-      }
+    }
+    // kUnits x C messages of 16 bytes, at most one per thread
+    static_assert(kUnits * kMaxPanelCluster <= PT, "one message per thread");
+    __syncthreads();
+    if (tid < kUnits * C) {
+      const int q = tid / kUnits, unit = tid - q * kUnits;
+      st_async16(mapa_u32(smem_u32(&slot[b][crank]) + 16 * unit, q), reinterpret_cast<const uint4 *>(&stage)[unit],
+                 mapa_u32(mb, q));
     }
   };
   // wait until column c's C messages are in this CTA's slots
