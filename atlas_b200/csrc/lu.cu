@@ -1208,8 +1208,9 @@ void getrf_rec(int off, int M, int N, T *A, long lda, int *ipiv, int *dinfo, cud
 // panel.  Small and skinny, so a plain GEMM pays its K-loop pipeline and
 // tiling for a single 32-deep step; here one CTA loads all of B and a
 // 16*RT-row slice of A into shared memory once, every thread computes RT
-// rows x up to 16 columns, and the old C values are loaded before any
-// result is stored.
+// rows (16 apart, so a half-warp touches 16 consecutive rows of a column)
+// x up to 16 columns, and the old C values are loaded before any result is
+// stored.
 template <typename T, int RT>
 __global__ void __launch_bounds__(256)
 rank_update_kernel(int m, int nr, int k, const T *__restrict__ A, const T *__restrict__ B, T *__restrict__ C,
@@ -1229,7 +1230,7 @@ rank_update_kernel(int m, int nr, int k, const T *__restrict__ A, const T *__res
     sB[i * nrp + c] = (i < k && c < nr) ? B[i + (long)c * lda] : T(0);
   }
   __syncthreads();
-  const int tr = tid % 16, tc = tid / 16;  // rows tr*RT .. +RT-1, columns tc + 16 q
+  const int tr = tid % 16, tc = tid / 16;  // rows tr + 16 a, columns tc + 16 q
   const int nq = (nr - tc + 15) / 16;      // this thread's columns (<= 16)
   T acc[RT][16];
 #pragma unroll
@@ -1240,7 +1241,7 @@ rank_update_kernel(int m, int nr, int k, const T *__restrict__ A, const T *__res
   for (int i = 0; i < 32; i++) {
     T av[RT];
 #pragma unroll
-    for (int a = 0; a < RT; a++) av[a] = sA[i][tr * RT + a];
+    for (int a = 0; a < RT; a++) av[a] = sA[i][tr + 16 * a];
 #pragma unroll
     for (int q = 0; q < 16; q++) {
       if (q < nq) {  // sB holds nrp columns only
@@ -1255,14 +1256,14 @@ rank_update_kernel(int m, int nr, int k, const T *__restrict__ A, const T *__res
   for (int q = 0; q < 16; q++)
 #pragma unroll
     for (int a = 0; a < RT; a++) {
-      const int r = r0 + tr * RT + a, c = tc + 16 * q;
+      const int r = r0 + tr + 16 * a, c = tc + 16 * q;
       old[a][q] = (q < nq && r < m) ? C[r + (long)c * lda] : T(0);
     }
 #pragma unroll
   for (int q = 0; q < 16; q++)
 #pragma unroll
     for (int a = 0; a < RT; a++) {
-      const int r = r0 + tr * RT + a, c = tc + 16 * q;
+      const int r = r0 + tr + 16 * a, c = tc + 16 * q;
       if (q < nq && r < m) C[r + (long)c * lda] = old[a][q] - acc[a][q];
     }
 }

@@ -80,7 +80,6 @@ trsv_kernel(int n, int nrhs, const T *__restrict__ Tp, long tr, long tc, int low
       const uint64_t t0 = gtimer();
       while (ld_acquire(flags + bj) != epoch) {
         if (gtimer() - t0 > 1000000000ull) { atomicExch(err, 1); break; }
-        __nanosleep(32);
       }
     }
     __syncwarp();
@@ -103,17 +102,24 @@ trsv_kernel(int n, int nrhs, const T *__restrict__ Tp, long tr, long tc, int low
     sx[rr][q] = sb[rr][q] - (sacc[0][rr][q] + sacc[1][rr][q] + sacc[2][rr][q] + sacc[3][rr][q]);
   }
   __syncthreads();
+  // x = W (b - acc): thread (r, part) sums columns part*16 .. +15 of row r
+  // (four short chains instead of one 64-long one), then the parts add up
+#pragma unroll
+  for (int q = 0; q < NR; q++) {
+    T v = T(0);
+#pragma unroll
+    for (int c = 16 * part; c < 16 * part + 16; c++) v = fma(sW[r][c], sx[c][q], v);
+    sacc[part][r][q] = v;
+  }
+  __syncthreads();
   for (int idx = tid; idx < BS * NR; idx += 256) {
     const int rr = idx % BS, q = idx / BS;
     if (rr >= rows || q >= nrhs) continue;
-    T v = T(0);
-#pragma unroll 8
-    for (int c = 0; c < BS; c++) v = fma(sW[rr][c], sx[c][q], v);
-    X[r0 + rr + (long)q * ldx] = v;
+    X[r0 + rr + (long)q * ldx] = (sacc[0][rr][q] + sacc[1][rr][q]) + (sacc[2][rr][q] + sacc[3][rr][q]);
   }
-  __threadfence();
   __syncthreads();
-  if (tid == 0) {
+  if (tid == 0) {  // the barrier orders every thread's x stores before this release
+    __threadfence();
     asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(flags + bi), "r"(epoch) : "memory");
   }
 }
