@@ -54,6 +54,10 @@ void gemm_dev(int ta, int tb, int M, int N, int K, T alpha, const T *A, long lda
 template <typename T>
 void trsm_dev(int side, int uplo, int trans, int diag, int M, int N, T alpha, const T *A, long lda,
               T *B, long ldb, cudaStream_t st, SgemmFn gemm = nullptr);
+// B = L^-1 B for L unit lower triangular of order m <= 256 (left, lower,
+// no transpose, unit diagonal) in one launch.
+template <typename T>
+void trsm_llu_small_dev(int m, int n, const T *L, long lda, T *B, long ldb, cudaStream_t st);
 // The TRSM with its workspace supplied: W holds ceil(n/64) blocks of 64x64
 // elements (n = order of the triangle).
 template <typename T>

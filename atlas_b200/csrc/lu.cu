@@ -1339,7 +1339,7 @@ void getrf_dev(int M, int N, T *A, long lda, int *ipiv, int *dinfo, cudaStream_t
         if (nr > 0) {
           T *A12 = Ad + (long)jb * lda;
           laswp_dev<T>(nr, A + (long)(j + jb) * lda, lda, j, j + jb, ipiv, 1, st);
-          trsm_dev<T>(kLeft, kLower, kNoTrans, kUnit, jb, nr, T(1), Ad, lda, A12, lda, st, gemm);
+          trsm_llu_small_dev<T>(jb, nr, Ad, lda, A12, lda, st);
           if (M - j - jb > 0) update_gemm(gemm, M - j - jb, nr, jb, Ad + jb, A12, A12 + jb, lda, st);
         }
       }
@@ -1365,7 +1365,7 @@ void getrf_dev(int M, int N, T *A, long lda, int *ipiv, int *dinfo, cudaStream_t
           SideScope side;
           T *An = A + (long)jn * lda;
           laswp_dev<T>(jbn, An, lda, j, jn, ipiv, 1, s1);
-          trsm_dev<T>(kLeft, kLower, kNoTrans, kUnit, jb, jbn, T(1), Ad, lda, An + j, lda, s1, gemm);
+          trsm_llu_small_dev<T>(jb, jbn, Ad, lda, An + j, lda, s1);
           if (M - jn > 0) update_gemm(gemm, M - jn, jbn, jb, Ad + jb, An + j, An + jn, lda, s1);
           if (!getrf_block<T>(jn, M, jbn, A, lda, ipiv, dinfo, s1, gemm))
             getrf_rec<T>(jn, M - jn, jbn, A, lda, ipiv, dinfo, s1, gemm);
@@ -1376,7 +1376,7 @@ void getrf_dev(int M, int N, T *A, long lda, int *ipiv, int *dinfo, cudaStream_t
         if (nr > 0) {
           T *Ar = A + (long)c0 * lda;
           laswp_dev<T>(nr, Ar, lda, j, jn, ipiv, 1, st);
-          trsm_dev<T>(kLeft, kLower, kNoTrans, kUnit, jb, nr, T(1), Ad, lda, Ar + j, lda, st, gemm);
+          trsm_llu_small_dev<T>(jb, nr, Ad, lda, Ar + j, lda, st);
           // the trailing update may leave SMs to the side stream's panel
           const int reserve = jbn > 0 ? tune(kTuneLookaheadReserve) : 0;
           GemmCtaCap cap(reserve > 0 ? std::max(1, num_sms() - reserve) : 0);

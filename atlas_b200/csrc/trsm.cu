@@ -489,6 +489,106 @@ template void trsm_dev<double>(int, int, int, int, int, int, double, const doubl
 template void trsm_dev<float>(int, int, int, int, int, int, float, const float *, long, float *,
                               long, cudaStream_t, SgemmFn);
 
+namespace {
+// X = L^-1 B in place, L unit lower triangular of order m <= 256, B m x n:
+// the U12 = L11^-1 A12 step of the blocked LU in ONE launch (the recursive
+// trsm_dev issues a TRSM/GEMM cascade of ~8 kernels for it).  CTA q solves
+// columns 32q .. 32q+31, the whole column tile in shared memory: for each
+// 32-row block, the product of L's 32 x (32 ib) panel with the rows already
+// solved (L read in 32 x 32 tiles, the next tile fetched into registers while
+// the current one is used), then forward substitution with the unit lower
+// 32 x 32 diagonal tile (lane = row, x_k by shuffle, four columns per warp).
+constexpr int LLU_COLS = 32, LLU_MAX = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(256, 1)
+trsm_llu_small_kernel(int m, int n, const T *__restrict__ L, long lda, T *B, long ldb) {
+  extern __shared__ __align__(16) unsigned char llu_smem[];
+  T(*sX)[LLU_COLS + 1] = reinterpret_cast<T(*)[LLU_COLS + 1]>(llu_smem);  // [LLU_MAX]: B, then X
+  T(*sL)[33] = reinterpret_cast<T(*)[33]>(sX + LLU_MAX);                  // [32]: one tile of L
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int c0 = blockIdx.x * LLU_COLS, nc = min(LLU_COLS, n - c0);
+  for (int idx = tid; idx < LLU_MAX * LLU_COLS; idx += 256) {
+    const int r = idx % LLU_MAX, c = idx / LLU_MAX;
+    sX[r][c] = (r < m && c < nc) ? B[r + (long)(c0 + c) * ldb] : T(0);
+  }
+  const int nblk = (m + 31) / 32;
+  const int rr = tid % 32, cq = tid / 32;  // update: row rr of the block, columns 4 cq .. 4 cq + 3
+  // a thread's four elements of an L tile (rows r0 + i, columns k0 + k)
+  auto fetch = [&](int r0, int k0, T (&v)[4]) {
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const int idx = tid + 256 * e, i = idx % 32, k = idx / 32;
+      v[e] = (r0 + i < m && k0 + k < m) ? L[r0 + i + (long)(k0 + k) * lda] : T(0);
+    }
+  };
+  auto store = [&](const T (&v)[4]) {
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const int idx = tid + 256 * e;
+      sL[idx % 32][idx / 32] = v[e];
+    }
+  };
+  for (int ib = 0; ib < nblk; ib++) {
+    const int r0 = ib * 32;
+    T acc[4] = {T(0), T(0), T(0), T(0)};
+    T nxt[4];
+    fetch(r0, 0, nxt);  // tile (ib, 0), or the diagonal tile when ib == 0
+    for (int kt = 0; kt < ib; kt++) {
+      __syncthreads();  // the previous tile has been used
+      store(nxt);
+      __syncthreads();
+      fetch(r0, (kt + 1) * 32, nxt);  // the next tile (the diagonal one after the last)
+#pragma unroll 8
+      for (int k = 0; k < 32; k++) {
+        const T lv = sL[rr][k];
+#pragma unroll
+        for (int e = 0; e < 4; e++) acc[e] = fma(lv, sX[kt * 32 + k][4 * cq + e], acc[e]);
+      }
+    }
+    __syncthreads();  // every thread is done with sL and the rows it read
+#pragma unroll
+    for (int e = 0; e < 4; e++) sX[r0 + rr][4 * cq + e] -= acc[e];
+    store(nxt);       // the diagonal tile
+    __syncthreads();
+    T x[4];
+#pragma unroll
+    for (int e = 0; e < 4; e++) x[e] = sX[r0 + lane][4 * warp + e];
+#pragma unroll
+    for (int k = 0; k < 31; k++) {
+      const T lk = sL[lane][k];
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const T xk = __shfl_sync(0xffffffffu, x[e], k);
+        if (lane > k) x[e] = fma(-lk, xk, x[e]);
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < 4; e++) sX[r0 + lane][4 * warp + e] = x[e];
+    __syncthreads();
+  }
+  for (int idx = tid; idx < LLU_MAX * LLU_COLS; idx += 256) {
+    const int r = idx % LLU_MAX, c = idx / LLU_MAX;
+    if (r < m && c < nc) B[r + (long)(c0 + c) * ldb] = sX[r][c];
+  }
+}
+}  // namespace
+
+template <typename T>
+void trsm_llu_small_dev(int m, int n, const T *L, long lda, T *B, long ldb, cudaStream_t st) {
+  if (m <= 0 || n <= 0) return;
+  constexpr int smem = (LLU_MAX * (LLU_COLS + 1) + 32 * 33) * (int)sizeof(T);
+  static bool configured = false;
+  if (!configured) {
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(trsm_llu_small_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    configured = true;
+  }
+  trsm_llu_small_kernel<T><<<cdiv(n, LLU_COLS), 256, smem, st>>>(m, n, L, lda, B, ldb);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
+template void trsm_llu_small_dev<double>(int, int, const double *, long, double *, long, cudaStream_t);
+template void trsm_llu_small_dev<float>(int, int, const float *, long, float *, long, cudaStream_t);
+
 void dtrmm_dev(int side, int uplo, int trans, int diag, int M, int N, double alpha,
                const double *A, long lda, double *B, long ldb, cudaStream_t st) {
   if (M <= 0 || N <= 0) return;
