@@ -332,11 +332,39 @@ laswp_plan_kernel(int k1, int k2, const int *__restrict__ ipiv, int inc, int *__
     }
   }
   __syncthreads();
-  for (int r = tid; r < span; r += blockDim.x) {
+  // the moves in increasing destination order (a block-wide prefix count), so
+  // that the apply kernel's neighbouring threads touch neighbouring rows
+  __shared__ int s_wsum[32];
+  const int chunk = (span + blockDim.x - 1) / blockDim.x, rbeg = tid * chunk, rend = min(span, rbeg + chunk);
+  int cnt = 0;
+  for (int r = rbeg; r < rend; r++) cnt += perm[r] != k1 + r;
+  const int lane = tid & 31, wid = tid >> 5;
+  int isc = cnt;  // inclusive scan within the warp
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, isc, o);
+    if (lane >= o) isc += v;
+  }
+  if (lane == 31) s_wsum[wid] = isc;
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x / 32;
+    int w = lane < nw ? s_wsum[lane] : 0, wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += v;
+    }
+    if (lane < nw) s_wsum[lane] = wi - w;  // exclusive warp offsets
+    if (lane == nw - 1) s_cnt = wi;
+  }
+  __syncthreads();
+  int slot = s_wsum[wid] + isc - cnt;
+  for (int r = rbeg; r < rend; r++) {
     if (perm[r] != k1 + r) {
-      const int slot = atomicAdd(&s_cnt, 1);
-      moves[2 * slot] = k1 + r;     // destination row
+      moves[2 * slot] = k1 + r;       // destination row
       moves[2 * slot + 1] = perm[r];  // source row
+      slot++;
     }
   }
   __syncthreads();
@@ -350,13 +378,14 @@ laswp_apply_kernel(int ncols, T *A, long lda, const int *__restrict__ moves, con
   T *buf = reinterpret_cast<T *>(lsw_smem);  // [2*LSW_MAXP][LSW_COLS]
   const int nm = *nmoves, c0 = blockIdx.x * LSW_COLS, tid = threadIdx.x;
   const int nc = min(LSW_COLS, ncols - c0);
+  // moves fastest: neighbouring threads take neighbouring (sorted) rows of one column
   for (int idx = tid; idx < nm * LSW_COLS; idx += 256) {
-    const int m = idx / LSW_COLS, c = idx % LSW_COLS;
+    const int m = idx % nm, c = idx / nm;
     if (c < nc) buf[idx] = A[moves[2 * m + 1] + (long)(c0 + c) * lda];
   }
   __syncthreads();
   for (int idx = tid; idx < nm * LSW_COLS; idx += 256) {
-    const int m = idx / LSW_COLS, c = idx % LSW_COLS;
+    const int m = idx % nm, c = idx / nm;
     if (c < nc) A[moves[2 * m] + (long)(c0 + c) * lda] = buf[idx];
   }
 }
