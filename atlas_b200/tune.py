@@ -6,8 +6,9 @@ beside the library, which reads it on first use.
 
     python -m atlas_b200.tune [--n 8192] [--out PATH]
 
-Parameters (see atlas_b200/csrc/tuning.cu): getrf_nb, lookahead, potrf_nb,
-dgemm_group, dgemm_splitk, mixed_tc_min_work_log2.
+Parameters (see atlas_b200/csrc/tuning.cu): getrf_nb, lookahead,
+lookahead_reserve_sms, potrf_nb, dgemm_group, dgemm_splitk,
+mixed_tc_min_work_log2.
 """
 import argparse
 import os
@@ -19,15 +20,18 @@ import atlas_b200 as AB
 
 
 def _timer(torch, stream, fn, reps):
+    """Median of `reps` individually timed calls (after one untimed call)."""
     fn()
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
+    times = []
     for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
         fn()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    return e0.elapsed_time(e1) / reps
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return sorted(times)[len(times) // 2]
 
 
 def main():
@@ -82,20 +86,28 @@ def main():
     x = torch.empty(n, dtype=f64, device=dev)
     b = torch.rand(n, dtype=f64, device=dev, generator=g) * 2 - 1
     it = np.zeros(1, dtype=np.int32)
-    a_mixed = a_lu.clone()
+    # the mixed solvers are timed on the matrix class of the dgesv benchmark:
+    # Q1 diag(s) Q2^T, Q from QR of Gaussian matrices, s geometric, cond 1e2
+    q1, _ = torch.linalg.qr(torch.randn(n, n, dtype=f64, device=dev, generator=g))
+    q2, _ = torch.linalg.qr(torch.randn(n, n, dtype=f64, device=dev, generator=g))
+    sv = torch.logspace(0, -2, n, dtype=f64, device=dev)
+    a_mixed = ((q1 * sv) @ q2.T).T.contiguous()
+    del q1, q2
+    a_mixed0 = a_mixed.clone()
 
     def mixed():
         AB.atlb_dsgesv_ex(n, 1, a_mixed, n, ipiv, b, n, x, n, 3, 0, it)
         if it[0] < 0:
-            a_mixed.copy_(a_lu)
+            a_mixed.copy_(a_mixed0)
 
     search = [
         ("getrf_nb", [128, 192, 256], getrf, 3),
         ("lookahead", [0, 1], getrf, 3),
+        ("lookahead_reserve_sms", [0, 8, 16], getrf, 3),
         ("potrf_nb", [128, 256, 384, 512], potrf, 3),
         ("dgemm_group", [4, 8, 16], dgemm_big, 3),
         ("dgemm_splitk", [0, 1], dgemm_small, 5),
-        ("mixed_tc_min_work_log2", [26, 29, 31, 34], mixed, 3),
+        ("mixed_tc_min_work_log2", [24, 26, 28, 31], mixed, 7),
     ]
     lines = [f"# atlas_b200 tuning, {time.strftime('%Y-%m-%d %H:%M:%S')}, "
              f"{torch.cuda.get_device_name(0)}, factorization order {n}"]
