@@ -1319,7 +1319,8 @@ template <typename T>
 void getrf_dev(int M, int N, T *A, long lda, int *ipiv, int *dinfo, cudaStream_t st,
                SgemmFn gemm) {
   // the launch sequence depends only on (M, N, lda, pointers): replayed as a graph
-  const int NBO = tune(kTuneGetrfNB);  // multiple of 32, <= 256 (the fused panel's limit)
+  // multiple of 32, <= 256 (the fused panel's limit); the FP32 factorization has its own
+  const int NBO = tune(sizeof(T) == 4 ? kTuneSgetrfNB : kTuneGetrfNB);
   const std::vector<unsigned long long> key = {1ull + sizeof(T), (unsigned long long)tune_generation(),
       (unsigned long long)M,
       (unsigned long long)N, (unsigned long long)lda, (unsigned long long)(uintptr_t)A,

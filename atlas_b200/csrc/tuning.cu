@@ -34,6 +34,7 @@ const TuneDef kDefs[kNumTune] = {
     {"lookahead", 1, 0, 1, 1},                // depth-one look-ahead in getrf / potrf
     {"mixed_tc_min_work_log2", 31, 16, 40, 1},  // mixed solvers: M*N*K below 2^x runs on FP32 FMA
     {"lookahead_reserve_sms", 0, 0, 96, 1},   // SMs the trailing-update DGEMM leaves to the look-ahead panel
+    {"sgetrf_nb", 256, 64, 256, 32},          // outer LU block of the FP32 factorization (mixed solvers)
 };
 
 std::atomic<int> g_val[kNumTune];

@@ -7,7 +7,7 @@ beside the library, which reads it on first use.
     python -m atlas_b200.tune [--n 8192] [--out PATH]
 
 Parameters (see atlas_b200/csrc/tuning.cu): getrf_nb, lookahead,
-lookahead_reserve_sms, potrf_nb, dgemm_group, dgemm_splitk,
+lookahead_reserve_sms, potrf_nb, dgemm_group, dgemm_splitk, sgetrf_nb,
 mixed_tc_min_work_log2.
 """
 import argparse
@@ -107,6 +107,7 @@ def main():
         ("potrf_nb", [128, 256, 384, 512], potrf, 3),
         ("dgemm_group", [4, 8, 16], dgemm_big, 3),
         ("dgemm_splitk", [0, 1], dgemm_small, 5),
+        ("sgetrf_nb", [192, 256], mixed, 7),
         ("mixed_tc_min_work_log2", [24, 26, 28, 31], mixed, 7),
     ]
     lines = [f"# atlas_b200 tuning, {time.strftime('%Y-%m-%d %H:%M:%S')}, "

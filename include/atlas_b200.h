@@ -130,7 +130,8 @@ int atlb_dsyrk_dev(int Uplo, int Trans, int N, int K, double alpha, const double
  * candidates on the GPU and writes tuning.conf beside the library, which is
  * read on first use (ATLAS_B200_TUNE_FILE overrides the path, "none" skips
  * it).  Names: getrf_nb, potrf_nb, dgemm_group, dgemm_splitk, lookahead,
- * mixed_tc_min_work_log2.  get returns INT_MIN for an unknown name; set
+ * mixed_tc_min_work_log2, lookahead_reserve_sms, sgetrf_nb.  get returns
+ * INT_MIN for an unknown name; set
  * returns the stored (clamped) value or -1; load returns the number of values
  * read or -1. */
 int atlb_tune_get(const char *name);
