@@ -117,14 +117,20 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-template <int KIND, int BN, int STAGES, int EPI>
+// MS M-subtiles of BM rows per CTA: each k-step issues MS MMAs that share
+// the stage's B tile, into MS accumulators side by side in TMEM (MS * BN
+// columns); a 256 x 256 tile moves half the operand bytes per product of a
+// 128 x 256 one.
+template <int KIND, int BN, int STAGES, int EPI, int MS = 1>
 __global__ void __launch_bounds__(THREADS, 1)
 tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                int M, int N, int K, EpiParams ep, int *err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1024-byte aligned base for the swizzled tiles
   unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  constexpr int A_BYTES = BM * SLAB, B_BYTES = BN * SLAB, STAGE = A_BYTES + B_BYTES;
+  constexpr int BMT = BM * MS;  // rows of the CTA's tile
+  static_assert(MS * BN <= 512, "TMEM holds 512 columns");
+  constexpr int A_BYTES = BMT * SLAB, B_BYTES = BN * SLAB, STAGE = A_BYTES + B_BYTES;
   uint64_t *bars = (uint64_t *)(smem + STAGES * STAGE);
   uint32_t *tmem_slot = (uint32_t *)(bars + 2 * STAGES + 1);
   const uint32_t sbase = smem_u32(smem);
@@ -134,8 +140,8 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int tiles_n = (N + BN - 1) / BN;
   const int tm = blockIdx.x / tiles_n, tn = blockIdx.x % tiles_n;
-  const int m0 = tm * BM, n0 = tn * BN;
-  if (EPI == kEpiF32 && ep.tri == 1 && m0 + BM - 1 < n0) return;
+  const int m0 = tm * BMT, n0 = tn * BN;
+  if (EPI == kEpiF32 && ep.tri == 1 && m0 + BMT - 1 < n0) return;
   if (EPI == kEpiF32 && ep.tri == 2 && m0 > n0 + BN - 1) return;
 
   constexpr int ELEM = (KIND == kKindBF16) ? 2 : (KIND == kKindTF32 ? 4 : 1);
@@ -153,9 +159,9 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
-  if (warp == 2) {  // allocate BN TMEM columns (power of two >= 32)
+  if (warp == 2) {  // allocate MS * BN TMEM columns (power of two >= 32)
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                 ::"r"(smem_u32(tmem_slot)), "r"(BN));
+                 ::"r"(smem_u32(tmem_slot)), "r"(MS * BN));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -184,8 +190,10 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       const uint32_t a_addr = sbase + s * STAGE, b_addr = a_addr + A_BYTES;
 #pragma unroll
       for (int k = 0; k < KPS / KPM; k++) {
-        mma_issue<KIND>(tmem, smem_desc(a_addr + k * 32), smem_desc(b_addr + k * 32), idesc,
-                        (kb > 0 || k > 0) ? 1u : 0u);
+#pragma unroll
+        for (int ms = 0; ms < MS; ms++)
+          mma_issue<KIND>(tmem + ms * BN, smem_desc(a_addr + ms * BM * SLAB + k * 32), smem_desc(b_addr + k * 32),
+                          idesc, (kb > 0 || k > 0) ? 1u : 0u);
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                    ::"r"(bar_empty + 8 * s) : "memory");
@@ -202,12 +210,14 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   __syncwarp();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (!done) atomicExch(err, 3);
-  const int m = m0 + warp * 32 + lane;
+#pragma unroll 1
+  for (int ms = 0; ms < MS; ms++) {
+  const int m = m0 + ms * BM + warp * 32 + lane;
   if (done && nkb > 0) {
 #pragma unroll 1
     for (int c = 0; c < BN / 32; c++) {
       uint32_t r[32];
-      tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + c * 32, r);
+      tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + ms * BN + c * 32, r);
       if (m < M) {
         // all 32 old values of C first (independent loads, latencies overlap),
         // then the 32 results: the loads are not serialized behind the stores
@@ -253,10 +263,11 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       *p = ep.beta == 0.f ? 0.f : ep.beta * *p;
     }
   }
+  }  // M-subtiles
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 2) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(MS * BN));
   }
 }
 
@@ -308,23 +319,23 @@ int *err_flag() {
   return d;
 }
 
-template <int KIND, int BN, int STAGES, int EPI>
+template <int KIND, int BN, int STAGES, int EPI, int MS = 1>
 void launch_t(const void *A, long lda, const void *B, long ldb, int M, int N, int K,
               const EpiParams &ep, cudaStream_t st) {
   CUtensorMap ma, mb;
-  if (!make_map(&ma, KIND, A, M, K, lda, BM) || !make_map(&mb, KIND, B, N, K, ldb, BN)) {
+  if (!make_map(&ma, KIND, A, M, K, lda, BM * MS) || !make_map(&mb, KIND, B, N, K, ldb, BN)) {
     fprintf(stderr, "atlas_b200: tensor-map encoding failed (alignment)\n");
     set_cuda_error(cudaErrorInvalidValue);
     return;
   }
-  constexpr int smem = STAGES * (BM + BN) * SLAB + 1024 + (2 * STAGES + 2) * 8 + 16;
-  auto kern = tc_gemm_kernel<KIND, BN, STAGES, EPI>;
+  constexpr int smem = STAGES * (BM * MS + BN) * SLAB + 1024 + (2 * STAGES + 2) * 8 + 16;
+  auto kern = tc_gemm_kernel<KIND, BN, STAGES, EPI, MS>;
   static bool configured = false;
   if (!configured) {
     ATLB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     configured = true;
   }
-  const int tiles = cdiv(M, BM) * cdiv(N, BN);
+  const int tiles = cdiv(M, BM * MS) * cdiv(N, BN);
   kern<<<tiles, THREADS, smem, st>>>(ma, mb, M, N, K, ep, err_flag());
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
@@ -337,7 +348,9 @@ void tc_gemm(int kind, int epi, const void *A, long lda, const void *B, long ldb
   } else if (kind == kKindTF32) {
     if (epi == kEpiF32) launch_t<kKindTF32, 128, 6, kEpiF32>(A, lda, B, ldb, M, N, K, ep, st);
   } else {
-    if (epi == kEpiF64Acc) launch_t<kKindI8, 128, 6, kEpiF64Acc>(A, lda, B, ldb, M, N, K, ep, st);
+    // 256 x 256 tiles (two 128-row accumulators): half the operand traffic
+    // per product of 128 x 128 tiles
+    if (epi == kEpiF64Acc) launch_t<kKindI8, 256, 3, kEpiF64Acc, 2>(A, lda, B, ldb, M, N, K, ep, st);
   }
 }
 
