@@ -66,7 +66,7 @@ enum ScratchSlot {
   kSlotInfo, kSlotMixedA, kSlotMixedR, kSlotMixedX, kSlotMixedD,
   kSlotOzA, kSlotOzB, kSlotOzScale, kSlotBatch0, kSlotBatch1, kSlotBatch2,
   kSlotBatch3, kSlotAdj0, kSlotAdj1, kSlotAdj2, kSlotTc0, kSlotTc1, kSlotTrsmW, kSlotTrsvCtl, kSlotLaswp,
-  kSlotMixedWL, kSlotMixedWU, kSlotMixedPerm, kSlotGemmSplit,
+  kSlotMixedWL, kSlotMixedWU, kSlotMixedPerm, kSlotGemmSplit, kSlotPermPlan,
   kNumSlots
 };
 

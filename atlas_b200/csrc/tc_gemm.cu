@@ -376,17 +376,25 @@ __global__ void to_kmajor_kernel(int rows, int K, const float *__restrict__ X, l
   __shared__ float t[32][33];
   const int r0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
   const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
-  for (int j = ty; j < 32; j += 8) {
+  float v[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {  // the four loads in flight together
+    const int j = ty + 8 * q;
     int r, k;
     if (rcontig) { r = r0 + tx; k = k0 + j; } else { k = k0 + tx; r = r0 + j; }
-    float v = (r < rows && k < K) ? X[rcontig ? (r + (long)k * ld) : (k + (long)r * ld)] : 0.f;
-    if (rcontig) t[j][tx] = v; else t[tx][j] = v;  // t[k_local][r_local]
+    v[q] = (r < rows && k < K) ? X[rcontig ? (r + (long)k * ld) : (k + (long)r * ld)] : 0.f;
+  }
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int j = ty + 8 * q;
+    if (rcontig) t[j][tx] = v[q]; else t[tx][j] = v[q];  // t[k_local][r_local]
   }
   __syncthreads();
-  for (int j = ty; j < 32; j += 8) {
-    const int r = r0 + j, k = k0 + tx;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int j = ty + 8 * q, r = r0 + j, k = k0 + tx;
     if (r < rows && k < K) {
-      float v = t[tx][j];
+      const float v = t[tx][j];
       if (KIND == kKindBF16) {
         ((unsigned short *)out)[k + (long)r * ldo] = __bfloat16_as_ushort(__float2bfloat16_rn(v));
       } else {
@@ -403,29 +411,51 @@ __global__ void to_kmajor_kernel(int rows, int K, const float *__restrict__ X, l
 // TF32-rounded remainder x - hi(x) (bit q = 1).  A uses [hi lo hi], B uses
 // [hi hi lo], so one GEMM over K' = 3*ldk sums hi*hi + lo*hi + hi*lo, the
 // FP32-accurate product (the lo*lo term is below FP32 rounding).
-__global__ void to_kmajor_split_kernel(int rows, int K, const float *__restrict__ X, long ld,
-                                       int rcontig, float *__restrict__ out, long ldk, int pat) {
+struct SplitOperand {
+  int rows, K;
+  const float *X;
+  long ld;
+  int rcontig;  // X(r, k) at r + k*ld (else k + r*ld)
+  float *out;
+  int pat;
+};
+// Both operands of one GEMM in one launch: CTAs with blockIdx.y < ya convert
+// A's 32 x 32 tiles, the others B's.  Each thread's four loads are issued
+// before any is used.
+__global__ void __launch_bounds__(256)
+to_kmajor_split_kernel(SplitOperand opa, SplitOperand opb, int ya, long ldk) {
   __shared__ float t[32][33];
-  const int r0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
+  const bool isa = (int)blockIdx.y < ya;
+  const SplitOperand &op = isa ? opa : opb;
+  const int r0 = (isa ? blockIdx.y : blockIdx.y - ya) * 32, k0 = blockIdx.x * 32;
+  if (k0 >= op.K) return;
   const int tx = threadIdx.x, ty = threadIdx.y;
-  for (int j = ty; j < 32; j += 8) {
+  float v[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int j = ty + 8 * q;
     int r, k;
-    if (rcontig) { r = r0 + tx; k = k0 + j; } else { k = k0 + tx; r = r0 + j; }
-    float v = (r < rows && k < K) ? X[rcontig ? (r + (long)k * ld) : (k + (long)r * ld)] : 0.f;
-    if (rcontig) t[j][tx] = v; else t[tx][j] = v;
+    if (op.rcontig) { r = r0 + tx; k = k0 + j; } else { k = k0 + tx; r = r0 + j; }
+    v[q] = (r < op.rows && k < op.K) ? op.X[op.rcontig ? (r + (long)k * op.ld) : (k + (long)r * op.ld)] : 0.f;
+  }
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int j = ty + 8 * q;
+    if (op.rcontig) t[j][tx] = v[q]; else t[tx][j] = v[q];
   }
   __syncthreads();
-  for (int j = ty; j < 32; j += 8) {
-    const int r = r0 + j, k = k0 + tx;
-    if (r < rows && k < K) {
-      const float v = t[tx][j];
-      uint32_t hi, lo;
-      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(v));
-      const float rem = v - __uint_as_float(hi);
-      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(rem));
-      float *o = out + (long)r * 3 * ldk + k;
 #pragma unroll
-      for (int q = 0; q < 3; q++) o[q * ldk] = __uint_as_float(((pat >> q) & 1) ? lo : hi);
+  for (int q = 0; q < 4; q++) {
+    const int j = ty + 8 * q, r = r0 + j, k = k0 + tx;
+    if (r < op.rows && k < op.K) {
+      const float x = t[tx][j];
+      uint32_t hi, lo;
+      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(x));
+      const float rem = x - __uint_as_float(hi);
+      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(rem));
+      float *o = op.out + (long)r * 3 * ldk + k;
+#pragma unroll
+      for (int e = 0; e < 3; e++) o[e * ldk] = __uint_as_float(((op.pat >> e) & 1) ? lo : hi);
     }
   }
 }
@@ -448,9 +478,10 @@ void sgemm_tf32x3(int ta, int tb, int M, int N, int K, float alpha, const float 
   if (ldk != K) {  // zero the K padding once per call
     ATLB_CUDA_CHECK(cudaMemsetAsync(buf, 0, abytes + bbytes + 256, st));
   }
-  dim3 blk(32, 8);
-  to_kmajor_split_kernel<<<dim3(cdiv(K, 32), cdiv(M, 32)), blk, 0, st>>>(M, K, A, lda, ta == kNoTrans, Ak, ldk, 0b010);
-  to_kmajor_split_kernel<<<dim3(cdiv(K, 32), cdiv(N, 32)), blk, 0, st>>>(N, K, B, ldb, tb != kNoTrans, Bk, ldk, 0b100);
+  const SplitOperand opa = {M, K, A, lda, ta == kNoTrans, Ak, 0b010};
+  const SplitOperand opb = {N, K, B, ldb, tb != kNoTrans, Bk, 0b100};
+  const int ya = cdiv(M, 32);
+  to_kmajor_split_kernel<<<dim3(cdiv(K, 32), ya + cdiv(N, 32)), dim3(32, 8), 0, st>>>(opa, opb, ya, ldk);
   ATLB_CUDA_CHECK(cudaGetLastError());
   tc_gemm(kKindTF32, kEpiF32, Ak, 3 * ldk, Bk, 3 * ldk, M, N, (int)(3 * ldk), ep, st);
 }

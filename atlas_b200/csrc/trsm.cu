@@ -294,9 +294,9 @@ void eff_solve(const Eff<T> &e, int r0, int n, int m, SgemmFn fn, cudaStream_t s
 // them; longer ranges are split) are first reduced to their net effect by one
 // CTA: a permutation of the rows [k1, hi) simulated in shared memory, then
 // compacted into the list of (destination, source) row moves.  The apply
-// kernel then moves only those rows, in parallel over columns (16 per CTA):
-// all sources are read into shared memory before any destination is written,
-// so the in-place permutation needs no ordering.
+// kernel then moves only those rows, in parallel over columns (up to 16 per
+// CTA): all sources are read into shared memory before any destination is
+// written, so the in-place permutation needs no ordering.
 constexpr int LSW_MAXP = 256;               // pivots per plan
 constexpr int LSW_SPAN = 24576;             // rows a plan can track in shared memory
 constexpr int LSW_COLS = 16;
@@ -371,45 +371,61 @@ laswp_plan_kernel(int k1, int k2, const int *__restrict__ ipiv, int inc, int *__
   if (tid == 0) { *nmoves = s_cnt; *ok = 1; }
 }
 
+// One CTA per `cpc` columns (at most LSW_COLS): the move list first comes
+// into shared memory, then every thread gathers its sources eight loads at a
+// time (independent loads in flight instead of one dependent round trip per
+// element), and after one barrier writes them to their destinations.  When
+// the plan could not track the rows (*ok == 0), the CTA's first threads
+// replay the swaps sequentially on its columns instead, one thread per column.
 template <typename T>
 __global__ void __launch_bounds__(256)
-laswp_apply_kernel(int ncols, T *A, long lda, const int *__restrict__ moves, const int *__restrict__ nmoves) {
+laswp_apply_kernel(int ncols, int cpc, T *A, long lda, const int *__restrict__ moves,
+                   const int *__restrict__ nmoves, const int *__restrict__ ok, int k1, int k2,
+                   const int *__restrict__ ipiv, int inc) {
   extern __shared__ __align__(16) unsigned char lsw_smem[];
-  T *buf = reinterpret_cast<T *>(lsw_smem);  // [2*LSW_MAXP][LSW_COLS]
-  const int nm = *nmoves, c0 = blockIdx.x * LSW_COLS, tid = threadIdx.x;
-  const int nc = min(LSW_COLS, ncols - c0);
+  T *buf = reinterpret_cast<T *>(lsw_smem);                        // [2*LSW_MAXP][LSW_COLS]
+  int *smv = reinterpret_cast<int *>(buf + 2 * LSW_MAXP * LSW_COLS);  // [2*LSW_MAXP][2]
+  const int c0 = blockIdx.x * cpc, tid = threadIdx.x;
+  const int nc = min(cpc, ncols - c0);
+  if (!*ok) {
+    if (tid >= nc) return;
+    T *col = A + (long)(c0 + tid) * lda;
+    if (inc > 0) {
+      for (int k = k1; k < k2; k++) {
+        const int p = ipiv[k];
+        if (p != k) { T t = col[k]; col[k] = col[p]; col[p] = t; }
+      }
+    } else {
+      for (int k = k2 - 1; k >= k1; k--) {
+        const int p = ipiv[k];
+        if (p != k) { T t = col[k]; col[k] = col[p]; col[p] = t; }
+      }
+    }
+    return;
+  }
+  const int nm = *nmoves;
+  for (int i = tid; i < 2 * nm; i += 256) smv[i] = moves[i];
+  __syncthreads();
   // moves fastest: neighbouring threads take neighbouring (sorted) rows of one column
-  for (int idx = tid; idx < nm * LSW_COLS; idx += 256) {
-    const int m = idx % nm, c = idx / nm;
-    if (c < nc) buf[idx] = A[moves[2 * m + 1] + (long)(c0 + c) * lda];
+  const int total = nm * nc;
+  for (int base = tid; base < total; base += 8 * 256) {
+    T v[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int idx = base + 256 * q;
+      if (idx < total) {
+        const int m = idx % nm, c = idx / nm;
+        v[q] = A[smv[2 * m + 1] + (long)(c0 + c) * lda];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++)
+      if (base + 256 * q < total) buf[base + 256 * q] = v[q];
   }
   __syncthreads();
-  for (int idx = tid; idx < nm * LSW_COLS; idx += 256) {
+  for (int idx = tid; idx < total; idx += 256) {
     const int m = idx % nm, c = idx / nm;
-    if (c < nc) A[moves[2 * m] + (long)(c0 + c) * lda] = buf[idx];
-  }
-}
-
-// Sequential fallback (one thread per column) for pivots spread over more
-// rows than a plan can track.
-template <typename T>
-__global__ void __launch_bounds__(256)
-laswp_seq_kernel(int ncols, T *A, long lda, int k1, int k2, const int *__restrict__ ipiv, int inc,
-                 const int *__restrict__ ok) {
-  if (*ok) return;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncols) return;
-  T *col = A + (long)c * lda;
-  if (inc > 0) {
-    for (int k = k1; k < k2; k++) {
-      const int p = ipiv[k];
-      if (p != k) { T t = col[k]; col[k] = col[p]; col[p] = t; }
-    }
-  } else {
-    for (int k = k2 - 1; k >= k1; k--) {
-      const int p = ipiv[k];
-      if (p != k) { T t = col[k]; col[k] = col[p]; col[p] = t; }
-    }
+    A[smv[2 * m] + (long)(c0 + c) * lda] = buf[idx];
   }
 }
 
@@ -601,11 +617,142 @@ trsm_llu_small_kernel(int m, int n, const T *__restrict__ L, long lda, T *B, lon
     if (r < m && c < nc) B[r + (long)(c0 + c) * ldb] = sX[r][c];
   }
 }
+
+// The same solve in FP32 (the factorization inside the mixed solvers), with
+// no global load on its dependency chain: L's lower 32 x 32 tiles (at most 36,
+// 144 KB) reach shared memory in one burst of cp.async copies, warp w inverts
+// the unit lower diagonal tile w (lane i solves row i of the inverse,
+// y L = e_i, by backward substitution), and block row ib is then
+//   X_ib = inv(L_ib,ib) (B_ib - sum_{kt < ib} L_ib,kt X_kt),
+// 32-term dot products instead of the 31-step shuffle chain.  Entries of L
+// above the diagonal (U's, in a packed LU) are never read.  NCOL = 8 CPT
+// columns per CTA, CPT per thread: 256 columns spread over 32 CTAs.
+// Tile (ib, kt) sits at t = ib (ib + 1) / 2 + kt, stored [k][i] = L[32 ib + i][32 kt + k]
+// (lane = row: conflict-free reads).
+constexpr int LLI_TILES = 36;
+
+template <int CPT>
+__global__ void __launch_bounds__(256, 1)
+trsm_llu_inv_kernel(int m, int n, const float *__restrict__ L, long lda, float *B, long ldb) {
+  constexpr int NCOL = 8 * CPT;
+  extern __shared__ __align__(16) unsigned char lli_smem[];
+  float *sLT = reinterpret_cast<float *>(lli_smem);  // the tiles, 1024 floats each
+  float *sX = sLT + LLI_TILES * 1024;                 // [NCOL][256]: B, then X
+  float *sY = sX + NCOL * LLU_MAX;                    // [NCOL][32]: one block row before inv(L_ib,ib)
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int c0 = blockIdx.x * NCOL, nc = min(NCOL, n - c0);
+  const int nblk = (m + 31) / 32;
+  for (int ib = 0; ib < nblk; ib++)
+    for (int kt = 0; kt <= ib; kt++) {
+      float *dst = sLT + (ib * (ib + 1) / 2 + kt) * 1024;
+      for (int e = tid; e < 1024; e += 256) {
+        const int k = e >> 5, i = e & 31, r = 32 * ib + i, c = 32 * kt + k;
+        const bool ok = r < m && c < m && (kt < ib || i > k);  // strictly lower, zero elsewhere
+        cp_async4(dst + e, ok ? L + r + (long)c * lda : L, ok);
+      }
+    }
+  for (int e = tid; e < NCOL * LLU_MAX; e += 256) {
+    const int c = e / LLU_MAX, r = e % LLU_MAX;
+    const bool ok = r < m && c < nc;
+    cp_async4(sX + e, ok ? B + r + (long)(c0 + c) * ldb : B, ok);
+  }
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  if (warp < nblk) {
+    float *D = sLT + (warp * (warp + 1) / 2 + warp) * 1024;
+    float y[32];
+#pragma unroll
+    for (int k = 31; k >= 0; k--) {
+      float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+      for (int j = k + 1; j < 32; j++) {
+        if ((j - k) & 1) s0 = fmaf(y[j], D[k * 32 + j], s0);
+        else s1 = fmaf(y[j], D[k * 32 + j], s1);
+      }
+      y[k] = k == lane ? 1.f : (k > lane ? 0.f : -(s0 + s1));
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 32; k++) D[k * 32 + lane] = y[k];  // inv(L)[lane][k], same layout
+  }
+  __syncthreads();
+  for (int ib = 0; ib < nblk; ib++) {
+    const int r0 = 32 * ib;
+    float acc[CPT][2];
+#pragma unroll
+    for (int e = 0; e < CPT; e++) acc[e][0] = acc[e][1] = 0.f;
+    for (int kt = 0; kt < ib; kt++) {
+      const float *T = sLT + (ib * (ib + 1) / 2 + kt) * 1024;
+#pragma unroll 4
+      for (int k = 0; k < 32; k += 4) {
+        float lv[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) lv[q] = T[(k + q) * 32 + lane];
+#pragma unroll
+        for (int e = 0; e < CPT; e++) {
+          const float4 xv = *reinterpret_cast<const float4 *>(sX + (warp + 8 * e) * LLU_MAX + 32 * kt + k);
+          acc[e][0] = fmaf(lv[0], xv.x, acc[e][0]);
+          acc[e][1] = fmaf(lv[1], xv.y, acc[e][1]);
+          acc[e][0] = fmaf(lv[2], xv.z, acc[e][0]);
+          acc[e][1] = fmaf(lv[3], xv.w, acc[e][1]);
+        }
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < CPT; e++) {
+      const int c = warp + 8 * e;
+      sY[c * 32 + lane] = sX[c * LLU_MAX + r0 + lane] - (acc[e][0] + acc[e][1]);
+    }
+    __syncthreads();
+    const float *D = sLT + (ib * (ib + 1) / 2 + ib) * 1024;
+#pragma unroll
+    for (int e = 0; e < CPT; e++) acc[e][0] = acc[e][1] = 0.f;
+#pragma unroll 4
+    for (int k = 0; k < 32; k += 4) {
+      float lv[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) lv[q] = D[(k + q) * 32 + lane];
+#pragma unroll
+      for (int e = 0; e < CPT; e++) {
+        const float4 yv = *reinterpret_cast<const float4 *>(sY + (warp + 8 * e) * 32 + k);
+        acc[e][0] = fmaf(lv[0], yv.x, acc[e][0]);
+        acc[e][1] = fmaf(lv[1], yv.y, acc[e][1]);
+        acc[e][0] = fmaf(lv[2], yv.z, acc[e][0]);
+        acc[e][1] = fmaf(lv[3], yv.w, acc[e][1]);
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < CPT; e++) sX[(warp + 8 * e) * LLU_MAX + r0 + lane] = acc[e][0] + acc[e][1];
+    __syncthreads();
+  }
+  for (int e = tid; e < NCOL * LLU_MAX; e += 256) {
+    const int c = e / LLU_MAX, r = e % LLU_MAX;
+    if (r < m && c < nc) B[r + (long)(c0 + c) * ldb] = sX[e];
+  }
+}
+
+template <int CPT>
+void trsm_llu_inv_launch(int m, int n, const float *L, long lda, float *B, long ldb, cudaStream_t st) {
+  constexpr int smem = (LLI_TILES * 1024 + 8 * CPT * (LLU_MAX + 32)) * (int)sizeof(float);
+  static bool configured = false;
+  if (!configured) {
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(trsm_llu_inv_kernel<CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    configured = true;
+  }
+  trsm_llu_inv_kernel<CPT><<<cdiv(n, 8 * CPT), 256, smem, st>>>(m, n, L, lda, B, ldb);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
 }  // namespace
 
 template <typename T>
 void trsm_llu_small_dev(int m, int n, const T *L, long lda, T *B, long ldb, cudaStream_t st) {
   if (m <= 0 || n <= 0) return;
+  if (sizeof(T) == 4) {  // FP32: L in shared memory, inverted diagonal tiles
+    if (n <= 8 * num_sms()) trsm_llu_inv_launch<1>(m, n, (const float *)L, lda, (float *)B, ldb, st);
+    else trsm_llu_inv_launch<4>(m, n, (const float *)L, lda, (float *)B, ldb, st);
+    return;
+  }
   constexpr int smem = (LLU_MAX * (LLU_COLS + 1) + 32 * 33) * (int)sizeof(T);
   static bool configured = false;
   if (!configured) {
@@ -643,7 +790,7 @@ void laswp_dev(int ncols, T *A, long lda, int k1, int k2, const int *ipiv, int i
   if (ncols <= 0 || k2 <= k1) return;
   int *ws = (int *)scratch(kSlotLaswp, sizeof(int) * (4 * LSW_MAXP + 64));
   int *moves = ws + 64, *nmoves = ws, *ok = ws + 1;
-  constexpr int smem = 2 * LSW_MAXP * LSW_COLS * (int)sizeof(T);
+  constexpr int smem = 2 * LSW_MAXP * LSW_COLS * (int)sizeof(T) + 4 * LSW_MAXP * (int)sizeof(int);
   static bool configured = false;
   if (!configured) {
     ATLB_CUDA_CHECK(cudaFuncSetAttribute(laswp_apply_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -651,53 +798,113 @@ void laswp_dev(int ncols, T *A, long lda, int k1, int k2, const int *ipiv, int i
                                          LSW_SPAN * (int)sizeof(int)));
     configured = true;
   }
+  // columns per CTA: enough CTAs to cover the GPU twice, at most LSW_COLS
+  const int cpc = std::max(1, std::min(LSW_COLS, ncols / (2 * num_sms())));
   const int nchunk = cdiv(k2 - k1, LSW_MAXP);
   for (int ci = 0; ci < nchunk; ci++) {
     const int ch = inc > 0 ? ci : nchunk - 1 - ci;
     const int a = k1 + ch * LSW_MAXP, b = std::min(k2, a + LSW_MAXP);
     laswp_plan_kernel<<<1, 1024, LSW_SPAN * sizeof(int), st>>>(a, b, ipiv, inc, moves, nmoves, ok);
-    laswp_apply_kernel<T><<<cdiv(ncols, LSW_COLS), 256, smem, st>>>(ncols, A, lda, moves, nmoves);
-    laswp_seq_kernel<T><<<cdiv(ncols, 256), 256, 0, st>>>(ncols, A, lda, a, b, ipiv, inc, ok);
+    laswp_apply_kernel<T><<<cdiv(ncols, cpc), 256, smem, st>>>(ncols, cpc, A, lda, moves, nmoves, ok, a, b,
+                                                               ipiv, inc);
   }
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
 
 namespace {
-// One thread replays the n interchanges on an index vector (the chain is
-// sequential); the vector sits in shared memory when it fits.
-__global__ void ipiv_perm_kernel(int n, const int *__restrict__ ipiv, int *__restrict__ perm, int use_smem) {
-  extern __shared__ int sp[];
-  int *pv = use_smem ? sp : perm;
-  int *ip = use_smem ? sp + n : nullptr;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    pv[i] = i;
-    if (use_smem) ip[i] = ipiv[i];
-  }
+// The net row permutation of n interchanges (perm[i] = the original row that
+// ends at position i), in two launches instead of one n-step chain:
+//  1. perm_plan_kernel, one CTA per chunk of 256 interchanges, all chunks at
+//     once: a chunk touches its own 256 positions and the distinct pivot rows
+//     below them (at most 256 more), so its net effect is a permutation of at
+//     most 512 slots; thread 0 replays the chunk's swaps on the slots and
+//     slot s leaves as the pair (destination, source) (destination -1 for an
+//     unused slot);
+//  2. perm_compose_kernel, one CTA: the chunks' pairs applied in order to the
+//     index vector (all sources read, barrier, all destinations written).
+constexpr int PP_CHUNK = 256;
+
+__global__ void __launch_bounds__(PP_CHUNK)
+perm_plan_kernel(int n, const int *__restrict__ ipiv, int *__restrict__ moves) {
+  __shared__ int sp[PP_CHUNK], bslot[PP_CHUNK];
+  __shared__ int pos[2 * PP_CHUNK], val[2 * PP_CHUNK];
+  const int tid = threadIdx.x, k1 = blockIdx.x * PP_CHUNK, nk = min(PP_CHUNK, n - k1), k2 = k1 + nk;
+  if (tid < nk) sp[tid] = ipiv[k1 + tid];
+  pos[tid] = tid < nk ? k1 + tid : -1;
+  pos[PP_CHUNK + tid] = -1;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int k = 0; k < n; k++) {
-      const int b = use_smem ? ip[k] : ipiv[k];
-      const int t = pv[k];
-      pv[k] = pv[b];
-      pv[b] = t;
+  if (tid < nk) {
+    const int p = sp[tid];
+    int s = tid;                           // an interchange outside [k1, n) is skipped
+    if (p >= k1 && p < k2) s = p - k1;
+    else if (p >= k2 && p < n) {
+      int first = tid;                     // the slot of a pivot row is its first occurrence's
+      for (int q = 0; q < tid; q++)
+        if (sp[q] == p) { first = q; break; }
+      s = PP_CHUNK + first;
+      if (first == tid) pos[s] = p;
     }
+    bslot[tid] = s;
   }
   __syncthreads();
+  val[tid] = pos[tid];
+  val[PP_CHUNK + tid] = pos[PP_CHUNK + tid];
+  __syncthreads();
+  if (tid == 0)
+    for (int k = 0; k < nk; k++) {
+      const int b = bslot[k], t = val[k];
+      val[k] = val[b];
+      val[b] = t;
+    }
+  __syncthreads();
+  int *mv = moves + (long)blockIdx.x * 4 * PP_CHUNK;
+  for (int s = tid; s < 2 * PP_CHUNK; s += PP_CHUNK) {
+    mv[2 * s] = pos[s];
+    mv[2 * s + 1] = val[s];
+  }
+}
+
+__global__ void __launch_bounds__(1024)
+perm_compose_kernel(int n, int nchunk, const int *__restrict__ moves, int *__restrict__ perm, int use_smem) {
+  extern __shared__ int spv[];
+  int *pv = use_smem ? spv : perm;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < n; i += blockDim.x) pv[i] = i;
+  int d = -1, s = 0;
+  if (tid < 2 * PP_CHUNK) { d = moves[2 * tid]; s = moves[2 * tid + 1]; }
+  __syncthreads();
+  for (int c = 0; c < nchunk; c++) {
+    int dn = -1, sn = 0;  // the next chunk's pair, fetched while this one is applied
+    if (tid < 2 * PP_CHUNK && c + 1 < nchunk) {
+      const int *mv = moves + (long)(c + 1) * 4 * PP_CHUNK;
+      dn = mv[2 * tid];
+      sn = mv[2 * tid + 1];
+    }
+    const int v = d >= 0 ? pv[s] : 0;
+    __syncthreads();
+    if (d >= 0) pv[d] = v;
+    __syncthreads();
+    d = dn;
+    s = sn;
+  }
   if (use_smem)
-    for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = pv[i];
+    for (int i = tid; i < n; i += blockDim.x) perm[i] = pv[i];
 }
 }  // namespace
 
 void ipiv_to_perm_dev(int n, const int *ipiv, int *perm, cudaStream_t st) {
   if (n <= 0) return;
-  const size_t bytes = sizeof(int) * 2 * (size_t)n;
+  const int nchunk = cdiv(n, PP_CHUNK);
+  int *moves = (int *)scratch(kSlotPermPlan, sizeof(int) * 4 * PP_CHUNK * (size_t)nchunk);
+  const size_t bytes = sizeof(int) * (size_t)n;
   const int use_smem = bytes <= 200 * 1024;
   static bool configured = false;
   if (!configured) {
-    ATLB_CUDA_CHECK(cudaFuncSetAttribute(ipiv_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(perm_compose_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     configured = true;
   }
-  ipiv_perm_kernel<<<1, 1024, use_smem ? bytes : 0, st>>>(n, ipiv, perm, use_smem);
+  perm_plan_kernel<<<nchunk, PP_CHUNK, 0, st>>>(n, ipiv, moves);
+  perm_compose_kernel<<<1, 1024, use_smem ? bytes : 0, st>>>(n, nchunk, moves, perm, use_smem);
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
 

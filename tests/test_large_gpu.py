@@ -6,7 +6,10 @@
   tickets keep every wait on a block that is already running);
 * getrf and the mixed solver at n = 9000: more rows than one cluster of the
   fused leaf panel holds (16 x 512), so the first blocks go through the
-  recursive panel path and the later ones through the fused kernel.
+  recursive panel path and the later ones through the fused kernel;
+* getrf of a 30000 x 512 matrix: pivot rows farther below the block than a
+  row-interchange plan tracks (24576 rows), so the interchanges outside the
+  blocks take the sequential per-column path.
 
 References are computed on the GPU with torch (FP64) and the checks are the
 tester-style normwise residuals (bin/lutst.c, bin/slvtst.c: pass <= 100)."""
@@ -92,3 +95,30 @@ def test_mixed_dgesv_rows_beyond_one_cluster(gpu):
     r = b - a @ x
     berr = (r.abs().max() / (a.abs().sum(1).max() * x.abs().max() + b.abs().max())).item()
     assert berr <= n * 2.0 ** -53, berr
+
+
+def test_getrf_tall_pivots_beyond_plan_span(gpu):
+    import torch
+    m, n = 30000, 512
+    g = torch.Generator(device="cuda")
+    g.manual_seed(14)
+    a = torch.rand(m, n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    da = _colmajor(a)
+    ipiv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    assert AB.atlb_dgetrf_dev(m, n, da, m, ipiv, info) == 0
+    AB.atlb_sync()
+    assert int(info.item()) == 0
+    piv = ipiv.cpu().numpy()
+    assert (piv >= np.arange(n)).all() and piv.max() >= 256 + 24576   # some pivots lie beyond a plan's span
+    f = da.t()                                   # row-major view (m x n) of the packed factors
+    L = torch.tril(f, -1) + torch.eye(m, n, dtype=torch.float64, device="cuda")
+    U = torch.triu(f[:n])
+    perm = np.arange(m)
+    for k in range(n):
+        p = piv[k]
+        if p != k:
+            perm[k], perm[p] = perm[p], perm[k]
+    pa = a[torch.as_tensor(perm, device="cuda")]
+    resid = ((pa - L @ U).abs().sum(0).max() / (a.abs().sum(0).max() * m * 2.0 ** -52)).item()
+    assert resid <= 100.0, resid
