@@ -71,6 +71,8 @@ void trinv_dev(int n, const T *Tp, long tr, long tc, int lower, int unit, T *W, 
 template <typename T>
 void trsv_dev(int uplo, int trans, int diag, int n, int nrhs, const T *A, long lda, T *B, long ldb,
               cudaStream_t st);
+// W for trsv_w_dev: the inverted 128 x 128 diagonal blocks (W holds trsv_w_elems(n) elements)
+size_t trsv_w_elems(int n);
 template <typename T>
 void trsv_inverse_dev(int uplo, int trans, int diag, int n, const T *A, long lda, T *W, cudaStream_t st);
 template <typename T>

@@ -358,8 +358,8 @@ int atlb_dsgesv_ex(int N, int NRHS, double *A, int lda, int *ipiv, double *B, in
   // blocks and the net row permutation, computed once after the factorization
   const bool few = NRHS <= 8;
   const int nw = few ? (int)lds : 0;
-  float *WL = few ? (float *)scratch(kSlotMixedWL, sizeof(float) * (size_t)cdiv(nw, 64) * 64 * 64) : nullptr;
-  float *WU = few ? (float *)scratch(kSlotMixedWU, sizeof(float) * (size_t)cdiv(nw, 64) * 64 * 64) : nullptr;
+  float *WL = few ? (float *)scratch(kSlotMixedWL, sizeof(float) * trsv_w_elems(nw)) : nullptr;
+  float *WU = few ? (float *)scratch(kSlotMixedWU, sizeof(float) * trsv_w_elems(nw)) : nullptr;
   int *perm = (few && !pivoting) ? (int *)scratch(kSlotMixedPerm, sizeof(int) * (size_t)N) : nullptr;
   auto factor = [&]() {
     if (pivoting) {
@@ -455,8 +455,8 @@ int atlb_dsposv(int Uplo, int N, int NRHS, double *A, int lda, double *B, int ld
   float *S = (float *)scratch(kSlotMixedA, sizeof(float) * (size_t)N * N);
   float *Rs = (float *)scratch(kSlotMixedX, sizeof(float) * (size_t)N * NRHS);
   const bool few = NRHS <= 8;
-  float *W1 = few ? (float *)scratch(kSlotMixedWL, sizeof(float) * (size_t)cdiv(N, 64) * 64 * 64) : nullptr;
-  float *W2 = few ? (float *)scratch(kSlotMixedWU, sizeof(float) * (size_t)cdiv(N, 64) * 64 * 64) : nullptr;
+  float *W1 = few ? (float *)scratch(kSlotMixedWL, sizeof(float) * trsv_w_elems(N)) : nullptr;
+  float *W2 = few ? (float *)scratch(kSlotMixedWU, sizeof(float) * trsv_w_elems(N)) : nullptr;
   // A = U^T U: solve with U^T then U; A = L L^T: with L then L^T
   const int t1 = Uplo == kUpper ? kTrans : kNoTrans, t2 = Uplo == kUpper ? kNoTrans : kTrans;
   auto factor = [&]() {

@@ -9,8 +9,9 @@
 // ago are streamed in bulk: one warp looks up to 32 "done" flags at once
 // and the CTA then runs through every block found done without waiting
 // again; only the block just before it is awaited, with its matrix values
-// already in registers.  The two sub-blocks are then solved in turn with
-// the inverted 64x64 diagonal blocks (trinv_kernel's W) and the block is
+// already in registers.  The block is then solved by one product with the
+// inverse of its 128 x 128 diagonal block (computed once per factor by
+// trsv_inverse_dev, loaded into shared memory before any wait) and
 // published.  Every wait on a flag is bounded: after ~1 s the kernel records
 // an error in *err and stops waiting (the result is then wrong but the GPU
 // is released).  The launcher clears the ticket counter and the flags before
@@ -43,11 +44,10 @@ __global__ void __launch_bounds__(TT, 1)
 trsv_kernel(int n, int nrhs, const T *__restrict__ Tp, long tr, long tc, int lower,
             const T *__restrict__ W, T *X, long ldx, int *counter, int *flags, int epoch, int *err) {
   extern __shared__ __align__(16) unsigned char trsv_smem[];
-  T(*sW)[BS][BS + 1] = reinterpret_cast<T(*)[BS][BS + 1]>(trsv_smem);  // the two inverted diagonal blocks
-  T(*sxd)[CB][NR] = reinterpret_cast<T(*)[CB][NR]>(sW + 2);             // x of a solved block, double-buffered
-  T(*sb)[NR] = reinterpret_cast<T(*)[NR]>(sxd + 2);                     // this block's b, then its x
-  T(*spart)[BS][NR] = reinterpret_cast<T(*)[BS][NR]>(sb + CB);          // [4]: quarter sums
-  T(*sacc)[CB][NR] = reinterpret_cast<T(*)[CB][NR]>(spart + 4);         // [2]: the two halves' sums
+  T(*sW)[CB + 1] = reinterpret_cast<T(*)[CB + 1]>(trsv_smem);   // [CB]: the inverted diagonal block
+  T(*sxd)[CB][NR] = reinterpret_cast<T(*)[CB][NR]>(sW + CB);    // x of a solved block, double-buffered
+  T(*sb)[NR] = reinterpret_cast<T(*)[NR]>(sxd + 2);             // this block's b
+  T(*sacc)[CB][NR] = reinterpret_cast<T(*)[CB][NR]>(sb + CB);   // [2]: the two halves' sums
   __shared__ int s_bi, s_ready;
   const int tid = threadIdx.x, lane = tid & 31, nb = (n + CB - 1) / CB;
   if (tid == 0) {
@@ -56,11 +56,16 @@ trsv_kernel(int n, int nrhs, const T *__restrict__ Tp, long tr, long tc, int low
   }
   __syncthreads();
   const int bi = s_bi, r0 = bi * CB, rows = min(CB, n - r0);
-  const int nsub = (rows + BS - 1) / BS;  // 1 or 2 sub-blocks
   // everything that does not depend on other blocks is fetched first
-  for (int sbk = 0; sbk < nsub; sbk++) {
-    const T *Wb = W + (long)(r0 / BS + sbk) * BS * BS;
-    for (int idx = tid; idx < BS * BS; idx += TT) sW[sbk][idx % BS][idx / BS] = Wb[idx];
+  {
+    const T *Wb = W + (long)bi * CB * CB;  // column-major 128 x 128
+    for (int base = tid; base < CB * CB; base += 8 * TT) {  // eight loads in flight per thread
+      T v[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) v[q] = Wb[base + q * TT];
+#pragma unroll
+      for (int q = 0; q < 8; q++) sW[(base + q * TT) % CB][(base + q * TT) / CB] = v[q];
+    }
   }
   for (int idx = tid; idx < CB * NR; idx += TT) {
     const int rr = idx % CB, q = idx / CB;
@@ -105,18 +110,20 @@ trsv_kernel(int n, int nrhs, const T *__restrict__ Tp, long tr, long tc, int low
     const int nr = s_ready;
     for (int e = 0; e < nr; e++, d++) {
       const int bj = lower ? d : nb - 1 - d;
+      const int c0 = bj * CB + half * BS, cols = min(BS, n - c0);
+      // all 64 matrix loads in flight at once, issued before the barrier: a
+      // CTA far down the triangle streams many blocks, and this stream (not
+      // the chain of solves) bounds it when fewer loads are in flight
+      T tv[BS];
+#pragma unroll
+      for (int k = 0; k < BS; k++) tv[k] = (row < rows && k < cols) ? trow[(long)(c0 + k) * tc] : T(0);
       load_x(bj, buf);
       __syncthreads();
-      const int c0 = bj * CB + half * BS, cols = min(BS, n - c0);
-      if (row < rows) {
-        const T(*xs)[NR] = sxd[buf] + half * BS;
-#pragma unroll 16
-        for (int k = 0; k < BS; k++) {
-          const T tv = k < cols ? trow[(long)(c0 + k) * tc] : T(0);
+      const T(*xs)[NR] = sxd[buf] + half * BS;
 #pragma unroll
-          for (int q = 0; q < NR; q++) acc[q] = fma(tv, xs[k][q], acc[q]);
-        }
-      }
+      for (int k = 0; k < BS; k++)
+#pragma unroll
+        for (int q = 0; q < NR; q++) acc[q] = fma(tv[k], xs[k][q], acc[q]);
       buf ^= 1;
     }
     __syncthreads();  // s_ready is read by every thread before it is rewritten
@@ -145,54 +152,24 @@ trsv_kernel(int n, int nrhs, const T *__restrict__ Tp, long tr, long tc, int low
     sb[rr][q] -= sacc[0][rr][q] + sacc[1][rr][q];
   }
   __syncthreads();
-  // 3. the two sub-blocks in turn (lower: top first): x_s = W_s b_s, then
-  // the other sub-block's b -= T(other, s) x_s
-  const int i64 = tid % BS, part = tid / BS;  // row of a sub-block, quarter of its columns
-  for (int step = 0; step < nsub; step++) {
-    const int sbk = lower ? step : nsub - 1 - step;
+  // 3. x = inv(T_bb) b: thread (row, half) sums over half of the columns
+  {
+    T v[NR];
 #pragma unroll
-    for (int q = 0; q < NR; q++) {
-      T v = T(0);
+    for (int q = 0; q < NR; q++) v[q] = T(0);
+#pragma unroll 16
+    for (int c = half * BS; c < half * BS + BS; c++) {
+      const T w = sW[row][c];
 #pragma unroll
-      for (int c = 16 * part; c < 16 * part + 16; c++) v = fma(sW[sbk][i64][c], sb[sbk * BS + c][q], v);
-      spart[part][i64][q] = v;
+      for (int q = 0; q < NR; q++) v[q] = fma(w, sb[c][q], v[q]);
     }
-    __syncthreads();
-    for (int idx = tid; idx < BS * NR; idx += TT) {
-      const int rr = idx % BS, q = idx / BS;
-      sb[sbk * BS + rr][q] = (spart[0][rr][q] + spart[1][rr][q]) + (spart[2][rr][q] + spart[3][rr][q]);
-    }
-    __syncthreads();
-    if (step + 1 < nsub) {
-      const int oth = 1 - sbk;
-      // rows of sub-block oth, columns of sub-block sbk
-      const int gr = r0 + oth * BS + i64;
-      T v[NR];
 #pragma unroll
-      for (int q = 0; q < NR; q++) v[q] = T(0);
-      if (oth * BS + i64 < rows) {
-        const T *tr2 = Tp + (long)gr * tr;
-#pragma unroll
-        for (int c = 16 * part; c < 16 * part + 16; c++) {
-          const int gc = r0 + sbk * BS + c;  // a column of sub-block sbk (past n when it is the partial last one)
-          const T tv2 = gc < n ? tr2[(long)gc * tc] : T(0);
-#pragma unroll
-          for (int q = 0; q < NR; q++) v[q] = fma(tv2, sb[sbk * BS + c][q], v[q]);
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < NR; q++) spart[part][i64][q] = v[q];
-      __syncthreads();
-      for (int idx = tid; idx < BS * NR; idx += TT) {
-        const int rr = idx % BS, q = idx / BS;
-        sb[oth * BS + rr][q] -= (spart[0][rr][q] + spart[1][rr][q]) + (spart[2][rr][q] + spart[3][rr][q]);
-      }
-      __syncthreads();
-    }
+    for (int q = 0; q < NR; q++) sacc[half][row][q] = v[q];
   }
+  __syncthreads();
   for (int idx = tid; idx < CB * NR; idx += TT) {
     const int rr = idx % CB, q = idx / CB;
-    if (rr < rows && q < nrhs) X[r0 + rr + (long)q * ldx] = sb[rr][q];
+    if (rr < rows && q < nrhs) X[r0 + rr + (long)q * ldx] = sacc[0][rr][q] + sacc[1][rr][q];
   }
   __syncthreads();
   if (tid == 0) {  // the barrier orders every thread's x stores before this release
@@ -201,16 +178,100 @@ trsv_kernel(int n, int nrhs, const T *__restrict__ Tp, long tr, long tc, int low
   }
 }
 
+// The 128 x 128 diagonal blocks' inverses from the 64 x 64 ones (W64, as
+// trinv_kernel leaves them): lower [W0 0; -W1 T10 W0  W1], upper
+// [W0  -W0 T01 W1; 0 W1], with W1 = I when the last block has one sub-block.
+// One CTA per block, the 128 x 128 block in shared memory: the off-diagonal
+// quadrant first holds T's, then Y = T10 W0 (or T01 W1), then -W1 Y (or
+// -W0 Y).  Written column-major, 128 x 128 per block.
+template <typename T>
+__global__ void __launch_bounds__(256)
+trinv128_kernel(int n, const T *__restrict__ Tp, long tr, long tc, int lower, const T *__restrict__ W64,
+                T *__restrict__ W128) {
+  extern __shared__ __align__(16) unsigned char t128_smem[];
+  T(*s)[CB + 1] = reinterpret_cast<T(*)[CB + 1]>(t128_smem);
+  const int b = blockIdx.x, r0 = b * CB, tid = threadIdx.x;
+  const int nsub = min(2, (n - r0 + BS - 1) / BS);
+  for (int base = tid; base < CB * CB; base += 8 * 256) {  // eight loads in flight per thread
+    T v[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int idx = base + 256 * q;
+      const int i = idx % CB, k = idx / CB, qi = i / BS, qk = k / BS, ii = i % BS, kk = k % BS;
+      v[q] = T(0);
+      if (qi == qk) {
+        if (qi < nsub) v[q] = W64[(long)(2 * b + qi) * BS * BS + ii + kk * BS];
+        else v[q] = ii == kk ? T(1) : T(0);
+      } else if (lower ? qi == 1 : qi == 0) {  // the triangle's off-diagonal quadrant
+        const int gi = r0 + i, gk = r0 + k;
+        if (gi < n && gk < n) v[q] = Tp[gi * tr + gk * tc];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) s[(base + 256 * q) % CB][(base + 256 * q) / CB] = v[q];
+  }
+  __syncthreads();
+  // off-diagonal quadrant at (oi, ok); the products read the diagonal
+  // quadrants at (ok, ok) (first) and (oi, oi) (second)
+  const int oi = lower ? BS : 0, ok = lower ? 0 : BS;
+  T y[BS * BS / 256];
+#pragma unroll
+  for (int e = 0; e < BS * BS / 256; e++) {
+    const int idx = tid + 256 * e, i = idx % BS, j = idx / BS;
+    T acc = T(0);
+#pragma unroll 16
+    for (int k = 0; k < BS; k++) acc = fma(s[oi + i][ok + k], s[ok + k][ok + j], acc);
+    y[e] = acc;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int e = 0; e < BS * BS / 256; e++) {
+    const int idx = tid + 256 * e;
+    s[oi + idx % BS][ok + idx / BS] = y[e];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int e = 0; e < BS * BS / 256; e++) {
+    const int idx = tid + 256 * e, i = idx % BS, j = idx / BS;
+    T acc = T(0);
+#pragma unroll 16
+    for (int k = 0; k < BS; k++) acc = fma(s[oi + i][oi + k], s[oi + k][ok + j], acc);
+    y[e] = -acc;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int e = 0; e < BS * BS / 256; e++) {
+    const int idx = tid + 256 * e;
+    s[oi + idx % BS][ok + idx / BS] = y[e];
+  }
+  __syncthreads();
+  T *Wb = W128 + (long)b * CB * CB;
+  for (int idx = tid; idx < CB * CB; idx += 256) Wb[idx] = s[idx % CB][idx / CB];
+}
+
 }  // namespace
 
-// Inverted 64x64 diagonal blocks of op(A)'s triangle, as trsv_w_dev takes them.
+size_t trsv_w_elems(int n) { return (size_t)cdiv(n, CB) * CB * CB + (size_t)cdiv(n, BS) * BS * BS; }
+
+// Inverted 128 x 128 diagonal blocks of op(A)'s triangle, as trsv_w_dev takes
+// them (W holds trsv_w_elems(n) elements: the 128 x 128 inverses, then the
+// 64 x 64 ones they are assembled from).
 template <typename T>
 void trsv_inverse_dev(int uplo, int trans, int diag, int n, const T *A, long lda, T *W, cudaStream_t st) {
   if (n <= 0) return;
   const bool tr = trans != kNoTrans;
   const long tstr = tr ? lda : 1, tcol = tr ? 1 : lda;
   const int lower = (uplo == kLower) != tr;
-  trinv_dev<T>(n, A, tstr, tcol, lower, diag == kUnit, W, st);
+  T *W64 = W + (size_t)cdiv(n, CB) * CB * CB;
+  trinv_dev<T>(n, A, tstr, tcol, lower, diag == kUnit, W64, st);
+  constexpr int smem = CB * (CB + 1) * (int)sizeof(T);
+  static bool configured = false;
+  if (!configured) {
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(trinv128_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    configured = true;
+  }
+  trinv128_kernel<T><<<cdiv(n, CB), 256, smem, st>>>(n, A, tstr, tcol, lower, W64, W);
+  ATLB_CUDA_CHECK(cudaGetLastError());
 }
 template void trsv_inverse_dev<double>(int, int, int, int, const double *, long, double *, cudaStream_t);
 template void trsv_inverse_dev<float>(int, int, int, int, const float *, long, float *, cudaStream_t);
@@ -220,7 +281,7 @@ template <typename T>
 void trsv_dev(int uplo, int trans, int diag, int n, int nrhs, const T *A, long lda, T *B, long ldb,
               cudaStream_t st) {
   if (n <= 0 || nrhs <= 0) return;
-  T *W = (T *)scratch(kSlotTrsmW, sizeof(T) * (size_t)cdiv(n, BS) * BS * BS);
+  T *W = (T *)scratch(kSlotTrsmW, sizeof(T) * trsv_w_elems(n));
   trsv_inverse_dev<T>(uplo, trans, diag, n, A, lda, W, st);
   trsv_w_dev<T>(uplo, trans, n, nrhs, A, lda, W, B, ldb, st);
 }
@@ -242,8 +303,8 @@ void trsv_w_dev(int uplo, int trans, int n, int nrhs, const T *A, long lda, cons
   const int epoch = 1;
   int *counter = ctl, *err = ctl + 1, *flags = ctl + 64;
   ATLB_CUDA_CHECK(cudaMemsetAsync(ctl, 0, sizeof(int) * (nb + 64), st));  // counter, flags
-  // sW, sxd, sb, spart, sacc (trsv_kernel's layout), for the largest NR
-  constexpr int smem = (2 * BS * (BS + 1) + (2 * CB + CB + 4 * BS + 2 * CB) * 8) * (int)sizeof(T);
+  // sW, sxd, sb, sacc (trsv_kernel's layout), for the largest NR
+  constexpr int smem = (CB * (CB + 1) + (2 * CB + CB + 2 * CB) * 8) * (int)sizeof(T);
   static bool configured = false;
   if (!configured) {
     ATLB_CUDA_CHECK(cudaFuncSetAttribute(trsv_kernel<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
