@@ -77,6 +77,38 @@ abs_rowsum_partial_kernel(int N, const double *__restrict__ A, long lda, double 
   part[(long)blockIdx.y * N + i] = s;
 }
 
+// S = (float) A and abs_rowsum_partial_kernel's partials in one pass over A
+// (the mixed solvers need both before factoring): per 256-column chunk, thread
+// i converts its row's elements and sums their magnitudes in column order,
+// the order of abs_rowsum_partial_kernel, eight loads in flight.
+__global__ void __launch_bounds__(GV_ROWS)
+d2s_rowsum_kernel(int N, const double *__restrict__ A, long lda, float *__restrict__ S, long lds,
+                  double *__restrict__ part) {
+  const int i = blockIdx.x * GV_ROWS + threadIdx.x, c0 = blockIdx.y * GV_COLS;
+  if (i >= N) return;
+  const int c1 = min(N, c0 + GV_COLS);
+  const double *a = A + i + (long)c0 * lda;
+  float *o = S + i + (long)c0 * lds;
+  double s = 0.0;
+  int c = c0;
+  for (; c + 8 <= c1; c += 8, a += 8 * lda, o += 8 * lds) {
+    double v[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) v[q] = a[(long)q * lda];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      o[(long)q * lds] = (float)v[q];
+      s += fabs(v[q]);
+    }
+  }
+  for (; c < c1; c++, a += lda, o += lds) {
+    const double v = *a;
+    *o = (float)v;
+    s += fabs(v);
+  }
+  part[(long)blockIdx.y * N + i] = s;
+}
+
 // residual partials: part[(chunk * nrhs + r) * N + i] = sum_{c in chunk} A(i,c) X(c,r)
 template <int NR>
 __global__ void __launch_bounds__(GV_ROWS)
@@ -238,6 +270,16 @@ void dresid_dev(int N, int nrhs, const double *A, long lda, const double *X, lon
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
 
+// S = (float) A (N x N) and ||A||_inf into *out (as dnorm_inf_dev), one pass over A
+void d2s_norm_dev(int N, const double *A, long lda, float *S, long lds, double *part, unsigned long long *out,
+                  cudaStream_t st) {
+  const int nch = cdiv(N, GV_COLS);
+  ATLB_CUDA_CHECK(cudaMemsetAsync(out, 0, sizeof(unsigned long long), st));
+  d2s_rowsum_kernel<<<dim3(cdiv(N, GV_ROWS), nch), GV_ROWS, 0, st>>>(N, A, lda, S, lds, part);
+  rowsum_finish_kernel<<<std::min(cdiv(N, 256), 148), 256, 0, st>>>(N, nch, part, out);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
+
 void d2s_dev(int M, int N, const double *A, long lda, float *S, long lds, cudaStream_t st) {
   d2s_kernel<<<grid_for((long)M * N), 256, 0, st>>>(M, N, A, lda, S, lds);
   ATLB_CUDA_CHECK(cudaGetLastError());
@@ -256,8 +298,11 @@ void add_s2d_dev(int M, int N, const float *S, long lds, double *X, long ldx, cu
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
 
-// Refinement driver shared by the solvers.  `factor()` factors the low
-// precision copy and returns its info; `correct(R, ldr, X, ldx)` adds an
+// Refinement driver shared by the solvers.  `factor(part, nrm)` factors the
+// low precision copy and returns its info; it also leaves ||A||_inf (bits of
+// the double) in *nrm, with part (N * ceil(N/256) doubles) as workspace, so
+// that the copy and the norm can share one pass over A (d2s_norm_dev);
+// `correct(R, ldr, X, ldx)` adds an
 // approximate solution of A D = R to X (R, X FP64 device); `fallback()` runs
 // the FP64 solver.  X is overwritten with the solution.
 template <class Factor, class Correct, class Fallback>
@@ -270,8 +315,7 @@ int refine(int N, int nrhs, const double *A, long lda, const double *B, long ldb
   unsigned long long *red = (unsigned long long *)scratch(kSlotWork2, sizeof(unsigned long long) * (3 * nrhs + 8));
   unsigned long long *hred = (unsigned long long *)pinned(kSlotWork2, sizeof(unsigned long long) * (3 * nrhs + 8));
 
-  dnorm_inf_dev(N, A, lda, part, red + 3 * nrhs, st);
-  int finfo = factor();
+  int finfo = factor(part, red + 3 * nrhs);  // also leaves ||A||_inf (bits) in red[3 nrhs]
   double anrm = 0.0;
   {
     ATLB_CUDA_CHECK(cudaMemcpyAsync(hred, red + 3 * nrhs, 8, cudaMemcpyDeviceToHost, st));
@@ -361,13 +405,14 @@ int atlb_dsgesv_ex(int N, int NRHS, double *A, int lda, int *ipiv, double *B, in
   float *WL = few ? (float *)scratch(kSlotMixedWL, sizeof(float) * trsv_w_elems(nw)) : nullptr;
   float *WU = few ? (float *)scratch(kSlotMixedWU, sizeof(float) * trsv_w_elems(nw)) : nullptr;
   int *perm = (few && !pivoting) ? (int *)scratch(kSlotMixedPerm, sizeof(int) * (size_t)N) : nullptr;
-  auto factor = [&]() {
+  auto factor = [&](double *part, unsigned long long *nrm) {
     if (pivoting) {
+      dnorm_inf_dev(N, dA.d, dA.ld, part, nrm, st);
       rbt_init_dev(n4, rd, st);
       rbt_matrix_dev(N, dA.d, dA.ld, rd, S, st);
       getrf_nopiv_dev<float>(n4, S, lds, dinfo, st, g);
     } else {
-      d2s_dev(N, N, dA.d, dA.ld, S, lds, st);
+      d2s_norm_dev(N, dA.d, dA.ld, S, lds, part, nrm, st);
       getrf_dev<float>(N, N, S, lds, dip, dinfo, st, g);
       if (few) ipiv_to_perm_dev(N, dip, perm, st);
     }
@@ -459,8 +504,8 @@ int atlb_dsposv(int Uplo, int N, int NRHS, double *A, int lda, double *B, int ld
   float *W2 = few ? (float *)scratch(kSlotMixedWU, sizeof(float) * trsv_w_elems(N)) : nullptr;
   // A = U^T U: solve with U^T then U; A = L L^T: with L then L^T
   const int t1 = Uplo == kUpper ? kTrans : kNoTrans, t2 = Uplo == kUpper ? kNoTrans : kTrans;
-  auto factor = [&]() {
-    d2s_dev(N, N, Af, N, S, N, st);
+  auto factor = [&](double *part, unsigned long long *nrm) {
+    d2s_norm_dev(N, Af, N, S, N, part, nrm, st);
     potrf_dev<float>(Uplo, N, S, N, dinfo, st, g);
     if (few) {
       trsv_inverse_dev<float>(Uplo, t1, kNonUnit, N, S, N, W1, st);

@@ -298,17 +298,132 @@ void eff_solve(const Eff<T> &e, int r0, int n, int m, SgemmFn fn, cudaStream_t s
 // CTA): all sources are read into shared memory before any destination is
 // written, so the in-place permutation needs no ordering.
 constexpr int LSW_MAXP = 256;               // pivots per plan
-constexpr int LSW_SPAN = 24576;             // rows a plan can track in shared memory
+constexpr int LSW_SPAN = 24576;             // rows the sequential plan can track in shared memory
 constexpr int LSW_COLS = 16;
+
+// The plan without a sequential replay, for chunks whose pivots all lie at or
+// below their own row (ipiv[k] >= k, as getrf's are); returns false (every
+// thread) when the chunk has another pivot, for the replay below.
+// With the swaps applied in order k1, k1+1, .., position k's content is final
+// after swap k, and a position p is touched again only by swaps j with
+// ipiv[j] = p.  Let arr(k) be the row whose content stands at position k just
+// before swap k: arr(k) = arr(j) for the last j < k with ipiv[j] = k, and the
+// row k itself when there is none.  Then position k ends with arr(k) when
+// ipiv[k] = k, else with arr(j) for the last j < k with ipiv[j] = ipiv[k]
+// (or row ipiv[k] itself when there is none); a pivot row p >= k2 ends with
+// arr(j) for the last j with ipiv[j] = p.  The (pivot row, step) pairs are
+// sorted (bitonic, 256 keys) so that "the last j before" is the neighbour in
+// sorted order, and arr() follows its chain of earlier steps by pointer
+// jumping (8 rounds cover 256 steps).  Applied in the reverse order (inc < 0)
+// the swaps give the inverse permutation: each (destination, source) pair is
+// reversed.
+__device__ bool laswp_plan_parallel(int k1, int k2, const int *__restrict__ ipiv, int inc, int *__restrict__ moves,
+                                    int *__restrict__ nmoves, int *__restrict__ ok, int *s_back) {
+  __shared__ unsigned long long skey[LSW_MAXP];
+  __shared__ int sparent[LSW_MAXP], sprev[LSW_MAXP], sptr[2][LSW_MAXP], sdisp[LSW_MAXP], swsum[LSW_MAXP / 32];
+  const int tid = threadIdx.x, nk = k2 - k1, lane = tid & 31, wid = tid >> 5;
+  int myp = 0;
+  if (tid < LSW_MAXP) {
+    if (tid < nk) {
+      myp = ipiv[k1 + tid];
+      if (myp < k1 + tid) *s_back = 1;
+      skey[tid] = ((unsigned long long)(unsigned)myp << 16) | (unsigned)tid;
+    } else {
+      skey[tid] = ~0ull;
+    }
+    sparent[tid] = -1;
+    sprev[tid] = -1;
+  }
+  __syncthreads();
+  if (*s_back) return false;
+  for (int size = 2; size <= LSW_MAXP; size <<= 1)
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      if (tid < LSW_MAXP) {
+        const int partner = tid ^ stride;
+        if (partner > tid) {
+          const bool asc = (tid & size) == 0;
+          const unsigned long long a = skey[tid], b = skey[partner];
+          if ((a > b) == asc) { skey[tid] = b; skey[partner] = a; }
+        }
+      }
+      __syncthreads();
+    }
+  if (tid < nk) {  // sorted position tid
+    const unsigned long long key = skey[tid];
+    const int p = (int)(key >> 16), j = (int)(key & 0xffffu), pl = p - k1;
+    const bool next_same = tid + 1 < nk && (int)(skey[tid + 1] >> 16) == p;
+    if (tid > 0 && (int)(skey[tid - 1] >> 16) == p) sprev[j] = (int)(skey[tid - 1] & 0xffffu);
+    // the last step before pl that brought something to position pl
+    if (p < k2 && j < pl && (!next_same || (int)(skey[tid + 1] & 0xffffu) == pl)) sparent[pl] = j;
+    sdisp[tid] = p >= k2 && !next_same;  // the last swap with pivot row p, below the chunk
+  } else if (tid < LSW_MAXP) {
+    sdisp[tid] = 0;
+  }
+  __syncthreads();
+  if (tid < nk) sptr[0][tid] = sparent[tid] >= 0 ? sparent[tid] : tid;
+  __syncthreads();
+  int cur = 0;
+#pragma unroll 1
+  for (int r = 0; r < 8; r++) {
+    if (tid < nk) sptr[cur ^ 1][tid] = sptr[cur][sptr[cur][tid]];
+    __syncthreads();
+    cur ^= 1;
+  }
+  // position k1 + tid ends with row fin; the displaced row of sorted position tid
+  int fin = 0, dsrc = 0, ddst = 0;
+  bool fa = false, fb = false;
+  if (tid < nk) {
+    const int sv = myp == k1 + tid ? sptr[cur][tid] : sprev[tid];
+    fin = sv >= 0 ? k1 + sptr[cur][sv] : myp;
+    fa = fin != k1 + tid;
+    fb = sdisp[tid] != 0;
+    if (fb) {
+      const unsigned long long key = skey[tid];
+      ddst = (int)(key >> 16);
+      dsrc = k1 + sptr[cur][(int)(key & 0xffffu)];
+    }
+  }
+  // destinations in order: the chunk's rows, then the rows below it (block-wide prefix count)
+  const int v = (fa ? 1 : 0) | (fb ? 1 << 16 : 0);
+  int isc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int u = __shfl_up_sync(0xffffffffu, isc, o);
+    if (lane >= o) isc += u;
+  }
+  if (lane == 31 && wid < LSW_MAXP / 32) swsum[wid] = isc;
+  __syncthreads();
+  if (tid < LSW_MAXP) {
+    int off = 0, tot = 0;
+    for (int w = 0; w < LSW_MAXP / 32; w++) {
+      if (w < wid) off += swsum[w];
+      tot += swsum[w];
+    }
+    const int ex = off + isc - v, tota = tot & 0xffff;
+    if (fa) {
+      const int slot = ex & 0xffff;
+      moves[2 * slot] = inc > 0 ? k1 + tid : fin;
+      moves[2 * slot + 1] = inc > 0 ? fin : k1 + tid;
+    }
+    if (fb) {
+      const int slot = tota + (ex >> 16);
+      moves[2 * slot] = inc > 0 ? ddst : dsrc;
+      moves[2 * slot + 1] = inc > 0 ? dsrc : ddst;
+    }
+    if (tid == 0) { *nmoves = tota + (tot >> 16); *ok = 1; }
+  }
+  return true;
+}
 
 __global__ void __launch_bounds__(1024)
 laswp_plan_kernel(int k1, int k2, const int *__restrict__ ipiv, int inc, int *__restrict__ moves,
                   int *__restrict__ nmoves, int *__restrict__ ok) {
   extern __shared__ int perm[];  // LSW_SPAN entries
-  __shared__ int s_hi, s_cnt;
+  __shared__ int s_hi, s_cnt, s_back;
   const int tid = threadIdx.x;
-  if (tid == 0) { s_hi = k2; s_cnt = 0; }
+  if (tid == 0) { s_hi = k2; s_cnt = 0; s_back = 0; }
   __syncthreads();
+  if (laswp_plan_parallel(k1, k2, ipiv, inc, moves, nmoves, ok, &s_back)) return;
   for (int k = k1 + tid; k < k2; k += blockDim.x) atomicMax(&s_hi, ipiv[k] + 1);
   __syncthreads();
   const int span = s_hi - k1;

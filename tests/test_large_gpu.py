@@ -7,9 +7,10 @@
 * getrf and the mixed solver at n = 9000: more rows than one cluster of the
   fused leaf panel holds (16 x 512), so the first blocks go through the
   recursive panel path and the later ones through the fused kernel;
-* getrf of a 30000 x 512 matrix: pivot rows farther below the block than a
-  row-interchange plan tracks (24576 rows), so the interchanges outside the
-  blocks take the sequential per-column path.
+* getrf of a 30000 x 512 matrix: pivot rows up to ~30000 rows below their
+  block, farther than the sequential interchange plan can track (24576 rows);
+  getrf's pivots take the parallel plan, which keeps only the rows a chunk of
+  interchanges touches.
 
 References are computed on the GPU with torch (FP64) and the checks are the
 tester-style normwise residuals (bin/lutst.c, bin/slvtst.c: pass <= 100)."""
