@@ -741,32 +741,38 @@ trsm_llu_small_kernel(int m, int n, const T *__restrict__ L, long lda, T *B, lon
 //   X_ib = inv(L_ib,ib) (B_ib - sum_{kt < ib} L_ib,kt X_kt),
 // 32-term dot products instead of the 31-step shuffle chain.  Entries of L
 // above the diagonal (U's, in a packed LU) are never read.  NCOL = 8 CPT
-// columns per CTA, CPT per thread: 256 columns spread over 32 CTAs.
+// columns per CTA, CPT per thread: 256 columns spread over 32 CTAs.  With
+// KS = 2 (the narrow look-ahead block, one column per thread) each 32-term
+// product is split between two warps, whose halves meet in shared memory:
+// twice the warps per CTA to hide the chain's latency.
 // Tile (ib, kt) sits at t = ib (ib + 1) / 2 + kt, stored [k][i] = L[32 ib + i][32 kt + k]
 // (lane = row: conflict-free reads).
 constexpr int LLI_TILES = 36;
 
-template <int CPT>
-__global__ void __launch_bounds__(256, 1)
+template <int CPT, int KS>
+__global__ void __launch_bounds__(256 * KS, 1)
 trsm_llu_inv_kernel(int m, int n, const float *__restrict__ L, long lda, float *B, long ldb) {
   constexpr int NCOL = 8 * CPT;
   extern __shared__ __align__(16) unsigned char lli_smem[];
   float *sLT = reinterpret_cast<float *>(lli_smem);  // the tiles, 1024 floats each
   float *sX = sLT + LLI_TILES * 1024;                 // [NCOL][256]: B, then X
   float *sY = sX + NCOL * LLU_MAX;                    // [NCOL][32]: one block row before inv(L_ib,ib)
+  float *sP = sY + NCOL * 32;                         // [KS][NCOL][32]: the k-range halves' sums (KS = 2)
+  constexpr int NT = 256 * KS, KR = 32 / KS;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int cw = warp & 7, h = warp >> 3, kb = h * KR;  // columns cw + 8 e, k in [kb, kb + KR) of each tile
   const int c0 = blockIdx.x * NCOL, nc = min(NCOL, n - c0);
   const int nblk = (m + 31) / 32;
   for (int ib = 0; ib < nblk; ib++)
     for (int kt = 0; kt <= ib; kt++) {
       float *dst = sLT + (ib * (ib + 1) / 2 + kt) * 1024;
-      for (int e = tid; e < 1024; e += 256) {
+      for (int e = tid; e < 1024; e += NT) {
         const int k = e >> 5, i = e & 31, r = 32 * ib + i, c = 32 * kt + k;
         const bool ok = r < m && c < m && (kt < ib || i > k);  // strictly lower, zero elsewhere
         cp_async4(dst + e, ok ? L + r + (long)c * lda : L, ok);
       }
     }
-  for (int e = tid; e < NCOL * LLU_MAX; e += 256) {
+  for (int e = tid; e < NCOL * LLU_MAX; e += NT) {
     const int c = e / LLU_MAX, r = e % LLU_MAX;
     const bool ok = r < m && c < nc;
     cp_async4(sX + e, ok ? B + r + (long)(c0 + c) * ldb : B, ok);
@@ -800,13 +806,13 @@ trsm_llu_inv_kernel(int m, int n, const float *__restrict__ L, long lda, float *
     for (int kt = 0; kt < ib; kt++) {
       const float *T = sLT + (ib * (ib + 1) / 2 + kt) * 1024;
 #pragma unroll 4
-      for (int k = 0; k < 32; k += 4) {
+      for (int k = kb; k < kb + KR; k += 4) {
         float lv[4];
 #pragma unroll
         for (int q = 0; q < 4; q++) lv[q] = T[(k + q) * 32 + lane];
 #pragma unroll
         for (int e = 0; e < CPT; e++) {
-          const float4 xv = *reinterpret_cast<const float4 *>(sX + (warp + 8 * e) * LLU_MAX + 32 * kt + k);
+          const float4 xv = *reinterpret_cast<const float4 *>(sX + (cw + 8 * e) * LLU_MAX + 32 * kt + k);
           acc[e][0] = fmaf(lv[0], xv.x, acc[e][0]);
           acc[e][1] = fmaf(lv[1], xv.y, acc[e][1]);
           acc[e][0] = fmaf(lv[2], xv.z, acc[e][0]);
@@ -814,48 +820,75 @@ trsm_llu_inv_kernel(int m, int n, const float *__restrict__ L, long lda, float *
         }
       }
     }
+    if constexpr (KS == 1) {
 #pragma unroll
-    for (int e = 0; e < CPT; e++) {
-      const int c = warp + 8 * e;
-      sY[c * 32 + lane] = sX[c * LLU_MAX + r0 + lane] - (acc[e][0] + acc[e][1]);
+      for (int e = 0; e < CPT; e++) {
+        const int c = cw + 8 * e;
+        sY[c * 32 + lane] = sX[c * LLU_MAX + r0 + lane] - (acc[e][0] + acc[e][1]);
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < CPT; e++) sP[(h * NCOL + cw + 8 * e) * 32 + lane] = acc[e][0] + acc[e][1];
+      __syncthreads();
+      if (h == 0) {
+#pragma unroll
+        for (int e = 0; e < CPT; e++) {
+          const int c = cw + 8 * e;
+          sY[c * 32 + lane] = sX[c * LLU_MAX + r0 + lane] - (sP[c * 32 + lane] + sP[(NCOL + c) * 32 + lane]);
+        }
+      }
     }
     __syncthreads();
     const float *D = sLT + (ib * (ib + 1) / 2 + ib) * 1024;
 #pragma unroll
     for (int e = 0; e < CPT; e++) acc[e][0] = acc[e][1] = 0.f;
 #pragma unroll 4
-    for (int k = 0; k < 32; k += 4) {
+    for (int k = kb; k < kb + KR; k += 4) {
       float lv[4];
 #pragma unroll
       for (int q = 0; q < 4; q++) lv[q] = D[(k + q) * 32 + lane];
 #pragma unroll
       for (int e = 0; e < CPT; e++) {
-        const float4 yv = *reinterpret_cast<const float4 *>(sY + (warp + 8 * e) * 32 + k);
+        const float4 yv = *reinterpret_cast<const float4 *>(sY + (cw + 8 * e) * 32 + k);
         acc[e][0] = fmaf(lv[0], yv.x, acc[e][0]);
         acc[e][1] = fmaf(lv[1], yv.y, acc[e][1]);
         acc[e][0] = fmaf(lv[2], yv.z, acc[e][0]);
         acc[e][1] = fmaf(lv[3], yv.w, acc[e][1]);
       }
     }
+    if constexpr (KS == 1) {
 #pragma unroll
-    for (int e = 0; e < CPT; e++) sX[(warp + 8 * e) * LLU_MAX + r0 + lane] = acc[e][0] + acc[e][1];
+      for (int e = 0; e < CPT; e++) sX[(cw + 8 * e) * LLU_MAX + r0 + lane] = acc[e][0] + acc[e][1];
+    } else {
+#pragma unroll
+      for (int e = 0; e < CPT; e++) sP[(h * NCOL + cw + 8 * e) * 32 + lane] = acc[e][0] + acc[e][1];
+      __syncthreads();
+      if (h == 0) {
+#pragma unroll
+        for (int e = 0; e < CPT; e++) {
+          const int c = cw + 8 * e;
+          sX[c * LLU_MAX + r0 + lane] = sP[c * 32 + lane] + sP[(NCOL + c) * 32 + lane];
+        }
+      }
+    }
     __syncthreads();
   }
-  for (int e = tid; e < NCOL * LLU_MAX; e += 256) {
+  for (int e = tid; e < NCOL * LLU_MAX; e += NT) {
     const int c = e / LLU_MAX, r = e % LLU_MAX;
     if (r < m && c < nc) B[r + (long)(c0 + c) * ldb] = sX[e];
   }
 }
 
-template <int CPT>
+template <int CPT, int KS>
 void trsm_llu_inv_launch(int m, int n, const float *L, long lda, float *B, long ldb, cudaStream_t st) {
-  constexpr int smem = (LLI_TILES * 1024 + 8 * CPT * (LLU_MAX + 32)) * (int)sizeof(float);
+  constexpr int smem = (LLI_TILES * 1024 + 8 * CPT * (LLU_MAX + 32 + 32 * KS)) * (int)sizeof(float);
   static bool configured = false;
   if (!configured) {
-    ATLB_CUDA_CHECK(cudaFuncSetAttribute(trsm_llu_inv_kernel<CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(trsm_llu_inv_kernel<CPT, KS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         smem));
     configured = true;
   }
-  trsm_llu_inv_kernel<CPT><<<cdiv(n, 8 * CPT), 256, smem, st>>>(m, n, L, lda, B, ldb);
+  trsm_llu_inv_kernel<CPT, KS><<<cdiv(n, 8 * CPT), 256 * KS, smem, st>>>(m, n, L, lda, B, ldb);
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
 }  // namespace
@@ -864,8 +897,8 @@ template <typename T>
 void trsm_llu_small_dev(int m, int n, const T *L, long lda, T *B, long ldb, cudaStream_t st) {
   if (m <= 0 || n <= 0) return;
   if (sizeof(T) == 4) {  // FP32: L in shared memory, inverted diagonal tiles
-    if (n <= 8 * num_sms()) trsm_llu_inv_launch<1>(m, n, (const float *)L, lda, (float *)B, ldb, st);
-    else trsm_llu_inv_launch<4>(m, n, (const float *)L, lda, (float *)B, ldb, st);
+    if (n <= 8 * num_sms()) trsm_llu_inv_launch<1, 2>(m, n, (const float *)L, lda, (float *)B, ldb, st);
+    else trsm_llu_inv_launch<4, 1>(m, n, (const float *)L, lda, (float *)B, ldb, st);
     return;
   }
   constexpr int smem = (LLU_MAX * (LLU_COLS + 1) + 32 * 33) * (int)sizeof(T);
