@@ -142,14 +142,15 @@ const char *atlb_tune_name(int i);
 
 /* atlb_dtrsm_dev without any device allocation.  No counterpart in the
  * reference.  For callers that cannot let the library call cudaMalloc:
- * code running during a CUDA graph capture, applications whose device memory
- * is owned by their own pool or framework allocator, and programs with a
- * fixed memory budget.  The workspace is a 2 MiB array compiled into the
- * library (held on every GPU that loads it until exit), so the triangle's
- * order (M for Side = Left, N for Right) may be at most 4096; larger orders
- * are rejected with a message and -5 / -6.  The first call on a device looks
- * up the array's device address; make it before any stream capture starts.
- * All calls share the array: calls that overlap on the GPU race on it. */
+ * applications whose device memory is owned by their own pool or framework
+ * allocator, and programs with a fixed memory budget checked up front.  The
+ * workspace is a 2 MiB array compiled into the library (held on every GPU
+ * that loads it until exit), so the triangle's order (M for Side = Left, N
+ * for Right) may be at most 4096; larger orders are rejected with a message
+ * and -5 / -6.  The first call on a device looks up the array's device
+ * address (on the library's device, whatever device the calling thread has
+ * current); make it before any stream capture starts.  All calls share the
+ * array: calls that overlap on the GPU race on it. */
 int atlb_dtrsm_dev_noalloc(int Side, int Uplo, int TransA, int Diag, int M, int N, double alpha,
                            const double *A, int lda, double *B, int ldb);
 int atlb_dgetrf_dev(int M, int N, double *A, int lda, int *ipiv, int *dinfo);
