@@ -31,28 +31,10 @@ static int orc_nthreads = 1;
 void orc_set_threads(int n) { orc_nthreads = n < 1 ? 1 : n; }
 int orc_get_threads(void) { return orc_nthreads; }
 typedef void (*orc_range_fn)(void *ctx, int lo, int hi);
-struct orc_job { orc_range_fn fn; void *ctx; int lo, hi; };
-static void *orc_job_run(void *p)
-{
-  struct orc_job *j = (struct orc_job *)p;
-  j->fn(j->ctx, j->lo, j->hi);
-  return NULL;
-}
-static void orc_par_for(int n, orc_range_fn fn, void *ctx)
-{
-  int nt = orc_nthreads < n ? orc_nthreads : n;
-  if (nt <= 1) { if (n > 0) fn(ctx, 0, n); return; }
-  pthread_t th[256];
-  struct orc_job jobs[256];
-  if (nt > 256) nt = 256;
-  for (int t = 0; t < nt; t++) {
-    jobs[t].fn = fn; jobs[t].ctx = ctx;
-    jobs[t].lo = (int)((int64_t)n * t / nt); jobs[t].hi = (int)((int64_t)n * (t + 1) / nt);
-    if (t) pthread_create(&th[t], NULL, orc_job_run, &jobs[t]);
-  }
-  orc_job_run(&jobs[0]);
-  for (int t = 1; t < nt; t++) pthread_join(th[t], NULL);
-}
+/* Splits 0..n-1 into one range per host thread and runs fn on them (the
+ * persistent thread pool of orc_fast.c). */
+void orc_pool_ranges(int n, orc_range_fn fn, void *ctx);
+static void orc_par_for(int n, orc_range_fn fn, void *ctx) { orc_pool_ranges(n, fn, ctx); }
 
 #define ORC_COLMAJOR 102
 #define ORC_NOTRANS 111
@@ -200,12 +182,24 @@ static void dgemm_cols(void *p, int j0, int j1)
     }
   }
 }
+/* cache-blocked, threaded versions (orc_fast.c), used above these sizes */
+void orc_dgemm_blk(int ta, int tb, int M, int N, int K, double alpha, const double *A, int lda,
+                   const double *B, int ldb, double beta, double *C, int ldc);
+void orc_dtrsm_left_blk(int uplo, int trans, int diag, int M, int N, double alpha, const double *T,
+                        int ldt, double *B, int ldb);
+void orc_dlaswp_blk(int N, double *A, int lda, int k1, int k2, const int *ipiv, int inc);
+#define ORC_BLK_GEMM_WORK (16.0 * 16.0 * 16.0)
+
 void orc_dgemm(int TA, int TB, int M, int N, int K, double alpha,
                const double *A, int lda, const double *B, int ldb,
                double beta, double *C, int ldc)
 { /* C = alpha*op(A)*op(B) + beta*C; beta == 0 overwrites C without reading */
+  if ((double)M * N * K > ORC_BLK_GEMM_WORK) {
+    orc_dgemm_blk(TA, TB, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+    return;
+  }
   struct gemm_ctx g = {TA, TB, M, K, alpha, beta, A, lda, B, ldb, C, ldc};
-  orc_par_for(N, dgemm_cols, &g);
+  dgemm_cols(&g, 0, N);  /* small: one thread (waking the pool costs more) */
 }
 
 struct sgemm_ctx { int TA, TB, M, K; float alpha, beta; const float *A; int lda;
@@ -295,9 +289,15 @@ void orc_dtrsm(int side, int uplo, int transa, int diag, int M, int N,
                double alpha, const double *A, int lda, double *B, int ldb)
 { /* solve op(A)*X = alpha*B (Left) or X*op(A) = alpha*B (Right); X -> B.
      ATL_dreftrsm (src/blas/reference/level3/ATL_dreftrsm.c) */
+  if (side == ORC_LEFT && (double)M * M * N > ORC_BLK_GEMM_WORK) {
+    orc_dtrsm_left_blk(uplo, transa, diag, M, N, alpha, A, lda, B, ldb);
+    return;
+  }
   struct trsm_ctx t = {side, uplo, transa, diag, M, N,
                        (uplo == ORC_LOWER) == (transa == ORC_NOTRANS), alpha, A, lda, B, ldb};
-  orc_par_for(side == ORC_LEFT ? N : M, trsm_range, &t);
+  const double work = side == ORC_LEFT ? (double)M * M * N : (double)N * N * M;
+  if (work <= ORC_BLK_GEMM_WORK) trsm_range(&t, 0, side == ORC_LEFT ? N : M);
+  else orc_par_for(side == ORC_LEFT ? N : M, trsm_range, &t);
 }
 
 void orc_dtrmm(int side, int uplo, int transa, int diag, int M, int N,
@@ -362,6 +362,10 @@ void orc_dlaswp(int N, double *A, int lda, int K1, int K2, const int *ipiv, int 
 { /* ATL_laswp (src/lapack/ATL_laswp.c:7-116): for i=K1..K2-1 (or reversed
      when inci<0) swap rows i and ipiv[i] over N columns */
   if (K2 <= K1) return;
+  if (N >= 64 && (double)N * (K2 - K1) > 65536.0) {  /* 32-column blocks, as the reference does */
+    orc_dlaswp_blk(N, A, lda, K1, K2, ipiv, inci);
+    return;
+  }
   if (inci > 0) {
     for (int i = K1; i < K2; i++) {
       int ip = ipiv[i];

@@ -1,5 +1,6 @@
 """ctypes front end of the CPU oracle (oracle/atl_oracle.c) and of the
-reference's own C BLAS compiled into oracle/_ref/.
+reference's own C BLAS and LAPACK compiled into oracle/_ref/ by
+oracle/build_ref.sh.
 
 Test infrastructure only: imported by tests/, the smoke check and the CPU
 baseline leg of bench.py -- never by the library.  Arrays are numpy,
@@ -14,6 +15,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORC_LIB = os.path.join(HERE, "liborc.so")
 REF_LIB = os.path.join(HERE, "_ref", "libatlref.so")
+REF_LAPACK_LIB = os.path.join(HERE, "_ref", "libatlref_lapack.so")
 
 NoTrans, Trans = 111, 112
 Upper, Lower = 121, 122
@@ -64,8 +66,19 @@ _REF_SIGS = {
     "ATL_drefsyrk": (None, [_I, _I, _I, _I, _D, _P, _I, _D, _P, _I]),
 }
 
+# the reference's LAPACK entry points (src/lapack/ATL_getrf.c:8, ATL_getrs.c:8,
+# ATL_potrf.c:7, ATL_potrs.c:13, ATL_geqrf.c:29), type-prefixed as a DREAL build names them
+_REF_LAPACK_SIGS = {
+    "ATL_dgetrf": (_I, [_I, _I, _I, _P, _I, _P]),
+    "ATL_dgetrs": (None, [_I, _I, _I, _I, _P, _I, _P, _P, _I]),
+    "ATL_dpotrf": (_I, [_I, _I, _I, _P, _I]),
+    "ATL_dpotrs": (None, [_I, _I, _I, _I, _P, _I, _P, _I]),
+    "ATL_dgeqrf": (_I, [_I, _I, _P, _I, _P, _P, _I]),
+}
+
 _orc = None
 _ref = None
+_ref_lapack = None
 
 
 def _load(path, sigs):
@@ -96,6 +109,68 @@ def ref():
     if _ref is None:
         _ref = _load(REF_LIB, _REF_SIGS)
     return _ref
+
+
+def ref_lapack_available():
+    return os.path.exists(REF_LAPACK_LIB)
+
+
+def ref_lapack():
+    """The reference's own LAPACK path (oracle/_ref/libatlref_lapack.so)."""
+    global _ref_lapack
+    if _ref_lapack is None:
+        _ref_lapack = _load(REF_LAPACK_LIB, _REF_LAPACK_SIGS)
+    return _ref_lapack
+
+
+def ref_dgetrf(a, order=102):
+    """ATL_getrf of the reference on a copy of a: (LU, ipiv, info)."""
+    a = np.array(a, order="F", copy=True)
+    m, n = a.shape
+    if order == 101:  # row-major: the buffer holds the m x n matrix row by row
+        ld = n
+        buf = np.ascontiguousarray(a)
+    else:
+        ld = m
+        buf = a
+    ipiv = np.zeros(max(min(m, n), 1), dtype=np.int32)
+    info = ref_lapack().ATL_dgetrf(order, m, n, buf.ctypes.data, max(ld, 1), ipiv.ctypes.data)
+    out = np.asfortranarray(buf) if order == 101 else buf
+    return out, ipiv[:min(m, n)], info
+
+
+def ref_dgetrs(trans, lu, ipiv, b):
+    b = np.array(b, order="F", copy=True)
+    n = lu.shape[1]
+    ref_lapack().ATL_dgetrs(102, trans, n, b.shape[1], P(lu), lu.shape[0],
+                            np.ascontiguousarray(ipiv, np.int32).ctypes.data, P(b), b.shape[0])
+    return b
+
+
+def ref_dpotrf(uplo, a):
+    a = np.array(a, order="F", copy=True)
+    info = ref_lapack().ATL_dpotrf(102, uplo, a.shape[1], P(a), a.shape[0])
+    return a, info
+
+
+def ref_dpotrs(uplo, f, b):
+    b = np.array(b, order="F", copy=True)
+    ref_lapack().ATL_dpotrs(102, uplo, f.shape[1], b.shape[1], P(f), f.shape[0], P(b), b.shape[0])
+    return b
+
+
+def ref_dgeqrf(a):
+    """ATL_geqrf of the reference (workspace query, then the factorization)."""
+    a = np.array(a, order="F", copy=True)
+    m, n = a.shape
+    tau = np.zeros(max(min(m, n), 1))
+    w = np.zeros(1)
+    lib = ref_lapack()
+    lib.ATL_dgeqrf(m, n, P(a), max(m, 1), P(tau), P(w), -1)
+    lw = max(int(w[0]), 1)
+    w = np.zeros(lw)
+    info = lib.ATL_dgeqrf(m, n, P(a), max(m, 1), P(tau), P(w), lw)
+    return a, tau[:min(m, n)], info
 
 
 def P(a):

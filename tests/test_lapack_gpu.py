@@ -196,3 +196,68 @@ def test_device_api_getrf_potrf(gpu, orc):
     assert int(info.item()) == 0
     np.testing.assert_array_equal(ipiv.cpu().numpy(), rpiv)
     np.testing.assert_allclose(A.cpu().numpy().T, ref, rtol=1e-10, atol=1e-10)
+
+
+# ------------------------------------------------- pinned to the reference's own LAPACK
+import golden_lapack as GL  # noqa: E402
+
+
+def test_getrf_vs_reference_lapack_golden(gpu):
+    """ipiv and info identical to the reference's ATL_getrf (getrfC / getrfR) on
+    the testers' sizes, ties in the pivot search, zero columns, row-major and
+    1 x n / m x 1 edges; the factors agree to rounding."""
+    for i, a, order, lu_ref, ipiv_ref, info_ref in GL.getrf_cases():
+        m, n = a.shape
+        ipiv = np.zeros(max(min(m, n), 1), dtype=np.int32)
+        if order == RM:
+            buf = np.ascontiguousarray(a)
+            info = AB.clapack_dgetrf(RM, m, n, buf, max(n, 1), ipiv)
+            lu = buf
+        else:
+            lu = a.copy(order="F")
+            info = AB.clapack_dgetrf(CM, m, n, lu, max(m, 1), ipiv)
+        assert info == info_ref, f"getrf case {i}"
+        np.testing.assert_array_equal(ipiv[:min(m, n)], ipiv_ref, err_msg=f"getrf case {i}")
+        assert GL.close(lu, lu_ref, 1e-10), f"getrf case {i}"
+
+
+def test_getrs_vs_reference_lapack_golden(gpu):
+    cases = GL.getrf_cases()
+    for i, fi, trans, b, x_ref in GL.getrs_cases():
+        _, _, _, lu, ipiv, _ = cases[fi]
+        n = lu.shape[0]
+        x = np.array(b, order="F")
+        lu = np.asfortranarray(lu)
+        AB.clapack_dgetrs(CM, trans, n, x.shape[1], lu, n, np.ascontiguousarray(ipiv, np.int32), x, n)
+        assert GL.close(x, x_ref, 1e-9), f"getrs case {i}"
+
+
+def test_potrf_potrs_vs_reference_lapack_golden(gpu):
+    facs = []
+    for i, a, uplo, f_ref, info_ref in GL.potrf_cases():
+        n = a.shape[0]
+        f = a.copy(order="F")
+        info = AB.clapack_dpotrf(CM, uplo, n, f, n)
+        facs.append((f, uplo))
+        assert info == info_ref, f"potrf case {i}"
+        k = n if info == 0 else info - 1
+        assert GL.close(GL.tri(f, uplo)[:k, :k], f_ref[:k, :k], 1e-11), f"potrf case {i}"
+    for i, fi, b, x_ref in GL.potrs_cases():
+        f, uplo = facs[fi]
+        n = f.shape[0]
+        x = np.array(b, order="F")
+        AB.clapack_dpotrs(CM, uplo, n, x.shape[1], f, n, x, n)
+        assert GL.close(x, x_ref, 1e-9), f"potrs case {i}"
+
+
+def test_geqrf_vs_reference_lapack_golden(gpu):
+    """R, the Householder vectors and tau of the reference's ATL_geqrf
+    (ATLAS's larfg sign and tau conventions)."""
+    for i, a, qr_ref, tau_ref, info_ref in GL.geqrf_cases():
+        m, n = a.shape
+        qr = a.copy(order="F")
+        tau = np.zeros(max(min(m, n), 1))
+        info = AB.clapack_dgeqrf(CM, m, n, qr, max(m, 1), tau)
+        assert info == info_ref == 0, f"geqrf case {i}"
+        assert GL.close(qr, qr_ref, 1e-10), f"geqrf case {i}"
+        assert GL.close(tau[:min(m, n)], tau_ref, 1e-10), f"geqrf case {i}"
