@@ -68,6 +68,7 @@ _SIGS = {
     "atlb_tune_name": (_S, [_I]),
     "atlb_dsyrk_dev": (_I, [_I, _I, _I, _I, _D, _P, _I, _D, _P, _I]),
     "atlb_dgetrf_dev": (_I, [_I, _I, _P, _I, _P, _P]),
+    "atlb_sgetrf_dev": (_I, [_I, _I, _P, _I, _P, _P, _I]),
     "atlb_dgetrs_dev": (_I, [_I, _I, _I, _P, _I, _P, _P, _I]),
     "atlb_dpotrf_dev": (_I, [_I, _I, _P, _I, _P]),
     "atlb_dpotrs_dev": (_I, [_I, _I, _I, _P, _I, _P, _I]),

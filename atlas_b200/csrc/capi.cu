@@ -10,6 +10,7 @@
 #include <vector>
 #include "common.cuh"
 #include "kernels.h"
+#include "mixed.h"
 #include "../../include/atlas_b200.h"
 #include "staging.h"
 
@@ -590,6 +591,16 @@ int atlb_dgetrf_dev(int M, int N, double *A, int lda, int *ipiv, int *dinfo) {
   if (lda < std::max(1, M)) return -4;
   if (std::min(M, N) == 0) return 0;
   getrf_dev<double>(M, N, A, lda, ipiv, dinfo, stream());
+  return 0;
+}
+
+int atlb_sgetrf_dev(int M, int N, float *A, int lda, int *ipiv, int *dinfo, int prec) {
+  if (M < 0) return -1;
+  if (N < 0) return -2;
+  if (lda < std::max(1, M)) return -4;
+  if (prec < kPrecFP32 || prec > kPrecTF32x3) return -7;
+  if (std::min(M, N) == 0) return 0;
+  getrf_dev<float>(M, N, A, lda, ipiv, dinfo, stream(), factor_gemm(prec));
   return 0;
 }
 

@@ -629,271 +629,6 @@ getf2_fused_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restric
   panel_u12_solve<T, NB>(MN, ncols, nright, crank * (PT / 32) + warp, C * (PT / 32), A, lda);
 }
 
-// Tournament-pivoting panel for the FP32 factorization inside the
-// mixed-precision solvers (communication-avoiding LU: Grigori, Demmel & Xiang,
-// "CALU", SIAM J. Matrix Anal. Appl. 32(4), 2011).  Pivots are no longer those
-// of partial pivoting, which only the solver's FP64 refinement observes; in
-// exchange a 32-column panel needs four cluster barriers instead of one per
-// column:
-//   1. every CTA runs partial pivoting on its own rows (CTA barriers only) to
-//      select up to 32 candidate rows and sends their ORIGINAL values to CTA 0;
-//   2. CTA 0 runs partial pivoting on the candidates: the winners are the
-//      panel's pivot rows, in order, with their U11 rows and L11 multipliers;
-//      one warp replays the interchanges to produce ipiv and the final row of
-//      every row that moves;
-//   3. every row solves l U11 = (its original row) for its multipliers;
-//   4. rows go to their final positions, the block's other columns are
-//      interchanged and U12 = L11^-1 A12 is solved, as in getf2_fused_kernel.
-template <typename T, int NB>
-__global__ void __launch_bounds__(PT, 1)
-getf2_tournament_kernel(int M, int ncols, T *__restrict__ A, long lda, int *__restrict__ ipiv, int roff,
-                        int *__restrict__ dinfo, int nleft, int nright) {
-  static_assert(NB == 32, "one row element per lane");
-  cg::cluster_group cl = cg::this_cluster();
-  const int C = (int)cl.num_blocks(), crank = (int)cl.block_rank();
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int MN = min(M, ncols), CC = C * NB;
-  extern __shared__ __align__(16) unsigned char tourn_smem[];
-  T *Lsm = reinterpret_cast<T *>(tourn_smem);  // CTA 0: candidates [k][CC]; later the interchange stash
-  __shared__ __align__(16) T wrow[2][PT / 32][NB + 4];  // warp winners' rows (+ 1/pivot), by column parity
-  __shared__ unsigned long long wkey[2][PT / 32];
-  __shared__ unsigned wrid[2][PT / 32];
-  __shared__ int cand_row[kMaxPanelCluster * NB];
-  __shared__ T U11[NB][NB + 1], L11[NB][NB + 1];
-  __shared__ T urcp[NB];
-  __shared__ __align__(16) T zrow[NB];
-  __shared__ int P[NB];
-  __shared__ int e_row[2 * NB], e_pos[2 * NB];
-  __shared__ int s_ne;
-  if (tid < NB) zrow[tid] = T(0);
-  for (int idx = tid; idx < NB * (NB + 1); idx += PT) {
-    (&U11[0][0])[idx] = T(0);
-    (&L11[0][0])[idx] = T(0);
-  }
-  __syncwarp();
-  cluster_arrive();  // every CTA of the cluster runs before any remote store
-  cluster_wait();
-
-  const int r = crank * PT + tid;
-  const bool in = r < M;
-  T o[NB], a[NB];
-  {
-    const T *src = A + (in ? r : 0);
-#pragma unroll
-    for (int k = 0; k < NB; k++) {
-      o[k] = (in && k < ncols) ? __ldg(src) : T(0);
-      a[k] = o[k];
-      if (k + 1 < ncols) src += lda;
-    }
-  }
-  __syncthreads();
-
-  // One step of partial pivoting among the active rows of this CTA on the
-  // shifted rows a[]: returns the winner's row id; the winner leaves, the
-  // others are updated.  One __syncthreads per column.
-  bool act = in;
-  int myj = -1;
-  auto gepp_step = [&](int j, int rid, T &lout) -> int {
-    const int b = j & 1;
-    // tournament pivoting needs the largest |value|, not a particular tie
-    // rule: one redux on the value, ties to the lowest lane
-    // active rows rank above inactive ones: NaN -> 1, numbers -> |value| bits + 2
-    const unsigned key = act ? (unsigned)pivot_key(a[0]) + 1u : 0u;
-    const unsigned mk = __reduce_max_sync(0xffffffffu, key);
-    const int wl = __ffs(__ballot_sync(0xffffffffu, key == mk)) - 1;
-    const int wrid_w = __shfl_sync(0xffffffffu, act ? rid : -1, wl);
-    if (lane == wl && act) {
-      float4 *dst = reinterpret_cast<float4 *>(wrow[b][warp]);
-#pragma unroll
-      for (int q = 0; q < NB / 4; q++) dst[q] = make_float4(a[4 * q], a[4 * q + 1], a[4 * q + 2], a[4 * q + 3]);
-      wrow[b][warp][NB] = __frcp_rn(a[0]);
-    }
-    if (lane == 0) { wkey[b][warp] = mk; wrid[b][warp] = (unsigned)wrid_w; }
-    __syncthreads();
-    const unsigned k2 = lane < PT / 32 ? (unsigned)wkey[b][lane] : 0u;
-    const unsigned mk2 = __reduce_max_sync(0xffffffffu, k2);
-    const int cw = __ffs(__ballot_sync(0xffffffffu, lane < PT / 32 && k2 == mk2)) - 1;
-    const int i2 = (int)wrid[b][cw];
-    const T *u = wrow[b][cw];
-    const T piv = u[0];
-    lout = T(0);
-    if (act) {
-      if (rid == i2) {
-        act = false;
-        myj = j;
-      } else {
-        const bool nz = piv != T(0);
-        const T l = nz ? a[0] * u[NB] : T(0);
-        shift_update<T, NB>(a, l, nz ? u : zrow, 1);
-        lout = l;
-      }
-    }
-    return i2;
-  };
-
-  // 1. local candidates
-  const int rows_here = max(0, min(PT, M - crank * PT));
-  const int nloc = min(ncols, rows_here);
-  {
-    T ldummy;
-    for (int j = 0; j < nloc; j++) gepp_step(j, r, ldummy);
-  }
-  if (myj >= 0) {  // send the original row to CTA 0's candidate slot crank*NB + myj
-    const int t = crank * NB + myj;
-    T *dst = cl.map_shared_rank(Lsm, 0);
-#pragma unroll
-    for (int k = 0; k < NB; k++) dst[(long)k * CC + t] = o[k];
-    cl.map_shared_rank(cand_row, 0)[t] = r;
-  }
-  __syncwarp();
-  cluster_arrive();
-  cluster_wait();
-
-  // 2. the final among the candidates (CTA 0)
-  if (crank == 0) {
-    const int q = tid / NB, jq = tid % NB;
-    const int nq = min(ncols, max(0, min(PT, M - q * PT)));
-    const bool valid = tid < CC && jq < nq;
-    act = valid;
-    myj = -1;
-    const int rid = valid ? cand_row[tid] : INT_MAX;
-#pragma unroll
-    for (int k = 0; k < NB; k++) a[k] = valid ? Lsm[(long)k * CC + tid] : T(0);
-    __syncthreads();  // every candidate is in registers: Lsm now holds its multipliers
-    for (int j = 0; j < MN; j++) {
-      T l;
-      const int win = gepp_step(j, rid, l);
-      if (tid == 0) P[j] = win;
-      if (valid && act) Lsm[(long)j * CC + tid] = l;
-    }
-    if (myj >= 0) {  // chosen at column myj: its row is row myj of U, its multipliers row myj of L
-      const int j = myj;
-      if (a[0] == T(0)) atomicMin(dinfo, roff + j + 1);
-#pragma unroll
-      for (int k = 0; k < NB; k++)
-        if (j + k < NB) U11[j][j + k] = a[k];
-      for (int i = 0; i < j; i++) L11[j][i] = Lsm[(long)i * CC + tid];
-    }
-    __syncthreads();
-    if (warp == 0) {
-      // interchanges: rows at positions 0..MN-1 and pivot rows from below
-      if (lane == 0) {
-        int ne = 0;
-        for (int i = 0; i < MN; i++) { e_row[ne] = i; e_pos[ne] = i; ne++; }
-        for (int j = 0; j < MN; j++)
-          if (P[j] >= MN) { e_row[ne] = P[j]; e_pos[ne] = P[j]; ne++; }
-        s_ne = ne;
-      }
-      __syncwarp();
-      const int ne = s_ne;
-      int er0 = lane < ne ? e_row[lane] : -1, ep0 = lane < ne ? e_pos[lane] : -1;
-      int er1 = lane + 32 < ne ? e_row[lane + 32] : -1, ep1 = lane + 32 < ne ? e_pos[lane + 32] : -1;
-      for (int j = 0; j < MN; j++) {
-        const int pr = P[j];
-        const unsigned m0 = __ballot_sync(0xffffffffu, er0 == pr), m1 = __ballot_sync(0xffffffffu, er1 == pr);
-        const int p = m0 ? __shfl_sync(0xffffffffu, ep0, __ffs(m0) - 1) : __shfl_sync(0xffffffffu, ep1, __ffs(m1) - 1);
-        if (lane == 0) ipiv[j] = roff + p;
-        if (ep0 == j) ep0 = p;
-        if (ep1 == j) ep1 = p;
-        if (er0 == pr) ep0 = j;
-        if (er1 == pr) ep1 = j;
-      }
-      if (lane < ne) e_pos[lane] = ep0;
-      if (lane + 32 < ne) e_pos[lane + 32] = ep1;
-    }
-  }
-  __syncwarp();
-  cluster_arrive();
-  cluster_wait();
-
-  // 3. everybody: U11, L11, the pivot order and the moves from CTA 0
-  if (crank != 0) {
-    const T(*rU)[NB + 1] = cl.map_shared_rank(U11, 0);
-    const T(*rL)[NB + 1] = cl.map_shared_rank(L11, 0);
-    for (int idx = tid; idx < NB * NB; idx += PT) {
-      const int i = idx / NB, k = idx % NB;
-      U11[i][k] = rU[i][k];
-      L11[i][k] = rL[i][k];
-    }
-    if (tid < NB) P[tid] = cl.map_shared_rank(P, 0)[tid];
-    if (tid < 2 * NB) {
-      e_row[tid] = cl.map_shared_rank(e_row, 0)[tid];
-      e_pos[tid] = cl.map_shared_rank(e_pos, 0)[tid];
-    }
-    if (tid == 0) s_ne = *cl.map_shared_rank(&s_ne, 0);
-  }
-  __syncthreads();
-  if (tid < MN) urcp[tid] = T(1) / U11[tid][tid];
-  __syncthreads();
-  int pi = -1;
-  for (int i = 0; i < MN; i++)
-    if (P[i] == r) pi = i;
-  if (in) {
-    if (pi >= 0) {  // pivot row pi: multipliers, then its U row
-#pragma unroll
-      for (int k = 0; k < NB; k++) a[k] = k < pi ? L11[pi][k] : (k < ncols ? U11[pi][k] : T(0));
-    } else {  // l U11 = o, column by column (U11's diagonal through its reciprocal)
-#pragma unroll
-      for (int k = 0; k < NB; k++) {
-        T s = o[k];
-#pragma unroll
-        for (int i = 0; i < k; i++) s = fma(-a[i], U11[i][k], s);
-        a[k] = k < MN ? s * urcp[k] : T(0);
-      }
-    }
-  }
-  const int ne = s_ne;
-  int fp = r;
-  for (int e = 0; e < ne; e++)
-    if (e_row[e] == r) fp = e_pos[e];
-  if (in) {
-#pragma unroll
-    for (int k = 0; k < NB; k++)
-      if (k < ncols) A[fp + (long)k * lda] = a[k];
-  }
-
-  // 4. the block's other columns of the moved rows (balanced over the cluster)
-  const int nother = nleft + nright;
-  __shared__ int l_from[2 * NB], l_to[2 * NB];
-  __shared__ int s_nm;
-  if (tid == 0) {
-    int nm = 0;
-    for (int e = 0; e < ne; e++)
-      if (e_pos[e] != e_row[e]) { l_from[nm] = e_row[e]; l_to[nm] = e_pos[e]; nm++; }
-    s_nm = nother > 0 ? nm : 0;
-  }
-  __syncthreads();
-  const int total = s_nm * nother, per = (total + C - 1) / C;
-  const int g0 = crank * per, g1 = min(total, g0 + per);
-  for (int base = g0 + tid; base < g1; base += 4 * PT) {
-    T v[4];
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const int g = base + q * PT;
-      if (g < g1) {
-        const int i = g / nother, c = g - i * nother;
-        const int col = c < nleft ? c - nleft : ncols + (c - nleft);
-        v[q] = __ldcg(A + l_from[i] + (long)col * lda);
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < 4; q++)
-      if (base + q * PT < g1) Lsm[base + q * PT - g0] = v[q];
-  }
-  __syncwarp();
-  cluster_arrive();
-  cluster_wait();
-  for (int g = g0 + tid; g < g1; g += PT) {
-    const int i = g / nother, c = g - i * nother;
-    const int col = c < nleft ? c - nleft : ncols + (c - nleft);
-    A[l_to[i] + (long)col * lda] = Lsm[g - g0];
-  }
-  __syncwarp();
-  cluster_arrive();  // every row is in place
-  cluster_wait();
-  if (crank == 0 && nright > 0 && MN > 1) panel_u12_solve<T, NB>(MN, ncols, nright, warp, PT / 32, A, lda);
-}
-
 // Fallback for panels taller than a cluster can hold: one CTA, global memory.
 template <typename T>
 __global__ void __launch_bounds__(1024)
@@ -1068,69 +803,14 @@ bool launch_fused_panel(int M, int ncols, T *A, long lda, int *ipiv, int roff, i
   return true;
 }
 
-template <typename T>
-int max_cluster_tournament() {
-  static int cached = -1;
-  if (cached >= 0) return cached;
-  auto kern = getf2_tournament_kernel<T, 32>;
-  cached = 0;
-  if (cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, fused_smem_bytes<T>()) !=
-          cudaSuccess) {
-    cudaGetLastError();
-    return cached;
-  }
-  for (int c : {kMaxPanelCluster, 8}) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(c, 1, 1);
-    cfg.blockDim = dim3(PT, 1, 1);
-    cfg.dynamicSmemBytes = fused_smem_bytes<T>();
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = c;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    int n = 0;
-    if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess) { cudaGetLastError(); n = 0; }
-    if (n > 0) { cached = c; break; }
-  }
-  return cached;
-}
-
-// Tournament-pivoting panel (FP32 factorization of the mixed solvers only).
-bool launch_tournament_panel(int M, int ncols, float *A, long lda, int *ipiv, int roff, int *dinfo,
-                             int nleft, int nright, cudaStream_t st) {
-  if (ncols > 32 || nleft + nright > 256) return false;
-  const int C = cdiv(M, PT);
-  if (C > max_cluster_tournament<float>()) return false;
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(C, 1, 1);
-  cfg.blockDim = dim3(PT, 1, 1);
-  cfg.dynamicSmemBytes = fused_smem_bytes<float>();
-  cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = C;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  ATLB_CUDA_CHECK(cudaLaunchKernelEx(&cfg, getf2_tournament_kernel<float, 32>, M, ncols, A, lda, ipiv, roff,
-                                     dinfo, nleft, nright));
-  return true;
-}
-
-// Partial pivoting stays the default for the FP32 factorization too: on
-// B200 the tournament kernel's two rounds of 32 CTA-local pivot steps cost
-// more than the partial-pivoting kernel's 32 cluster rounds (measured).
-// ATLAS_B200_FP32_PIVOTING=tournament selects it.
-bool tournament_enabled() {
+// FP32 leaf panels (the factorization inside the mixed-precision solvers) use
+// tournament pivoting (calu.cu) unless ATLAS_B200_FP32_PIVOTING=partial asks
+// for partial pivoting, the FP64 path's pivot order.
+bool fp32_tournament() {
   static int v = -1;
   if (v < 0) {
     const char *e = getenv("ATLAS_B200_FP32_PIVOTING");
-    v = (e && strcmp(e, "tournament") == 0) ? 1 : 0;
+    v = (e && strcmp(e, "partial") == 0) ? 0 : 1;
   }
   return v == 1;
 }
@@ -1301,8 +981,8 @@ bool getrf_block(int j, int M, int jb, T *A, long lda, int *ipiv, int *dinfo, cu
     if (m <= 0) break;
     const int nright = jb - l - w;
     T *Ac = A + c + (long)c * lda;
-    if (!(sizeof(T) == 4 && tournament_enabled() &&
-          launch_tournament_panel((int)m, w, (float *)Ac, lda, ipiv + c, c, dinfo, l, nright, st)))
+    if (!(sizeof(T) == 4 && fp32_tournament() &&
+          launch_calu_panel((int)m, w, (float *)Ac, lda, ipiv + c, c, dinfo, l, nright, st)))
       launch_fused_panel<T>(m, w, Ac, lda, ipiv + c, c, dinfo, l, nright, st);
     if (nright > 0 && m - w > 0)  // rank-w update of the block's columns right of the leaf
       rank_update<T>(m - w, nright, w, Ac + w, Ac + (long)w * lda, Ac + w + (long)w * lda, lda, st);
