@@ -119,14 +119,6 @@ void potrs_dev(int uplo, int N, int NRHS, const T *A, long lda, T *B, long ldb, 
 // Householder QR (ATLAS conventions: tau in [1,2], beta = -sign(alpha)*norm).
 void dgeqrf_dev(int M, int N, double *A, long lda, double *tau, cudaStream_t st);
 
-// The FP32 leaf panel with tournament pivoting (calu.cu): factors the M x ncols
-// panel at A (ncols <= 32, M <= calu_max_rows()), writes ipiv (+ roff), and
-// applies its interchanges to the block's nleft columns left and nright right
-// of it, solving U12 on the right ones.  False when the shape does not fit.
-bool launch_calu_panel(int M, int ncols, float *A, long lda, int *ipiv, int roff, int *dinfo, int nleft,
-                       int nright, cudaStream_t st);
-int calu_max_rows();
-
 // Small utilities
 void set_info_kernel_launch(int *dinfo, cudaStream_t st);       // *dinfo = INT_MAX
 void finish_info_kernel_launch(int *dinfo, cudaStream_t st);    // INT_MAX -> 0

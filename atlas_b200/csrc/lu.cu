@@ -803,18 +803,6 @@ bool launch_fused_panel(int M, int ncols, T *A, long lda, int *ipiv, int roff, i
   return true;
 }
 
-// FP32 leaf panels (the factorization inside the mixed-precision solvers) use
-// tournament pivoting (calu.cu) unless ATLAS_B200_FP32_PIVOTING=partial asks
-// for partial pivoting, the FP64 path's pivot order.
-bool fp32_tournament() {
-  static int v = -1;
-  if (v < 0) {
-    const char *e = getenv("ATLAS_B200_FP32_PIVOTING");
-    v = (e && strcmp(e, "partial") == 0) ? 0 : 1;
-  }
-  return v == 1;
-}
-
 bool fused_panel_disabled() {
   static int v = -1;
   if (v < 0) {
@@ -981,9 +969,7 @@ bool getrf_block(int j, int M, int jb, T *A, long lda, int *ipiv, int *dinfo, cu
     if (m <= 0) break;
     const int nright = jb - l - w;
     T *Ac = A + c + (long)c * lda;
-    if (!(sizeof(T) == 4 && fp32_tournament() &&
-          launch_calu_panel((int)m, w, (float *)Ac, lda, ipiv + c, c, dinfo, l, nright, st)))
-      launch_fused_panel<T>(m, w, Ac, lda, ipiv + c, c, dinfo, l, nright, st);
+    launch_fused_panel<T>(m, w, Ac, lda, ipiv + c, c, dinfo, l, nright, st);
     if (nright > 0 && m - w > 0)  // rank-w update of the block's columns right of the leaf
       rank_update<T>(m - w, nright, w, Ac + w, Ac + (long)w * lda, Ac + w + (long)w * lda, lda, st);
   }

@@ -154,13 +154,10 @@ const char *atlb_tune_name(int i);
 int atlb_dtrsm_dev_noalloc(int Side, int Uplo, int TransA, int Diag, int M, int N, double alpha,
                            const double *A, int lda, double *B, int ldb);
 int atlb_dgetrf_dev(int M, int N, double *A, int lda, int *ipiv, int *dinfo);
-/* FP32 LU, the factorization inside the mixed-precision solvers (no
- * counterpart in the reference; LAPACK sgetrf's arguments).  Trailing
- * updates in FP32 (prec 0), TF32 (1), BF16 (2) or split TF32 (3).  The
- * 32-column leaf panels use tournament pivoting (CALU), so ipiv is a valid
- * interchange sequence but not partial pivoting's;
- * ATLAS_B200_FP32_PIVOTING=partial selects partial pivoting.  *dinfo: 0 or the
- * first zero pivot (1-based). */
+/* FP32 LU with partial pivoting, the factorization inside the mixed-precision
+ * solvers (no counterpart in the reference; LAPACK sgetrf's arguments).
+ * Trailing updates in FP32 (prec 0), TF32 (1), BF16 (2) or split TF32 (3).
+ * *dinfo: 0 or the first zero pivot (1-based). */
 int atlb_sgetrf_dev(int M, int N, float *A, int lda, int *ipiv, int *dinfo, int prec);
 int atlb_dgetrs_dev(int Trans, int N, int NRHS, const double *A, int lda, const int *ipiv,
                     double *B, int ldb);
