@@ -145,6 +145,15 @@ def backward_error(torch, acol, x, b):
     return (r.abs().max() / (an * x.abs().max() + b.abs().max())).item()
 
 
+def replica_throughput(ms_local, world):
+    """Whole-job solves/s of `world` independent replicas: every rank solved
+    one system per step; the job's time per step is the slowest rank's
+    (device time, MAX over ranks).  Returns (solves/s, ms per step)."""
+    from atlas_b200 import parallel as PAR
+    ms = PAR.max_over_ranks(ms_local)
+    return world * 1000.0 / ms, ms
+
+
 def host_system(n, kappa, seed):
     """The headline system as column-major host arrays (generated with torch on
     the GPU when there is one; the generation is not timed)."""
@@ -224,6 +233,48 @@ def timed(torch, stream, fn, reps):
     e1.record(stream)
     torch.cuda.synchronize()
     return e0.elapsed_time(e1) / reps
+
+
+def extra_sharded(torch, AB, dev, stream, rank, world):
+    """Paths that shard across GPUs (run when world > 1): DGEMM 8192^3 with C
+    split into column slabs (A broadcast from rank 0 over NCCL inside the
+    timed call, no other exchange), and the 10k batched SPD solves dealt out
+    by work.  Times are device time, MAX over ranks."""
+    from atlas_b200 import parallel as PAR
+    f64 = torch.float64
+    M = 8192
+    g = torch.Generator(device=dev)
+    g.manual_seed(99 + rank)
+    a = torch.rand(M, M, dtype=f64, device=dev, generator=g) * 2 - 1
+    s, w = PAR.column_slabs(M, world)[rank]
+    b = torch.rand(max(w, 1), M, dtype=f64, device=dev, generator=g) * 2 - 1
+    c = torch.zeros(max(w, 1), M, dtype=f64, device=dev)
+    call = lambda: PAR.sharded_dgemm(a, b, c, M, M, M)
+    for _ in range(2):
+        call()
+    ms = PAR.max_over_ranks(timed(torch, stream, call, 3))
+    out = {"sharded_dgemm_8192": {"ms": ms, "tflops_all_ranks": 2.0 * M ** 3 / ms / 1e9, "ranks": world,
+                                  "slab_of_rank0": list(PAR.column_slabs(M, world)[0]),
+                                  "includes": "NCCL broadcast of A (512 MiB) + the rank's DGEMM slab"}}
+    del a, b, c
+    rng = np.random.default_rng(2024)
+    sizes = rng.integers(8, 257, 10000).astype(np.int32)
+    parts = PAR.split_by_work(sizes.astype(np.float64) ** 3 / 3 + 8.0 * sizes.astype(np.float64) ** 2, world)
+    mine = parts[rank]
+    As = [torch.eye(int(n), dtype=f64, device=dev) * (n + 1.0) for n in sizes[mine]]
+    Bs = [torch.ones(4, int(n), dtype=f64, device=dev) for n in sizes[mine]]
+    aptr = np.zeros(len(sizes), np.uint64)
+    bptr = np.zeros(len(sizes), np.uint64)
+    aptr[mine] = [t.data_ptr() for t in As]
+    bptr[mine] = [t.data_ptr() for t in Bs]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    idx, info = PAR.sharded_posv_batched(sizes, aptr, sizes, bptr, sizes, np.full(len(sizes), 4))
+    t1 = time.perf_counter()
+    out["sharded_posv_10k"] = {"ms_max_over_ranks": PAR.max_over_ranks((t1 - t0) * 1e3), "ranks": world,
+                               "problems_rank0": int(len(parts[0])), "all_info_zero": bool(np.all(info == 0)),
+                               "timing": "wall clock around the synchronous call"}
+    return out
 
 
 def extra_factorizations(torch, AB, dev, stream):
@@ -608,16 +659,12 @@ def main():
         ev1.record(stream)
         torch.cuda.synchronize()
         torch.cuda.profiler.stop()
-    ms = ev0.elapsed_time(ev1) / args.steps
+    value, ms = replica_throughput(ev0.elapsed_time(ev1) / args.steps, world)
     if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = t.item()
         dist.barrier()
     per_step, kernel_names = count_kernels(torch, mixed_step)
     head_iter = int(it[0])
     head_berr = backward_error(torch, apristine, x, b0)
-    value = world * 1000.0 / ms
 
     # ---- plain FP64 GPU dgesv (getrf + getrs) on the same system
     A = torch.empty_like(acol0)
@@ -637,6 +684,8 @@ def main():
     del A
 
     out = {}
+    if world > 1:
+        out["multi_gpu"] = extra_sharded(torch, AB, dev, stream, rank, world)
     if not args.skip_extras:
         # ---- every mixed configuration (iterations, time, backward error)
         mixed = {}
