@@ -73,6 +73,17 @@ _SIGS = {
     "atlb_dpotrf_dev": (_I, [_I, _I, _P, _I, _P]),
     "atlb_dpotrs_dev": (_I, [_I, _I, _I, _P, _I, _P, _I]),
     "atlb_dgeqrf_dev": (_I, [_I, _I, _P, _I, _P]),
+    "atlb_dormqr_dev": (_I, [_I, _I, _I, _I, _I, _P, _I, _P, _P, _I]),
+    "cblas_dsymm": (None, [_I, _I, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I]),
+    "cblas_dsyr2k": (None, [_I, _I, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I]),
+    "cblas_zgemm": (None, [_I, _I, _I, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I]),
+    "clapack_dgetri": (_I, [_I, _I, _P, _I, _P]),
+    "clapack_dpotri": (_I, [_I, _I, _I, _P, _I]),
+    "clapack_dlauum": (_I, [_I, _I, _I, _P, _I]),
+    "clapack_dtrtri": (_I, [_I, _I, _I, _I, _P, _I]),
+    "clapack_dgels": (_I, [_I, _I, _I, _I, _I, _P, _I, _P, _I]),
+    "clapack_dgelqf": (_I, [_I, _I, _I, _P, _I, _P]),
+    "ATL_dormqr": (_I, [_I, _I, _I, _I, _I, _P, _I, _P, _P, _I, _P, _I]),
     "atlb_dgemm_ozaki_dev": (_I, [_I, _I, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I, _I]),
     "atlb_dgemm_ozaki": (_I, [_I, _I, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I, _I]),
     "atlb_dsgesv": (_I, [_I, _I, _P, _I, _P, _P, _I, _P, _I, _I, _P]),
@@ -86,6 +97,13 @@ _SIGS = {
     "atlb_dgetrf_adjoint_dev": (_I, [_I, _P, _I, _P, _P, _I, _P, _I, _P, _I]),
     "atlb_dsposv": (_I, [_I, _I, _I, _P, _I, _P, _I, _P, _I, _I, _P]),
 }
+# Fortran 77 entry points: every argument by address
+for _f, _n in (("dgemm_", 13), ("sgemm_", 13), ("zgemm_", 13), ("dtrsm_", 11), ("dtrmm_", 11),
+               ("dsyrk_", 10), ("dsymm_", 12), ("dsyr2k_", 12), ("dgetrf_", 6), ("dgetrs_", 9),
+               ("dgesv_", 8), ("dgetri_", 7), ("dpotrf_", 5), ("dpotrs_", 8), ("dposv_", 8),
+               ("dpotri_", 5), ("dtrtri_", 6), ("dlauum_", 5), ("dgeqrf_", 8), ("dgelqf_", 8),
+               ("dgels_", 11)):
+    _SIGS[_f] = (None, [_P] * _n)
 
 
 def lib():

@@ -30,6 +30,8 @@ __global__ void reflect_upper_kernel(int n, double *C, long ldc) {
   }
 }
 
+}  // namespace
+
 __global__ void transpose_kernel(int rows, int cols, const double *S, long lds, double *D,
                                  long ldd) {
   __shared__ double t[32][33];
@@ -50,6 +52,8 @@ void transpose_dev(int rows, int cols, const double *S, long lds, double *D, lon
   transpose_kernel<<<grid, block, 0, st>>>(rows, cols, S, lds, D, ldd);
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
+
+namespace {
 
 inline bool bad_trans(int t) { return t != kNoTrans && t != kTrans && t != kConjTrans; }
 

@@ -118,6 +118,14 @@ void potrs_dev(int uplo, int N, int NRHS, const T *A, long lda, T *B, long ldb, 
 
 // Householder QR (ATLAS conventions: tau in [1,2], beta = -sign(alpha)*norm).
 void dgeqrf_dev(int M, int N, double *A, long lda, double *tau, cudaStream_t st);
+// C = op(Q) C (side kLeft, Q of order M) or C op(Q) (kRight, order N), Q from
+// dgeqrf_dev's K reflectors in A and tau (ATL_ormqr).
+void dormqr_dev(int side, int trans, int M, int N, int K, const double *A, long lda, const double *tau,
+                double *C, long ldc, cudaStream_t st);
+// D (cols x rows) = S^T
+void transpose_dev(int rows, int cols, const double *S, long lds, double *D, long ldd, cudaStream_t st);
+// F = A with the triangle `uplo` mirrored into the other one (full symmetric copy)
+void symmetrize_dev(int uplo, int N, const double *A, long lda, double *F, long ldf, cudaStream_t st);
 
 // Small utilities
 void set_info_kernel_launch(int *dinfo, cudaStream_t st);       // *dinfo = INT_MAX

@@ -329,7 +329,53 @@ void build_vt(int m, int k, const double *P, long ldp, const double *tau, double
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
 
+// Apply the block reflector H = I - V T V^T (V explicit, len x k) or its
+// transpose to C: from the left (C is len x n) or the right (C is m x len).
+void larfb_gen(int side, int trans, int len, int other, int k, const double *V, const double *T, double *C,
+               long ldc, double *W, cudaStream_t st) {
+  if (len <= 0 || other <= 0 || k <= 0) return;
+  const int tt = trans == kNoTrans ? kNoTrans : kTrans;  // H^T = I - V T^T V^T
+  if (side == kLeft) {  // C (len x other) -= V op(T) V^T C
+    double *W1 = W, *W2 = W + (size_t)k * other;
+    dgemm_dev(kTrans, kNoTrans, k, other, len, 1.0, V, len, C, ldc, 0.0, W1, k, st);
+    dgemm_dev(tt, kNoTrans, k, other, k, 1.0, T, k, W1, k, 0.0, W2, k, st);
+    dgemm_dev(kNoTrans, kNoTrans, len, other, k, -1.0, V, len, W2, k, 1.0, C, ldc, st);
+  } else {              // C (other x len) -= C V op(T) V^T
+    double *W1 = W, *W2 = W + (size_t)other * k;
+    dgemm_dev(kNoTrans, kNoTrans, other, k, len, 1.0, C, ldc, V, len, 0.0, W1, other, st);
+    dgemm_dev(kNoTrans, tt, other, k, k, 1.0, W1, other, T, k, 0.0, W2, other, st);
+    dgemm_dev(kNoTrans, kTrans, other, len, k, -1.0, W2, other, V, len, 1.0, C, ldc, st);
+  }
+}
+
 }  // namespace
+
+// Q = H(0) H(1) ... H(K-1) from dgeqrf_dev's reflectors (columns of A below
+// the diagonal, tau) applied to C (M x N): Q C, Q^T C (Left; Q of order M) or
+// C Q, C Q^T (Right; Q of order N).  ATL_ormqr's operation
+// (src/lapack/ATL_ormqr.c:24), blocked: NBQ reflectors at a time as one block
+// reflector I - V T V^T (T from the Gram matrix V^T V, as in the
+// factorization), applied with three GEMMs.
+void dormqr_dev(int side, int trans, int M, int N, int K, const double *A, long lda, const double *tau,
+                double *C, long ldc, cudaStream_t st) {
+  if (M <= 0 || N <= 0 || K <= 0) return;
+  const int nq = side == kLeft ? M : N;   // order of Q
+  const int other = side == kLeft ? N : M;
+  size_t need = (size_t)nq * NBQ + 2 * (size_t)NBQ * NBQ + 2 * (size_t)NBQ * other;
+  double *ws = (double *)scratch(kSlotQrApply, sizeof(double) * need);
+  double *V = ws, *G = V + (size_t)nq * NBQ, *T = G + (size_t)NBQ * NBQ, *W = T + (size_t)NBQ * NBQ;
+  const int nblk = cdiv(K, NBQ);
+  // Q C = H0 (H1 (... C)): last block first; Q^T C: first block first (Left).
+  // C Q = ((C H0) H1) ...: first block first; C Q^T: last block first (Right).
+  const bool forward = (side == kLeft) == (trans != kNoTrans);
+  for (int t = 0; t < nblk; t++) {
+    const int b = forward ? t : nblk - 1 - t;
+    const int j = b * NBQ, kb = std::min(NBQ, K - j), len = nq - j;
+    build_vt(len, kb, A + j + (long)j * lda, lda, tau + j, V, G, T, st);
+    if (side == kLeft) larfb_gen(kLeft, trans, len, other, kb, V, T, C + j, ldc, W, st);
+    else larfb_gen(kRight, trans, len, other, kb, V, T, C + (long)j * ldc, ldc, W, st);
+  }
+}
 
 void dgeqrf_dev(int M, int N, double *A, long lda, double *tau, cudaStream_t st) {
   const int mn = std::min(M, N);

@@ -85,6 +85,90 @@ int clapack_dgeqrf(const enum CBLAS_ORDER Order, const int M, const int N, doubl
 int ATL_dgeqrf(const int M, const int N, double *A, const int lda, double *TAU, double *WORK,
                const int LWORK);
 
+/* cblas_dsymm: include/cblas.h, interfaces/blas/C/src/cblas_dsymm.c */
+void cblas_dsymm(const enum CBLAS_ORDER Order, const enum CBLAS_SIDE Side, const enum CBLAS_UPLO Uplo,
+                 const int M, const int N, const double alpha, const double *A, const int lda,
+                 const double *B, const int ldb, const double beta, double *C, const int ldc);
+/* cblas_dsyr2k: include/cblas.h, interfaces/blas/C/src/cblas_dsyr2k.c */
+void cblas_dsyr2k(const enum CBLAS_ORDER Order, const enum CBLAS_UPLO Uplo, const enum CBLAS_TRANSPOSE Trans,
+                  const int N, const int K, const double alpha, const double *A, const int lda,
+                  const double *B, const int ldb, const double beta, double *C, const int ldc);
+/* cblas_zgemm: include/cblas.h, interfaces/blas/C/src/cblas_zgemm.c (complex
+ * double, interleaved; alpha and beta point to two doubles) */
+void cblas_zgemm(const enum CBLAS_ORDER Order, const enum CBLAS_TRANSPOSE TransA,
+                 const enum CBLAS_TRANSPOSE TransB, const int M, const int N, const int K, const void *alpha,
+                 const void *A, const int lda, const void *B, const int ldb, const void *beta, void *C,
+                 const int ldc);
+/* clapack_dgetri: include/clapack.h:69, interfaces/lapack/C/src/clapack_dgetri.c */
+int clapack_dgetri(const enum CBLAS_ORDER Order, const int N, double *A, const int lda, const int *ipiv);
+/* clapack_dpotri: include/clapack.h:79, interfaces/lapack/C/src/clapack_dpotri.c */
+int clapack_dpotri(const enum CBLAS_ORDER Order, const enum CBLAS_UPLO Uplo, const int N, double *A,
+                   const int lda);
+/* clapack_dlauum: include/clapack.h:81, interfaces/lapack/C/src/clapack_dlauum.c */
+int clapack_dlauum(const enum CBLAS_ORDER Order, const enum CBLAS_UPLO Uplo, const int N, double *A,
+                   const int lda);
+/* clapack_dtrtri: include/clapack.h:83, interfaces/lapack/C/src/clapack_dtrtri.c */
+int clapack_dtrtri(const enum CBLAS_ORDER Order, const enum CBLAS_UPLO Uplo, const enum CBLAS_DIAG Diag,
+                   const int N, double *A, const int lda);
+/* clapack_dgels: include/clapack.h:86, interfaces/lapack/C/src/clapack_dgels.c */
+int clapack_dgels(const enum CBLAS_ORDER Order, const enum CBLAS_TRANSPOSE TA, const int M, const int N,
+                  const int NRHS, double *A, const int lda, double *B, const int ldb);
+/* clapack_dgelqf: include/clapack.h:90, interfaces/lapack/C/src/clapack_dgelqf.c */
+int clapack_dgelqf(const enum CBLAS_ORDER Order, const int M, const int N, double *A, const int lda,
+                   double *TAU);
+/* ATL_dormqr: src/lapack/ATL_ormqr.c:24-34 (LWORK < 0: workspace query) */
+int ATL_dormqr(const enum CBLAS_SIDE SIDE, const enum CBLAS_TRANSPOSE TRANS, const int M, const int N,
+               const int K, double *A, const int lda, const double *TAU, double *C, const int ldc, double *WORK,
+               const int LWORK);
+
+/* Fortran 77 calling convention (the reference's interfaces/blas/F77/src and
+ * interfaces/lapack/F77/src): every argument by address, characters by their
+ * first letter (hidden string lengths are not read), column-major arrays,
+ * 1-based IPIV in host memory, INFO through its argument; LWORK = -1 is a
+ * workspace query. */
+void dgemm_(const char *transa, const char *transb, const int *m, const int *n, const int *k, const double *alpha,
+            const double *a, const int *lda, const double *b, const int *ldb, const double *beta, double *c,
+            const int *ldc);                                          /* blas/F77/src/dgemm.f */
+void sgemm_(const char *transa, const char *transb, const int *m, const int *n, const int *k, const float *alpha,
+            const float *a, const int *lda, const float *b, const int *ldb, const float *beta, float *c,
+            const int *ldc);                                          /* blas/F77/src/sgemm.f */
+void zgemm_(const char *transa, const char *transb, const int *m, const int *n, const int *k, const double *alpha,
+            const double *a, const int *lda, const double *b, const int *ldb, const double *beta, double *c,
+            const int *ldc);                                          /* blas/F77/src/zgemm.f */
+void dtrsm_(const char *side, const char *uplo, const char *transa, const char *diag, const int *m, const int *n,
+            const double *alpha, const double *a, const int *lda, double *b, const int *ldb);  /* dtrsm.f */
+void dtrmm_(const char *side, const char *uplo, const char *transa, const char *diag, const int *m, const int *n,
+            const double *alpha, const double *a, const int *lda, double *b, const int *ldb);  /* dtrmm.f */
+void dsyrk_(const char *uplo, const char *trans, const int *n, const int *k, const double *alpha, const double *a,
+            const int *lda, const double *beta, double *c, const int *ldc);                   /* dsyrk.f */
+void dsymm_(const char *side, const char *uplo, const int *m, const int *n, const double *alpha, const double *a,
+            const int *lda, const double *b, const int *ldb, const double *beta, double *c,
+            const int *ldc);                                                                  /* dsymm.f */
+void dsyr2k_(const char *uplo, const char *trans, const int *n, const int *k, const double *alpha, const double *a,
+             const int *lda, const double *b, const int *ldb, const double *beta, double *c,
+             const int *ldc);                                                                 /* dsyr2k.f */
+void dgetrf_(const int *m, const int *n, double *a, const int *lda, int *ipiv, int *info);  /* lapack/F77/src/dgetrf.f */
+void dgetrs_(const char *trans, const int *n, const int *nrhs, const double *a, const int *lda, const int *ipiv,
+             double *b, const int *ldb, int *info);                                            /* dgetrs.f */
+void dgesv_(const int *n, const int *nrhs, double *a, const int *lda, int *ipiv, double *b, const int *ldb,
+            int *info);                                                                        /* dgesv.f */
+void dgetri_(const int *n, double *a, const int *lda, const int *ipiv, double *work, const int *lwork,
+             int *info);                                                                       /* dgetri.f */
+void dpotrf_(const char *uplo, const int *n, double *a, const int *lda, int *info);           /* dpotrf.f */
+void dpotrs_(const char *uplo, const int *n, const int *nrhs, const double *a, const int *lda, double *b,
+             const int *ldb, int *info);                                                       /* dpotrs.f */
+void dposv_(const char *uplo, const int *n, const int *nrhs, double *a, const int *lda, double *b, const int *ldb,
+            int *info);                                                                        /* dposv.f */
+void dpotri_(const char *uplo, const int *n, double *a, const int *lda, int *info);           /* dpotri.f */
+void dtrtri_(const char *uplo, const char *diag, const int *n, double *a, const int *lda, int *info); /* dtrtri.f */
+void dlauum_(const char *uplo, const int *n, double *a, const int *lda, int *info);           /* dlauum.f */
+void dgeqrf_(const int *m, const int *n, double *a, const int *lda, double *tau, double *work, const int *lwork,
+             int *info);                                                                       /* dgeqrf.f */
+void dgelqf_(const int *m, const int *n, double *a, const int *lda, double *tau, double *work, const int *lwork,
+             int *info);                                                                       /* dgelqf.f */
+void dgels_(const char *trans, const int *m, const int *n, const int *nrhs, double *a, const int *lda, double *b,
+            const int *ldb, double *work, const int *lwork, int *info);                        /* dgels.f */
+
 /* cblas_xerbla / cblas_errprn: interfaces/blas/C/src/cblas_xerbla.c:13-28,
  * cblas_errprn.c (error reporting of the drop-in entry points) */
 void cblas_xerbla(int p, const char *rout, const char *form, ...);
@@ -164,6 +248,10 @@ int atlb_dgetrs_dev(int Trans, int N, int NRHS, const double *A, int lda, const 
 int atlb_dpotrf_dev(int Uplo, int N, double *A, int lda, int *dinfo);
 int atlb_dpotrs_dev(int Uplo, int N, int NRHS, const double *A, int lda, double *B, int ldb);
 int atlb_dgeqrf_dev(int M, int N, double *A, int lda, double *tau);
+/* C = op(Q) C (Side Left) or C op(Q) (Right), Q from atlb_dgeqrf_dev's K
+ * reflectors (device pointers, asynchronous; ATL_ormqr's operation). */
+int atlb_dormqr_dev(int Side, int Trans, int M, int N, int K, const double *A, int lda, const double *tau,
+                    double *C, int ldc);
 
 /* Mixed-precision solvers (no counterpart in the reference; LAPACK's
  * dsgesv/dsposv contract).  Factor an FP32 copy of A on the GPU -- trailing
