@@ -179,11 +179,11 @@ def test_dgels(gpu, order, trans, m, n):
     b = r.uniform(-1, 1, (rows_b, nrhs))
     x_ref = np.linalg.lstsq(op, b, rcond=None)[0]  # least squares or minimum norm
     A, lda = _store(a, order)
-    bb = np.zeros((max(m, n), nrhs))
-    bb[:rows_b] = b
-    B, ldb = _store(bb, order)
-    assert AB.clapack_dgels(order, trans, m, n, nrhs, A, lda, B, ldb) == 0
-    x = _logical(B, order)[:cols_x]
+    # B is column-major in either order, as the reference's clapack_dgels takes it
+    B = np.zeros((max(m, n), nrhs), order="F")
+    B[:rows_b] = b
+    assert AB.clapack_dgels(order, trans, m, n, nrhs, A, lda, B, max(m, n)) == 0
+    x = B[:cols_x]
     assert _rel(x, x_ref) < 1e-10
 
 
