@@ -96,6 +96,8 @@ _SIGS = {
     "atlb_dgetrs_adjoint_dev": (_I, [_I, _I, _P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I]),
     "atlb_dgetrf_adjoint_dev": (_I, [_I, _P, _I, _P, _P, _I, _P, _I, _P, _I]),
     "atlb_dsposv": (_I, [_I, _I, _I, _P, _I, _P, _I, _P, _I, _I, _P]),
+    "atlb_dpotrf_adjoint_batched_dev": (_I, [_I, _P, _P, _P, _P, _P, _P, _P]),
+    "atlb_dpotrs_adjoint_batched_dev": (_I, [_I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
 }
 # Fortran 77 entry points: every argument by address
 for _f, _n in (("dgemm_", 13), ("sgemm_", 13), ("zgemm_", 13), ("dtrsm_", 11), ("dtrmm_", 11),

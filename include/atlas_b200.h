@@ -329,6 +329,19 @@ int atlb_dpotrs_adjoint_dev(int N, int NRHS, const double *L, int ldl, const dou
 int atlb_dgetrs_adjoint_dev(int N, int NRHS, const double *LU, int ldlu, const int *ipiv,
                             const double *X, int ldx, const double *Xbar, int ldxb, double *Bbar,
                             int ldbb, double *Abar, int ldab);
+/* Batched adjoints (no counterpart in the reference): the potrf and potrs
+ * adjoints above for `count` independent problems of order n[i] <= 256 in one
+ * persistent launch each.  The arrays of device pointers and sizes are host
+ * memory, copied before the call returns; the work itself is asynchronous on
+ * the library stream.  Return -2 .. -13: the first bad argument position of
+ * any problem. */
+int atlb_dpotrf_adjoint_batched_dev(int count, const int *n, const double *const *L, const int *ldl,
+                                    const double *const *Lbar, const int *ldlb, double *const *Abar,
+                                    const int *ldab);
+int atlb_dpotrs_adjoint_batched_dev(int count, const int *n, const int *nrhs, const double *const *L,
+                                    const int *ldl, const double *const *X, const int *ldx,
+                                    const double *const *Xbar, const int *ldxb, double *const *Bbar,
+                                    const int *ldbb, double *const *Abar, const int *ldab);
 int atlb_dgetrf_adjoint_dev(int N, const double *LU, int ldlu, const int *ipiv, const double *Lbar,
                             int ldlb, const double *Ubar, int ldub, double *Abar, int ldab);
 

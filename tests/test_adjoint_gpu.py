@@ -90,21 +90,90 @@ def test_potrf_potrs_adjoint(gpu, n):
         assert abs(fd - an) <= 1e-5 * max(1.0, abs(an)), (k, fd, an)
 
 
-def test_potrf_adjoint_batched_small(gpu):
-    # the batched variant of the loss: many systems at N=128 through the same kernels
+def _ptrs(np_, ts):
+    return np_.array([t.data_ptr() for t in ts], dtype=np_.uint64)
+
+
+def test_potrf_potrs_adjoint_batched_512x128(gpu):
+    """The Gaussian-likelihood loss of 512 systems at N = 128, its gradient in
+    two one-launch batched adjoints (potrf, then potrs) through the C ABI,
+    against the closed form A^-1 - a a^T of every system."""
     import torch
+    count, n = 512, 128
     g = torch.Generator(device="cuda")
     g.manual_seed(5)
-    Fn = make_gauss_fn(torch)
-    for k in range(32):
-        n = 128
+    As, Ls, Ys, Xs = [], [], [], []
+    for _ in range(count):
         B = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g)
-        A = (B @ B.T / n + torch.eye(n, dtype=torch.float64, device="cuda")).requires_grad_(True)
-        y = torch.rand(n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
-        Fn.apply(A, y).backward()
-        Ainv = torch.linalg.inv(A.detach())
-        a = Ainv @ y
-        assert torch.allclose(A.grad, Ainv - torch.outer(a, a), rtol=1e-9, atol=1e-11)
+        A = B @ B.T / n + torch.eye(n, dtype=torch.float64, device="cuda")
+        As.append(A)
+        Ls.append(A.clone())
+        y = torch.rand(1, n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+        Ys.append(y)
+        Xs.append(y.clone())
+    nv = np.full(count, n, np.int32)
+    info = np.zeros(count, np.int32)
+    # forward: L (lower) and x = A^-1 y for every system in one launch
+    assert AB.atlb_dposv_batched(count, nv, _ptrs(np, Ls), nv, _ptrs(np, Xs), nv, np.ones(count, np.int32),
+                                 info) == 0
+    assert np.all(info == 0)
+    Lbars, Abars, Bbars = [], [], []
+    for L in Ls:
+        Lc = L.T   # logical column-major factor
+        Lbars.append(torch.diag(2.0 / torch.diagonal(Lc)).T.contiguous())
+        Abars.append(torch.zeros(n, n, dtype=torch.float64, device="cuda"))
+        Bbars.append(torch.zeros(1, n, dtype=torch.float64, device="cuda"))
+    assert AB.atlb_dpotrf_adjoint_batched_dev(count, nv, _ptrs(np, Ls), nv, _ptrs(np, Lbars), nv,
+                                              _ptrs(np, Abars), nv) == 0
+    assert AB.atlb_dpotrs_adjoint_batched_dev(count, nv, np.ones(count, np.int32), _ptrs(np, Ls), nv,
+                                              _ptrs(np, Xs), nv, _ptrs(np, Ys), nv, _ptrs(np, Bbars), nv,
+                                              _ptrs(np, Abars), nv) == 0
+    assert AB.atlb_sync() == 0
+    worst = 0.0
+    for k in range(count):
+        Ainv = torch.linalg.inv(As[k])
+        a = Ainv @ Ys[k][0]
+        closed = Ainv - torch.outer(a, a)
+        worst = max(worst, ((Abars[k].T - closed).abs().max() / closed.abs().max()).item())
+        if k < 8:  # the same numbers as the unbatched kernels
+            Ab1 = torch.zeros(n, n, dtype=torch.float64, device="cuda")
+            Bb1 = torch.zeros(1, n, dtype=torch.float64, device="cuda")
+            assert AB.atlb_dpotrf_adjoint_dev(n, Ls[k], n, Lbars[k], n, Ab1, n) == 0
+            assert AB.atlb_dpotrs_adjoint_dev(n, 1, Ls[k], n, Xs[k], n, Ys[k], n, Bb1, n, Ab1, n) == 0
+            assert AB.atlb_sync() == 0
+            assert torch.allclose(Ab1, Abars[k], rtol=1e-10, atol=1e-12)
+    assert worst < 1e-10, worst
+
+
+def test_potrf_potrs_adjoint_4096_fd_64_directions(gpu):
+    """The benchmark configuration: N = 4096, A = B B^T / N + I, y uniform[-1,1];
+    the gradient against the closed form and central finite differences
+    (step 1e-6) on 64 random symmetric directions."""
+    import torch
+    n = 4096
+    g = torch.Generator(device="cuda")
+    g.manual_seed(4096)
+    B = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g)
+    A = (B @ B.T / n + torch.eye(n, dtype=torch.float64, device="cuda")).requires_grad_(True)
+    del B
+    y = torch.rand(n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    make_gauss_fn(torch).apply(A, y).backward()
+    grad = A.grad
+    Ad = A.detach()
+    Ainv = torch.linalg.inv(Ad)
+    a = Ainv @ y
+    closed = Ainv - torch.outer(a, a)
+    assert ((grad - closed).abs().max() / closed.abs().max()).item() < 1e-9
+    del Ainv, closed
+    h = 1e-6
+    for k in range(64):
+        E = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g)
+        E = (E + E.T) / 2
+        E /= E.norm()
+        fp = gauss_loss_forward(torch, Ad + h * E, y)[0].item()
+        fm = gauss_loss_forward(torch, Ad - h * E, y)[0].item()
+        an = torch.sum(grad * E).item()
+        assert abs((fp - fm) / (2 * h) - an) <= 1e-5 * max(1.0, abs(an)), (k, (fp - fm) / (2 * h), an)
 
 
 def _lu(torch, Acol, n):
@@ -116,11 +185,14 @@ def _lu(torch, Acol, n):
     return LU, ipiv
 
 
-@pytest.mark.parametrize("n", [300])
+@pytest.mark.parametrize("n", [300, 4096])
 def test_getrs_adjoint_closed_form_and_fd(gpu, n):
+    """L(A) = c^T A^-1 b (A = G/sqrt(n) + 4I; n = 4096 is the benchmark
+    configuration): the getrs adjoint against the closed form -A^-T c (A^-1 b)^T
+    and central finite differences."""
     import torch
     a0 = O.lu_matrix(n, 21)
-    Acol = torch.tensor(a0.T.copy(), device="cuda")          # storage of column-major a0
+    Acol = torch.tensor(np.ascontiguousarray(a0.T), device="cuda")  # storage of column-major a0
     rng = np.random.default_rng(3)
     b = torch.tensor(rng.uniform(-1, 1, n), device="cuda")
     c = torch.tensor(rng.uniform(-1, 1, n), device="cuda")

@@ -24,10 +24,8 @@ def _rng(s):
 def _store(a, order):
     """(buffer, ld) holding the logical matrix a in the given storage order."""
     if order == CM:
-        b = np.asfortranarray(a)
-        return b, max(1, a.shape[0])
-    b = np.ascontiguousarray(a)
-    return b, max(1, a.shape[1])
+        return np.array(a, order="F", copy=True), max(1, a.shape[0])
+    return np.array(a, order="C", copy=True), max(1, a.shape[1])
 
 
 def _logical(buf, order):
