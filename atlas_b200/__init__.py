@@ -91,6 +91,7 @@ _SIGS = {
     "atlb_dgemm_batched_dev": (_I, [_I, _I, _I, _P, _P, _P, _D, _P, _P, _P, _P, _D, _P, _P]),
     "atlb_dposv_batched": (_I, [_I, _P, _P, _P, _P, _P, _P, _P]),
     "atlb_dgesv_batched": (_I, [_I, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "atlb_dgetrf_batched": (_I, [_I, _P, _P, _P, _P, _P]),
     "atlb_dpotrf_adjoint_dev": (_I, [_I, _P, _I, _P, _I, _P, _I]),
     "atlb_dpotrs_adjoint_dev": (_I, [_I, _I, _P, _I, _P, _I, _P, _I, _P, _I, _P, _I]),
     "atlb_dgetrs_adjoint_dev": (_I, [_I, _I, _P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I]),

@@ -25,9 +25,10 @@ namespace atlb {
 namespace {
 
 constexpr int BT = 256;       // threads per CTA
-constexpr int SMALL = 96;     // whole-matrix-in-shared-memory bound
-constexpr int PW = 32;        // panel width for larger matrices
 constexpr int MAXN = 256;
+// Size buckets (tunable, tuning.cu): orders up to batch_posv_small (Cholesky)
+// / batch_getrf_smem (LU) are factored whole in shared memory, larger ones in
+// panels of batch_posv_pw columns.
 
 struct Prob {
   double *A;
@@ -38,28 +39,84 @@ struct Prob {
 
 // ---------------------------------------------------------------- Cholesky
 
-// unblocked right-looking Cholesky of an n x n lower matrix in shared memory
-// (ld = lds); returns 0 or the first non-positive pivot (1-based)
-__device__ int chol_smem(double *s, int lds, int n, int *sfail) {
+// C (lower part of rows/cols r0.., order mt) -= P P^T, P = the mt x jb block
+// of the panel at (rows r0..) in shared memory (ld lds); C in shared memory
+// (ldc, offset c0) or global.  16 x 16 threads, 4 x 4 register tiles over
+// 64 x 64 blocks of the lower triangle.
+template <typename CT>
+__device__ __forceinline__ void syrk_lower_update(int mt, int jb, const double *P, int lds, CT *C, long ldc) {
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  for (int ib = 0; ib < mt; ib += 64)
+    for (int kb = 0; kb <= ib; kb += 64) {
+      double acc[4][4];
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+      for (int q = 0; q < jb; q++) {
+        double pi[4], pk[4];
+#pragma unroll
+        for (int a = 0; a < 4; a++) {
+          const int i = ib + tx + 16 * a;
+          pi[a] = i < mt ? P[i + q * lds] : 0.0;
+        }
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+          const int k = kb + ty + 16 * b;
+          pk[b] = k < mt ? P[k + q * lds] : 0.0;
+        }
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+          for (int b = 0; b < 4; b++) acc[a][b] = fma(pi[a], pk[b], acc[a][b]);
+      }
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+          const int i = ib + tx + 16 * a, k = kb + ty + 16 * b;
+          if (i < mt && k <= i) C[i + (long)k * ldc] -= acc[a][b];
+        }
+    }
+}
+
+// Cholesky of the jb columns of the m x jb panel at s (ld lds, rows from the
+// panel's diagonal): unblocked within the panel (one row per thread).
+// Returns 0 or the first non-positive pivot (1-based, panel-relative).
+__device__ int chol_panel(double *s, int lds, int m, int jb, int *sfail) {
   const int tid = threadIdx.x;
-  for (int j = 0; j < n; j++) {
-    const double d = s[j + j * lds];
+  for (int c = 0; c < jb; c++) {
+    const double d = s[c + c * lds];
     if (!(d > 0.0)) {
-      if (tid == 0) *sfail = j + 1;
+      if (tid == 0) *sfail = c + 1;
       __syncthreads();
-      return j + 1;
+      return c + 1;
     }
-    const double r = sqrt(d);
-    __syncthreads();
-    if (tid == 0) s[j + j * lds] = r;
-    const double ri = 1.0 / r;
-    for (int i = j + 1 + tid; i < n; i += BT) s[i + j * lds] *= ri;
-    __syncthreads();
-    const int m = n - j - 1;
-    for (int idx = tid; idx < m * m; idx += BT) {
-      const int i = j + 1 + idx % m, k = j + 1 + idx / m;
-      if (k <= i) s[i + k * lds] = fma(-s[i + j * lds], s[k + j * lds], s[i + k * lds]);
+    const double ri = 1.0 / sqrt(d);
+    __syncthreads();  // every thread has read the pivot
+    for (int i = c + tid; i < m; i += BT) s[i + c * lds] = i == c ? d * ri : s[i + c * lds] * ri;
+    __syncthreads();  // column c holds the multipliers
+    for (int i = c + 1 + tid; i < m; i += BT) {  // the panel's columns right of c, row by row
+      const double l = s[i + c * lds];
+      const int kmax = min(jb - 1, i);
+      for (int k = c + 1; k <= kmax; k++) s[i + k * lds] = fma(-l, s[k + c * lds], s[i + k * lds]);
     }
+    __syncthreads();
+  }
+  return 0;
+}
+
+// blocked right-looking Cholesky of an n x n lower matrix in shared memory
+// (ld = lds): 16-column panels factored in place, the trailing lower triangle
+// updated with register tiles; returns 0 or the first non-positive pivot
+// (1-based)
+__device__ int chol_smem(double *s, int lds, int n, int *sfail) {
+  for (int j = 0; j < n; j += 16) {
+    const int jb = min(16, n - j), m = n - j;
+    double *P = s + j + j * lds;
+    const int f = chol_panel(P, lds, m, jb, sfail);
+    if (f) return j + f;
+    if (m > jb) syrk_lower_update(m - jb, jb, P + jb, lds, P + jb + jb * lds, lds);
     __syncthreads();
   }
   return 0;
@@ -90,7 +147,7 @@ __device__ void chol_solve(const double *L, int ldl, int n, double *B, int ldb, 
 
 __global__ void __launch_bounds__(BT)
 batched_posv_kernel(const Prob *__restrict__ probs, const int *__restrict__ order, int count,
-                    int *__restrict__ next, int *__restrict__ info) {
+                    int *__restrict__ next, int *__restrict__ info, int SMALL, int PW) {
   extern __shared__ __align__(16) double sm[];
   __shared__ int s_p, s_fail;
   const int tid = threadIdx.x;
@@ -125,21 +182,9 @@ batched_posv_kernel(const Prob *__restrict__ probs, const int *__restrict__ orde
         for (int idx = tid; idx < m * jb; idx += BT)
           sm[idx % m + (idx / m) * lds] = pr.A[j + idx % m + (long)(j + idx / m) * pr.lda];
         __syncthreads();
-        // unblocked on the m x jb panel: diagonal block and the rows below
-        for (int c = 0; c < jb; c++) {
-          const double d = sm[c + c * lds];
-          if (!(d > 0.0)) { fail = j + c + 1; break; }
-          const double r = sqrt(d);
-          __syncthreads();
-          if (tid == 0) sm[c + c * lds] = r;
-          const double ri = 1.0 / r;
-          for (int i = c + 1 + tid; i < m; i += BT) sm[i + c * lds] *= ri;
-          __syncthreads();
-          for (int idx = tid; idx < (m - c - 1) * (jb - c - 1); idx += BT) {
-            const int i = c + 1 + idx % (m - c - 1), k = c + 1 + idx / (m - c - 1);
-            if (k <= i) sm[i + k * lds] = fma(-sm[i + c * lds], sm[k + c * lds], sm[i + k * lds]);
-          }
-          __syncthreads();
+        {
+          const int f = chol_panel(sm, lds, m, jb, &s_fail);
+          if (f) fail = j + f;
         }
         for (int idx = tid; idx < m * jb; idx += BT) {
           const int i = idx % m, k = idx / m;
@@ -147,15 +192,7 @@ batched_posv_kernel(const Prob *__restrict__ probs, const int *__restrict__ orde
         }
         if (fail) break;
         // trailing update: A[j+jb.., j+jb..] -= P2 P2^T (lower), P2 = panel rows jb..m
-        const int mt = m - jb;
-        for (int idx = tid; idx < mt * mt; idx += BT) {
-          const int i = idx % mt, k = idx / mt;
-          if (k > i) continue;
-          double acc = 0.0;
-          for (int q = 0; q < jb; q++) acc = fma(sm[jb + i + q * lds], sm[jb + k + q * lds], acc);
-          double *a = pr.A + (j + jb + i) + (long)(j + jb + k) * pr.lda;
-          *a -= acc;
-        }
+        if (m > jb) syrk_lower_update(m - jb, jb, sm + jb, lds, pr.A + (j + jb) + (long)(j + jb) * pr.lda, pr.lda);
         __syncthreads();
       }
       __syncthreads();
@@ -209,10 +246,11 @@ __device__ int lu_smem(double *s, int lds, int n, int *ipiv, double *wv, int *wi
       const bool use_r = fabs(piv) >= DBL_MIN;
       for (int i = j + 1 + tid; i < n; i += BT) s[i + j * lds] = use_r ? s[i + j * lds] * r : s[i + j * lds] / piv;
       __syncthreads();
-      const int m = n - j - 1;
-      for (int idx = tid; idx < m * m; idx += BT) {
-        const int i = j + 1 + idx % m, k = j + 1 + idx / m;
-        s[i + k * lds] = fma(-s[i + j * lds], s[j + k * lds], s[i + k * lds]);
+      // rank-1 update: 16 x 16 threads, rows tx + 16 a, columns ty + 16 b
+      const int tx = tid % 16, ty = tid / 16;
+      for (int k = j + 1 + ty; k < n; k += 16) {
+        const double u = s[j + k * lds];
+        for (int i = j + 1 + tx; i < n; i += 16) s[i + k * lds] = fma(-s[i + j * lds], u, s[i + k * lds]);
       }
     }
     __syncthreads();
@@ -303,9 +341,14 @@ batched_getrs_kernel(const Prob *__restrict__ probs, const int *__restrict__ ord
 struct BatchBufs {
   Prob *probs;
   int *order, *next, *info;
+  unsigned char *h, *d;  // pinned staging copy of the problem list, its device copy
+  size_t bytes;          // bytes the upload copies
 };
 
-BatchBufs upload(const std::vector<Prob> &P, cudaStream_t st, int slot_p) {
+// The problem list, sorted by decreasing order, written into the pinned
+// staging buffer (host side, every call); enqueue_upload() copies it to the
+// device on the stream (a node of the captured graph on replays).
+BatchBufs prepare(const std::vector<Prob> &P, int slot_p) {
   const int count = (int)P.size();
   std::vector<int> order(count);
   for (int i = 0; i < count; i++) order[i] = i;
@@ -316,13 +359,19 @@ BatchBufs upload(const std::vector<Prob> &P, cudaStream_t st, int slot_p) {
   memcpy(h, P.data(), sizeof(Prob) * count);
   memcpy(h + sizeof(Prob) * count, order.data(), sizeof(int) * count);
   memset(h + sizeof(Prob) * count + sizeof(int) * count, 0, sizeof(int) * 64);
-  ATLB_CUDA_CHECK(cudaMemcpyAsync(d, h, bytes - sizeof(int) * count, cudaMemcpyHostToDevice, st));
   BatchBufs b;
   b.probs = (Prob *)d;
   b.order = (int *)(d + sizeof(Prob) * count);
   b.next = b.order + count;
   b.info = b.next + 64;
+  b.h = h;
+  b.d = d;
+  b.bytes = bytes - sizeof(int) * count;
   return b;
+}
+
+void enqueue_upload(const BatchBufs &b, cudaStream_t st) {
+  ATLB_CUDA_CHECK(cudaMemcpyAsync(b.d, b.h, b.bytes, cudaMemcpyHostToDevice, st));
 }
 
 int grid_size(size_t smem) {
@@ -332,12 +381,17 @@ int grid_size(size_t smem) {
 
 }  // namespace
 
+// One batched Cholesky + solve: upload, one persistent launch, info back to
+// info_out (pinned).  The launch sequence depends only on the batch's shape
+// and the buffers, so it is replayed from a CUDA graph from the third call on
+// (run_graph): the problem list itself travels in the captured copy.
 void batched_posv_dev(const std::vector<Prob> &P, int *info_out, cudaStream_t st) {
   const int count = (int)P.size();
   if (!count) return;
-  BatchBufs b = upload(P, st, kSlotBatch0);
+  BatchBufs b = prepare(P, kSlotBatch0);
   int maxn = 0;
   for (auto &p : P) maxn = std::max(maxn, p.n);
+  const int SMALL = tune(kTuneBatchPosvSmall), PW = tune(kTuneBatchPosvPW);
   const int sn = std::min(maxn, SMALL);
   const size_t sm_bytes = std::max(sizeof(double) * sn * (sn + 1),
                                    maxn > SMALL ? sizeof(double) * (size_t)(maxn + 1) * PW : (size_t)0);
@@ -346,9 +400,48 @@ void batched_posv_dev(const std::vector<Prob> &P, int *info_out, cudaStream_t st
     ATLB_CUDA_CHECK(cudaFuncSetAttribute(batched_posv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     configured = true;
   }
-  batched_posv_kernel<<<grid_size(sm_bytes), BT, sm_bytes, st>>>(b.probs, b.order, count, b.next, b.info);
-  ATLB_CUDA_CHECK(cudaGetLastError());
-  ATLB_CUDA_CHECK(cudaMemcpyAsync(info_out, b.info, sizeof(int) * count, cudaMemcpyDeviceToHost, st));
+  const std::vector<unsigned long long> key = {0xBA7C0001ull, (unsigned long long)tune_generation(),
+      (unsigned long long)count, (unsigned long long)maxn, (unsigned long long)(uintptr_t)b.d,
+      (unsigned long long)(uintptr_t)b.h, (unsigned long long)(uintptr_t)info_out,
+      (unsigned long long)(uintptr_t)st};
+  run_graph(key, st, [&]() {
+    enqueue_upload(b, st);
+    batched_posv_kernel<<<grid_size(sm_bytes), BT, sm_bytes, st>>>(b.probs, b.order, count, b.next, b.info, SMALL,
+                                                                    PW);
+    ATLB_CUDA_CHECK(cudaGetLastError());
+    ATLB_CUDA_CHECK(cudaMemcpyAsync(info_out, b.info, sizeof(int) * count, cudaMemcpyDeviceToHost, st));
+  });
+}
+
+// Batched LU (+ the solve when nrhs > 0 for the problems), the same way.
+void batched_gesv_dev(const std::vector<Prob> &P, bool solve, int *info_out, cudaStream_t st) {
+  const int count = (int)P.size();
+  if (!count) return;
+  BatchBufs b = prepare(P, kSlotBatch0);
+  int maxn = 0;
+  for (auto &p : P) maxn = std::max(maxn, p.n);
+  static bool configured = false;
+  if (!configured) {
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(batched_getrf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024));
+    configured = true;
+  }
+  const int sm_max = std::min(maxn, tune(kTuneBatchGetrfSmem));  // FP64 in shared memory: 206 KB at 160
+  const size_t smb = sizeof(double) * (size_t)sm_max * (sm_max + 1);
+  const std::vector<unsigned long long> key = {0xBA7C0002ull + (solve ? 1 : 0),
+      (unsigned long long)tune_generation(), (unsigned long long)count, (unsigned long long)maxn,
+      (unsigned long long)(uintptr_t)b.d, (unsigned long long)(uintptr_t)b.h,
+      (unsigned long long)(uintptr_t)info_out, (unsigned long long)(uintptr_t)st};
+  run_graph(key, st, [&]() {
+    enqueue_upload(b, st);
+    batched_getrf_kernel<<<grid_size(smb), BT, smb, st>>>(b.probs, b.order, count, b.next, sm_max, b.info);
+    ATLB_CUDA_CHECK(cudaGetLastError());
+    if (solve) {
+      ATLB_CUDA_CHECK(cudaMemsetAsync(b.next, 0, sizeof(int), st));
+      batched_getrs_kernel<<<num_sms() * 4, BT, 0, st>>>(b.probs, b.order, count, b.next, b.info);
+      ATLB_CUDA_CHECK(cudaGetLastError());
+    }
+    ATLB_CUDA_CHECK(cudaMemcpyAsync(info_out, b.info, sizeof(int) * count, cudaMemcpyDeviceToHost, st));
+  });
 }
 
 }  // namespace atlb
@@ -390,35 +483,24 @@ int atlb_dgesv_batched(int count, const int *n, double *const *A, const int *lda
   if (count < 0) return -1;
   if (count == 0) return 0;
   std::vector<Prob> P(count);
-  int maxn = 0;
   for (int i = 0; i < count; i++) {
     if (n[i] < 0 || n[i] > MAXN) return -2;
     if (lda[i] < std::max(1, n[i])) return -4;
     if (B && (ldb[i] < std::max(1, n[i]) || nrhs[i] < 0)) return -7;
     P[i] = {A[i], B ? B[i] : nullptr, ipiv[i], n[i], lda[i], B ? ldb[i] : 1, B ? nrhs[i] : 0};
-    maxn = std::max(maxn, n[i]);
   }
   cudaStream_t st = stream();
-  BatchBufs b = upload(P, st, kSlotBatch0);
-  static bool configured = false;
-  if (!configured) {
-    ATLB_CUDA_CHECK(cudaFuncSetAttribute(batched_getrf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024));
-    configured = true;
-  }
-  const int sm_max = std::min(maxn, 160);  // orders up to 160 factor in shared memory (FP64: 206 KB)
-  const size_t smb = sizeof(double) * (size_t)sm_max * (sm_max + 1);
-  batched_getrf_kernel<<<grid_size(smb), BT, smb, st>>>(b.probs, b.order, count, b.next, sm_max, b.info);
-  ATLB_CUDA_CHECK(cudaGetLastError());
-  if (B) {
-    ATLB_CUDA_CHECK(cudaMemsetAsync(b.next, 0, sizeof(int), st));
-    batched_getrs_kernel<<<num_sms() * 4, BT, 0, st>>>(b.probs, b.order, count, b.next, b.info);
-    ATLB_CUDA_CHECK(cudaGetLastError());
-  }
   int *hinfo = (int *)pinned(kSlotBatch1, sizeof(int) * count);
-  ATLB_CUDA_CHECK(cudaMemcpyAsync(hinfo, b.info, sizeof(int) * count, cudaMemcpyDeviceToHost, st));
+  batched_gesv_dev(P, B != nullptr, hinfo, st);
   ATLB_CUDA_CHECK(cudaStreamSynchronize(st));
   memcpy(info, hinfo, sizeof(int) * count);
   return 0;
+}
+
+// Batched LU with partial pivoting only (LAPACK getrf semantics per problem:
+// A[i] overwritten by L\U, ipiv[i] 0-based device arrays, info[i] host).
+int atlb_dgetrf_batched(int count, const int *n, double *const *A, const int *lda, int *const *ipiv, int *info) {
+  return atlb_dgesv_batched(count, n, A, lda, ipiv, nullptr, nullptr, nullptr, info);
 }
 
 }  // extern "C"

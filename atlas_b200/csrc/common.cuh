@@ -76,7 +76,8 @@ inline int cdiv(long a, long b) { return (int)((a + b - 1) / b); }
 // Tunable driver parameters (tuning.cu; chosen by atlas_b200/tune.py).
 enum TuneParam {
   kTuneGetrfNB = 0, kTunePotrfNB, kTuneGemmGroup, kTuneSplitK, kTuneLookahead, kTuneTcMinWorkLog2,
-  kTuneLookaheadReserve, kTuneSgetrfNB, kNumTune
+  kTuneLookaheadReserve, kTuneSgetrfNB, kTuneQrNB, kTuneBatchPosvSmall, kTuneBatchPosvPW,
+  kTuneBatchGetrfSmem, kNumTune
 };
 int tune(int p);
 int tune_generation();  // bumps whenever a parameter changes (part of graph keys)

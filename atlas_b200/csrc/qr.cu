@@ -29,7 +29,7 @@ namespace atlb {
 namespace {
 
 constexpr int QT = 512;
-constexpr int NBQ = 128;  // outer panel width (the trailing update's K)
+constexpr int NBQ_MAX = 128;  // largest outer panel width (the trailing update's K)
 
 template <int NB>
 struct QPub {
@@ -322,7 +322,7 @@ void build_vt(int m, int k, const double *P, long ldp, const double *tau, double
   static bool cfg = false;
   if (!cfg) {
     ATLB_CUDA_CHECK(cudaFuncSetAttribute(larft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)(sizeof(double) * NBQ * NBQ)));
+                                         (int)(sizeof(double) * NBQ_MAX * NBQ_MAX)));
     cfg = true;
   }
   larft_kernel<<<1, 256, sm, st>>>(k, G, tau, T);
@@ -359,6 +359,7 @@ void larfb_gen(int side, int trans, int len, int other, int k, const double *V, 
 void dormqr_dev(int side, int trans, int M, int N, int K, const double *A, long lda, const double *tau,
                 double *C, long ldc, cudaStream_t st) {
   if (M <= 0 || N <= 0 || K <= 0) return;
+  const int NBQ = tune(kTuneQrNB);
   const int nq = side == kLeft ? M : N;   // order of Q
   const int other = side == kLeft ? N : M;
   size_t need = (size_t)nq * NBQ + 2 * (size_t)NBQ * NBQ + 2 * (size_t)NBQ * other;
@@ -380,6 +381,7 @@ void dormqr_dev(int side, int trans, int M, int N, int K, const double *A, long 
 void dgeqrf_dev(int M, int N, double *A, long lda, double *tau, cudaStream_t st) {
   const int mn = std::min(M, N);
   if (mn <= 0) return;
+  const int NBQ = tune(kTuneQrNB);  // the outer panel width (ATL_ilaenv's NB, tuned)
   // workspace: V (M x NBQ), G and T (NBQ x NBQ each), W (2 x NBQ x N)
   size_t need = (size_t)M * NBQ + 2 * (size_t)NBQ * NBQ + 2 * (size_t)NBQ * N;
   double *ws = (double *)scratch(kSlotWork, sizeof(double) * need);

@@ -307,6 +307,8 @@ int atlb_dgemm_batched_dev(int TransA, int TransB, int count, const int *M, cons
                            const int *ldc);
 int atlb_dposv_batched(int count, const int *n, double *const *A, const int *lda, double *const *B,
                        const int *ldb, const int *nrhs, int *info);
+/* atlb_dgetrf_batched: the factorization alone (atlb_dgesv_batched with B NULL). */
+int atlb_dgetrf_batched(int count, const int *n, double *const *A, const int *lda, int *const *ipiv, int *info);
 int atlb_dgesv_batched(int count, const int *n, double *const *A, const int *lda, int *const *ipiv,
                        double *const *B, const int *ldb, const int *nrhs, int *info);
 

@@ -109,3 +109,64 @@ def test_batched_dgemm_uneven(gpu, orc):
         c0 = np.asfortranarray(C0[i].cpu().numpy().T)
         c = np.asfortranarray(Cs[i].cpu().numpy().T)
         assert orc.resid_gemm(111, 111, int(M[i]), int(N[i]), int(K[i]), 1.5, a, b, -0.5, c0, c) < 50
+
+
+@pytest.mark.parametrize("small,pw", [(96, 32), (128, 16), (64, 64)])
+def test_batched_posv_buckets_and_graph_replays(gpu, small, pw):
+    """Every size bucket setting of the tuner gives the same solves, and the
+    third and later calls of one batch shape (replayed from a CUDA graph) solve
+    the new data each call carries."""
+    import torch
+    old = (AB.atlb_tune_get("batch_posv_small"), AB.atlb_tune_get("batch_posv_pw"))
+    AB.atlb_tune_set("batch_posv_small", small)
+    AB.atlb_tune_set("batch_posv_pw", pw)
+    try:
+        rng = np.random.default_rng(small + pw)
+        count, nr = 64, 2
+        ns = rng.integers(8, 257, count)
+        ns[:4] = [small, small + 1, 8, 256]
+        for call in range(4):
+            As, Bs, a0s, b0s = [], [], [], []
+            for n in ns:
+                g = rng.standard_normal((n, n))
+                a = g @ g.T + n * np.eye(n)
+                b = rng.uniform(-1, 1, (n, nr))
+                a0s.append(a)
+                b0s.append(b)
+                As.append(torch.tensor(a, device="cuda"))            # symmetric: either order
+                Bs.append(torch.tensor(np.ascontiguousarray(b.T), device="cuda"))
+            info = np.zeros(count, dtype=np.int32)
+            assert AB.atlb_dposv_batched(count, _int_array(ns), _ptr_array(As), _int_array(ns), _ptr_array(Bs),
+                                         _int_array(ns), _int_array([nr] * count), info) == 0
+            assert np.all(info == 0)
+            for i in range(count):
+                x = Bs[i].cpu().numpy().T
+                res = np.abs(a0s[i] @ x - b0s[i]).max() / (np.abs(a0s[i]).sum(1).max() * np.abs(x).max())
+                assert res < 1e-14, (call, i, ns[i], res)
+    finally:
+        AB.atlb_tune_set("batch_posv_small", old[0])
+        AB.atlb_tune_set("batch_posv_pw", old[1])
+
+
+def test_batched_getrf_only_matches_oracle(gpu):
+    import torch
+    rng = np.random.default_rng(21)
+    count = 40
+    ns = rng.integers(8, 257, count)
+    As, Ps, a0s = [], [], []
+    for n in ns:
+        a = O.lu_matrix(int(n), int(n) + 1)
+        a0s.append(a)
+        As.append(torch.tensor(np.ascontiguousarray(a.T), device="cuda"))
+        Ps.append(torch.zeros(int(n), dtype=torch.int32, device="cuda"))
+    info = np.zeros(count, dtype=np.int32)
+    for _ in range(3):  # replays from the graph on the later calls
+        for i, a in enumerate(a0s):
+            As[i].copy_(torch.tensor(np.ascontiguousarray(a.T), device="cuda"))
+        assert AB.atlb_dgetrf_batched(count, _int_array(ns), _ptr_array(As), _int_array(ns), _ptr_array(Ps),
+                                      info) == 0
+        assert np.all(info == 0)
+        for i in range(count):
+            ref, rpiv, _ = O.dgetrf(a0s[i].copy(order="F"))
+            np.testing.assert_array_equal(Ps[i].cpu().numpy(), rpiv)
+            assert np.abs(As[i].cpu().numpy().T - ref).max() < 1e-12
