@@ -235,6 +235,79 @@ def timed(torch, stream, fn, reps):
     return e0.elapsed_time(e1) / reps
 
 
+def measured_traffic(kernel):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) that
+    one ncu capture measured for `kernel`, from the data file kept beside the
+    profile summaries (None when absent)."""
+    path = os.path.join(ROOT, "profiles", "roofline_traffic.txt")
+    try:
+        for line in open(path):
+            if line.startswith("#") or "\t" not in line:
+                continue
+            name, val = line.rstrip("\n").split("\t")[:2]
+            if name == kernel:
+                return int(val)
+    except OSError:
+        pass
+    return None
+
+
+def peak_tf32_tflops():
+    """Dense TF32 tensor peak: half the measured dense BF16 burst rate of this
+    pool's B200s (MEASURED_PEAKS.json; the tensor cores run TF32 at half the
+    BF16 rate), or half the fallback 1.59 PFLOP/s."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)["bf16_tflops"] / 2.0, "half of measured bf16 burst (MEASURED_PEAKS.json)"
+    except (OSError, KeyError, ValueError):
+        return 1590.0 / 2.0, "half of the fallback bf16 1.59 PFLOP/s"
+
+
+def headline_roofline(torch, AB, dev, stream):
+    """Roofline of the headline's tensor-core kernel: the split-TF32 GEMM of the
+    FP32 factorization's first trailing update (M = 7936, N = 7680, K = 256;
+    A and B split into TF32 high and low parts, three products = K 768 on the
+    tensor cores), timed with CUDA events on the library's stream over 10 calls
+    (each call also runs the operand-split kernel).  Algorithmic work per call:
+    2 * M * N * (3 K) TF32 flop.  Beside it, the latency of the FP32 leaf panel
+    (one 8192 x 32 panel through atlb_sgetrf_dev) per column."""
+    f32 = torch.float32
+    M, N, K = 7936, 7680, 256
+    g = torch.Generator(device=dev)
+    g.manual_seed(77)
+    a = torch.rand(K, M, dtype=f32, device=dev, generator=g) - 0.5   # column-major M x K
+    b = torch.rand(N, K, dtype=f32, device=dev, generator=g) - 0.5   # column-major K x N
+    c = torch.rand(N, M, dtype=f32, device=dev, generator=g) - 0.5
+    call = lambda: AB.atlb_sgemm_tc_dev(3, 111, 111, M, N, K, -1.0, a, M, b, K, 1.0, c, M)
+    for _ in range(3):
+        call()
+    ms = timed(torch, stream, call, 10)
+    tflop = 2.0 * M * N * 3 * K / 1e12
+    achieved = tflop / (ms / 1e3)
+    peak, how = peak_tf32_tflops()
+    # the leaf panel: one 8192 x 32 FP32 panel (partial pivoting)
+    pn = 8192
+    p = torch.rand(32, pn, dtype=f32, device=dev, generator=g) - 0.5
+    p0 = p.clone()
+    ip = torch.zeros(32, dtype=torch.int32, device=dev)
+    inf = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def panel():
+        p.copy_(p0)
+        AB.atlb_sgetrf_dev(pn, 32, p, pn, ip, inf, 0)
+    for _ in range(3):
+        panel()
+    copy_ms = timed(torch, stream, lambda: p.copy_(p0), 10)
+    panel_ms = timed(torch, stream, panel, 10) - copy_ms
+    del a, b, c, p, p0
+    name = "tc_gemm split-TF32 7936x7680x256"
+    return {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "traffic": measured_traffic(name), "kernel": name + " (2*M*N*3K TF32 flop per call)",
+            "peak_note": how + "; of measured",
+            "panel_us_per_column": panel_ms * 1e3 / 32,
+            "panel_note": "FP32 leaf panel 8192 x 32 (fused partial-pivoting kernel), latency-bound"}
+
+
 def extra_sharded(torch, AB, dev, stream, rank, world):
     """Paths that shard across GPUs (run when world > 1): DGEMM 8192^3 with C
     split into column slabs (A broadcast from rank 0 over NCCL inside the
@@ -402,18 +475,14 @@ def extra_batched(torch, AB, dev, stream):
         return AB.atlb_dposv_batched(count, ns, ptrs(work), ns, ptrs(Bs), ns, nr, info)
     # restore inputs outside the timed region, one timed launch at a time
     ts = []
-    for rep in range(3):
+    for rep in range(4):   # the third and later calls replay a captured graph
         for w, a in zip(work, A0s):
             w.copy_(a)
         for b, b0 in zip(Bs, rhs0):
             b.copy_(b0)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        assert posv() == 0
-        torch.cuda.synchronize()
-        ts.append(time.perf_counter() - t0)
+        ts.append(timed(torch, stream, lambda: posv(), 1))
     flop = float(np.sum(ns.astype(np.float64) ** 3 / 3 + 2.0 * ns.astype(np.float64) ** 2 * 4))
-    batch_ms = min(ts[1:]) * 1e3
+    batch_ms = min(ts[2:])
     sample = 300
     info_d = torch.zeros(1, dtype=torch.int32, device=dev)
 
@@ -428,7 +497,8 @@ def extra_batched(torch, AB, dev, stream):
     loop_ms = timed(torch, stream, loop, 1) * count / sample
     res["posv_10k"] = {"ms_one_launch": batch_ms, "gflops": flop / batch_ms / 1e6, "all_info_zero": bool((info == 0).all()),
                        "ms_per_instance_loop_scaled": loop_ms, "loop_sample": sample,
-                       "speedup_vs_loop": loop_ms / batch_ms, "timing": "wall clock around the synchronous call"}
+                       "speedup_vs_loop": loop_ms / batch_ms,
+                       "timing": "CUDA events around the call (upload, launch, info back), graph replay"}
     del work, rhs0, A0s
     # LU solves: A = G/sqrt(n) + 4I, 1 RHS
     A0s, work = [None] * count, [None] * count
@@ -443,15 +513,12 @@ def extra_batched(torch, AB, dev, stream):
     piv = [torch.zeros(int(n), dtype=torch.int32, device=dev) for n in ns]
     one = np.ones(count, dtype=np.int32)
     ts = []
-    for rep in range(3):
+    for rep in range(4):
         for w, a in zip(work, A0s):
             w.copy_(a)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        assert AB.atlb_dgesv_batched(count, ns, ptrs(work), ns, ptrs(piv), ptrs(rh), ns, one, info) == 0
-        torch.cuda.synchronize()
-        ts.append(time.perf_counter() - t0)
-    batch_ms = min(ts[1:]) * 1e3
+        ts.append(timed(torch, stream, lambda: AB.atlb_dgesv_batched(count, ns, ptrs(work), ns, ptrs(piv),
+                                                                    ptrs(rh), ns, one, info), 1))
+    batch_ms = min(ts[2:])
     flop = float(np.sum(2.0 / 3.0 * ns.astype(np.float64) ** 3 + 2.0 * ns.astype(np.float64) ** 2))
 
     def loop2():
@@ -463,49 +530,51 @@ def extra_batched(torch, AB, dev, stream):
     loop_ms = timed(torch, stream, loop2, 1) * count / sample
     res["gesv_10k"] = {"ms_one_launch": batch_ms, "gflops": flop / batch_ms / 1e6, "all_info_zero": bool((info == 0).all()),
                        "ms_per_instance_loop_scaled": loop_ms, "loop_sample": sample,
-                       "speedup_vs_loop": loop_ms / batch_ms, "timing": "wall clock around the synchronous call"}
+                       "speedup_vs_loop": loop_ms / batch_ms,
+                       "timing": "CUDA events around the call (upload, launch, info back), graph replay"}
     del work, A0s, rh, piv
     torch.cuda.empty_cache()
-    # 50,000 uneven DGEMMs: operands are sub-blocks of two shared 512 x 512 matrices, C distinct
+    # 50,000 uneven DGEMMs, every problem with its own A, B and C (about 84 GB
+    # of operands, far beyond L2: the launch streams them from HBM)
     cnt = 50000
-    M = rng.integers(16, 513, cnt).astype(np.int32)
-    N = rng.integers(16, 513, cnt).astype(np.int32)
-    K = rng.integers(16, 513, cnt).astype(np.int32)
-    abig = torch.rand(512, 512, dtype=f64, device=dev, generator=g) * 2 - 1
-    bbig = torch.rand(512, 512, dtype=f64, device=dev, generator=g) * 2 - 1
-    sizes = M.astype(np.int64) * N.astype(np.int64)
-    offs = np.concatenate([[0], np.cumsum(sizes)])
-    cbuf = torch.zeros(int(offs[-1]), dtype=f64, device=dev)
-    base = cbuf.data_ptr()
-    cp = (ctypes.c_void_p * cnt)(*[base + 8 * int(o) for o in offs[:-1]])
-    ap = (ctypes.c_void_p * cnt)(*([abig.data_ptr()] * cnt))
-    bp = (ctypes.c_void_p * cnt)(*([bbig.data_ptr()] * cnt))
-    ld = np.full(cnt, 512, dtype=np.int32)
+    M = rng.integers(16, 513, cnt).astype(np.int64)
+    N = rng.integers(16, 513, cnt).astype(np.int64)
+    K = rng.integers(16, 513, cnt).astype(np.int64)
+    oa = np.concatenate([[0], np.cumsum(M * K)])
+    ob = np.concatenate([[0], np.cumsum(K * N)])
+    oc = np.concatenate([[0], np.cumsum(M * N)])
+    abuf = torch.empty(int(oa[-1]), dtype=f64, device=dev)
+    bbuf = torch.empty(int(ob[-1]), dtype=f64, device=dev)
+    cbuf = torch.zeros(int(oc[-1]), dtype=f64, device=dev)
+    for buf in (abuf, bbuf):   # generated in 1 Gi-element chunks
+        for c0 in range(0, buf.numel(), 1 << 30):
+            buf[c0:c0 + (1 << 30)].uniform_(-1.0, 1.0, generator=g)
+    ap = (ctypes.c_void_p * cnt)(*[abuf.data_ptr() + 8 * int(o) for o in oa[:-1]])
+    bp = (ctypes.c_void_p * cnt)(*[bbuf.data_ptr() + 8 * int(o) for o in ob[:-1]])
+    cp = (ctypes.c_void_p * cnt)(*[cbuf.data_ptr() + 8 * int(o) for o in oc[:-1]])
+    M32, N32, K32 = M.astype(np.int32), N.astype(np.int32), K.astype(np.int32)
 
     def grouped():
-        return AB.atlb_dgemm_batched_dev(111, 111, cnt, M, N, K, 1.0, ap, ld, bp, ld, 0.0, cp, M)
+        return AB.atlb_dgemm_batched_dev(111, 111, cnt, M32, N32, K32, 1.0, ap, M32, bp, K32, 0.0, cp, M32)
     grouped()
-    torch.cuda.synchronize()
-    ts = []
-    for rep in range(3):
-        t0 = time.perf_counter()
-        grouped()
-        torch.cuda.synchronize()
-        ts.append(time.perf_counter() - t0)
-    batch_ms = min(ts) * 1e3
-    flop = float(np.sum(2.0 * M.astype(np.float64) * N * K))
+    batch_ms = min(timed(torch, stream, grouped, 1) for _ in range(3))
+    flop = float(np.sum(2.0 * M * N * K))
+    algo_bytes = float(8 * np.sum(M * K + K * N + M * N))
     sample = 2000
 
     def loop3():
         for i in range(sample):
-            AB.atlb_dgemm_dev(111, 111, int(M[i]), int(N[i]), int(K[i]), 1.0, abig, 512, bbig, 512, 0.0,
-                              base + 8 * int(offs[i]), int(M[i]))
+            AB.atlb_dgemm_dev(111, 111, int(M[i]), int(N[i]), int(K[i]), 1.0, ap[i], int(M[i]), bp[i], int(K[i]),
+                              0.0, cp[i], int(M[i]))
     loop3()
     loop_ms = timed(torch, stream, loop3, 1) * cnt / sample
     res["dgemm_50k"] = {"ms_one_launch": batch_ms, "gflops": flop / batch_ms / 1e6,
+                        "operand_gbytes": algo_bytes / 1e9, "operand_gb_per_s": algo_bytes / batch_ms / 1e6,
                         "ms_per_instance_loop_scaled": loop_ms, "loop_sample": sample,
-                        "speedup_vs_loop": loop_ms / batch_ms, "timing": "wall clock around the synchronous call"}
-    del cbuf, abig, bbig
+                        "speedup_vs_loop": loop_ms / batch_ms,
+                        "operands": "distinct A, B, C per problem (HBM-resident, beyond L2)",
+                        "timing": "CUDA events"}
+    del abuf, bbuf, cbuf
     torch.cuda.empty_cache()
     return res
 
@@ -540,7 +609,63 @@ def extra_adjoints(torch, AB, dev, stream):
     av = ainv @ y
     closed = ainv - torch.outer(av, av)
     err = ((Abar - closed).abs().max() / closed.abs().max()).item()
-    return {"gaussian_loss_4096": {"ms_forward_plus_adjoint": ms, "rel_err_vs_closed_form": err}}
+    out = {"gaussian_loss_4096": {"ms_forward_plus_adjoint": ms, "rel_err_vs_closed_form": err}}
+    del ainv, closed, L, Lbar
+    # L(A) = c^T A^-1 b, A = G/sqrt(N) + 4I: getrf + getrs forward, the getrs adjoint
+    ag = torch.randn(n, n, dtype=f64, device=dev, generator=g) / n ** 0.5 + 4.0 * torch.eye(n, dtype=f64, device=dev)
+    acol = ag.T.contiguous()
+    bv = torch.rand(n, dtype=f64, device=dev, generator=g) * 2 - 1
+    cv = torch.rand(n, dtype=f64, device=dev, generator=g) * 2 - 1
+    LU, xv, ipiv = torch.empty_like(acol), torch.empty_like(bv), torch.zeros(n, dtype=torch.int32, device=dev)
+    Abar2 = torch.zeros_like(acol)
+
+    def lu_fwd_bwd():
+        LU.copy_(acol)
+        xv.copy_(bv)
+        AB.atlb_dgetrf_dev(n, n, LU, n, ipiv, info)
+        AB.atlb_dgetrs_dev(111, n, 1, LU, n, ipiv, xv, n)
+        Abar2.zero_()
+        AB.atlb_dgetrs_adjoint_dev(n, 1, LU, n, ipiv, xv, n, cv, n, Bbar, n, Abar2, n)
+    lu_fwd_bwd()
+    ms2 = timed(torch, stream, lu_fwd_bwd, 3)
+    closed2 = -torch.outer(torch.linalg.solve(ag.T, cv), torch.linalg.solve(ag, bv))
+    err2 = ((Abar2.T - closed2).abs().max() / closed2.abs().max()).item()
+    out["getrs_adjoint_4096"] = {"ms_forward_plus_adjoint": ms2, "rel_err_vs_closed_form": err2,
+                                 "loss": "c^T A^-1 b, A = G/sqrt(N) + 4I"}
+    del ag, acol, LU, Abar2, closed2
+    # the Gaussian loss of 512 systems at N = 128: batched forward (one launch) and
+    # the two batched adjoints (one launch each)
+    cnt, nb = 512, 128
+    Bm = torch.randn(cnt, nb, nb, dtype=f64, device=dev, generator=g)
+    A0 = Bm @ Bm.transpose(1, 2) / nb + torch.eye(nb, dtype=f64, device=dev)
+    Ys = torch.rand(cnt, 1, nb, dtype=f64, device=dev, generator=g) * 2 - 1
+    Lw, Xw = A0.clone(), Ys.clone()
+    Lb = torch.zeros_like(A0)
+    Ab3 = torch.zeros_like(A0)
+    Bb3 = torch.zeros_like(Ys)
+    pl = lambda t: np.array([t[i].data_ptr() for i in range(cnt)], dtype=np.uint64)
+    nv = np.full(cnt, nb, np.int32)
+    ones = np.ones(cnt, np.int32)
+    inf3 = np.zeros(cnt, np.int32)
+    pL, pX, pY, pLb, pAb, pBb = pl(Lw), pl(Xw), pl(Ys), pl(Lb), pl(Ab3), pl(Bb3)
+
+    def batched_fwd_bwd():
+        Lw.copy_(A0)
+        Xw.copy_(Ys)
+        AB.atlb_dposv_batched(cnt, nv, pL, nv, pX, nv, ones, inf3)
+        Lb.zero_()
+        Lb.diagonal(dim1=1, dim2=2).copy_(2.0 / Lw.diagonal(dim1=1, dim2=2))
+        AB.atlb_dpotrf_adjoint_batched_dev(cnt, nv, pL, nv, pLb, nv, pAb, nv)
+        AB.atlb_dpotrs_adjoint_batched_dev(cnt, nv, ones, pL, nv, pX, nv, pY, nv, pBb, nv, pAb, nv)
+    batched_fwd_bwd()
+    ms3 = timed(torch, stream, batched_fwd_bwd, 3)
+    ainv = torch.linalg.inv(A0)
+    av = (ainv @ Ys.transpose(1, 2))[..., 0]
+    closed3 = ainv - av[:, :, None] * av[:, None, :]
+    err3 = ((Ab3.transpose(1, 2) - closed3).abs().amax() / closed3.abs().amax()).item()
+    out["gaussian_loss_batched_512x128"] = {"ms_forward_plus_adjoint": ms3, "rel_err_vs_closed_form": err3,
+                                            "launches": "batched posv + batched potrf adjoint + batched potrs adjoint"}
+    return out
 
 
 def run_probe(torch, AB, what, n, acol0, b0, x, ipiv, it, hprec, hpiv, dev):
@@ -556,6 +681,15 @@ def run_probe(torch, AB, what, n, acol0, b0, x, ipiv, it, hprec, hpiv, dev):
             call = lambda: AB.atlb_dgemm_dev(111, 111, n, n, n, 1.0, ga, n, gb, n, 0.0, gc, n)
         else:
             call = lambda: AB.atlb_dgemm_ozaki_dev(111, 111, n, n, n, 1.0, ga, n, gb, n, 0.0, gc, n, 8)
+    elif what == "tcgemm":  # the headline roofline's split-TF32 GEMM (n is ignored)
+        f32 = torch.float32
+        M, N, K = 7936, 7680, 256
+        g = torch.Generator(device=dev)
+        g.manual_seed(77)
+        a = torch.rand(K, M, dtype=f32, device=dev, generator=g) - 0.5
+        b = torch.rand(N, K, dtype=f32, device=dev, generator=g) - 0.5
+        c = torch.rand(N, M, dtype=f32, device=dev, generator=g) - 0.5
+        call = lambda: AB.atlb_sgemm_tc_dev(3, 111, 111, M, N, K, -1.0, a, M, b, K, 1.0, c, M)
     elif what == "getrf":
         A = torch.empty_like(acol0)
         info = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -590,7 +724,7 @@ def main():
     ap.add_argument("--n", type=int, default=N_DEFAULT, help="matrix order (default 8192; smaller for profiling)")
     ap.add_argument("--skip-e2e", action="store_true", help="omit the host-buffer leg (profiling)")
     ap.add_argument("--skip-extras", action="store_true", help="only the headline and FP64 solves (profiling)")
-    ap.add_argument("--probe", choices=["dgemm", "getrf", "mixed", "ozaki"],
+    ap.add_argument("--probe", choices=["dgemm", "getrf", "mixed", "ozaki", "tcgemm"],
                     help="profiling aid: warm up, then run ONE call of the named path at order --n between "
                          "cudaProfilerStart/Stop (ncu --profile-from-start off) and exit")
     args = ap.parse_args()
@@ -715,14 +849,11 @@ def main():
             torch.matmul(ga, gb, out=gc)
         cublas_ms = timed(torch, stream, lambda: torch.matmul(ga, gb, out=gc), 5)
         dgemm_tf, cublas_tf = flop / dgemm_ms / 1e9, flop / cublas_ms / 1e9
-        out["dgemm_8192"] = {"ms": dgemm_ms, "tflops": dgemm_tf, "cublas_fp64_tflops": cublas_tf}
-        out["roofline"] = {"bound": "tensor", "achieved": dgemm_tf, "peak": cublas_tf, "unit": "TFLOP/s",
-                           "frac": dgemm_tf / cublas_tf, "traffic": 7295669760,
-                           "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one 8192^3 launch "
-                                           "(ncu, profiles/dgemm_dmma_8192.md); algorithmic minimum 1.61e9 B",
-                           "kernel": "dgemm_dmma_kernel 8192^3 (2*M*N*K flop per launch)",
-                           "peak_note": "no FP64 figure in MEASURED_PEAKS.json; peak = cuBLAS DGEMM 8192^3 measured in this run"}
+        out["dgemm_8192"] = {"ms": dgemm_ms, "tflops": dgemm_tf, "cublas_fp64_tflops": cublas_tf,
+                             "frac_of_cublas": dgemm_tf / cublas_tf,
+                             "dram_bytes_per_launch": measured_traffic("dgemm_dmma_kernel 8192^3")}
         del ga, gb
+        out["roofline"] = headline_roofline(torch, AB, dev, stream)
 
         # ---- split-integer (Ozaki) DGEMM 8192^3 on the INT8 tensor cores
         # operands x = u * 2^e, u ~ U[-1,1], e ~ U{-10..10}; storage tensors hold
