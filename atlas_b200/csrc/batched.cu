@@ -17,6 +17,7 @@
 #include <cstring>
 #include <vector>
 #include "common.cuh"
+#include "chol_blocks.cuh"
 #include "kernels.h"
 #include "staging.h"
 #include "../../include/atlas_b200.h"
@@ -38,89 +39,6 @@ struct Prob {
 };
 
 // ---------------------------------------------------------------- Cholesky
-
-// C (lower part of rows/cols r0.., order mt) -= P P^T, P = the mt x jb block
-// of the panel at (rows r0..) in shared memory (ld lds); C in shared memory
-// (ldc, offset c0) or global.  16 x 16 threads, 4 x 4 register tiles over
-// 64 x 64 blocks of the lower triangle.
-template <typename CT>
-__device__ __forceinline__ void syrk_lower_update(int mt, int jb, const double *P, int lds, CT *C, long ldc) {
-  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  for (int ib = 0; ib < mt; ib += 64)
-    for (int kb = 0; kb <= ib; kb += 64) {
-      double acc[4][4];
-#pragma unroll
-      for (int a = 0; a < 4; a++)
-#pragma unroll
-        for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
-      for (int q = 0; q < jb; q++) {
-        double pi[4], pk[4];
-#pragma unroll
-        for (int a = 0; a < 4; a++) {
-          const int i = ib + tx + 16 * a;
-          pi[a] = i < mt ? P[i + q * lds] : 0.0;
-        }
-#pragma unroll
-        for (int b = 0; b < 4; b++) {
-          const int k = kb + ty + 16 * b;
-          pk[b] = k < mt ? P[k + q * lds] : 0.0;
-        }
-#pragma unroll
-        for (int a = 0; a < 4; a++)
-#pragma unroll
-          for (int b = 0; b < 4; b++) acc[a][b] = fma(pi[a], pk[b], acc[a][b]);
-      }
-#pragma unroll
-      for (int a = 0; a < 4; a++)
-#pragma unroll
-        for (int b = 0; b < 4; b++) {
-          const int i = ib + tx + 16 * a, k = kb + ty + 16 * b;
-          if (i < mt && k <= i) C[i + (long)k * ldc] -= acc[a][b];
-        }
-    }
-}
-
-// Cholesky of the jb columns of the m x jb panel at s (ld lds, rows from the
-// panel's diagonal): unblocked within the panel (one row per thread).
-// Returns 0 or the first non-positive pivot (1-based, panel-relative).
-__device__ int chol_panel(double *s, int lds, int m, int jb, int *sfail) {
-  const int tid = threadIdx.x;
-  for (int c = 0; c < jb; c++) {
-    const double d = s[c + c * lds];
-    if (!(d > 0.0)) {
-      if (tid == 0) *sfail = c + 1;
-      __syncthreads();
-      return c + 1;
-    }
-    const double ri = 1.0 / sqrt(d);
-    __syncthreads();  // every thread has read the pivot
-    for (int i = c + tid; i < m; i += BT) s[i + c * lds] = i == c ? d * ri : s[i + c * lds] * ri;
-    __syncthreads();  // column c holds the multipliers
-    for (int i = c + 1 + tid; i < m; i += BT) {  // the panel's columns right of c, row by row
-      const double l = s[i + c * lds];
-      const int kmax = min(jb - 1, i);
-      for (int k = c + 1; k <= kmax; k++) s[i + k * lds] = fma(-l, s[k + c * lds], s[i + k * lds]);
-    }
-    __syncthreads();
-  }
-  return 0;
-}
-
-// blocked right-looking Cholesky of an n x n lower matrix in shared memory
-// (ld = lds): 16-column panels factored in place, the trailing lower triangle
-// updated with register tiles; returns 0 or the first non-positive pivot
-// (1-based)
-__device__ int chol_smem(double *s, int lds, int n, int *sfail) {
-  for (int j = 0; j < n; j += 16) {
-    const int jb = min(16, n - j), m = n - j;
-    double *P = s + j + j * lds;
-    const int f = chol_panel(P, lds, m, jb, sfail);
-    if (f) return j + f;
-    if (m > jb) syrk_lower_update(m - jb, jb, P + jb, lds, P + jb + jb * lds, lds);
-    __syncthreads();
-  }
-  return 0;
-}
 
 // forward then backward substitution with L (lower, in shared memory or
 // global, ld = ldl) for nrhs columns of B (global)
@@ -149,13 +67,12 @@ __global__ void __launch_bounds__(BT)
 batched_posv_kernel(const Prob *__restrict__ probs, const int *__restrict__ order, int count,
                     int *__restrict__ next, int *__restrict__ info, int SMALL, int PW) {
   extern __shared__ __align__(16) double sm[];
-  __shared__ int s_p, s_fail;
+  __shared__ int s_p;
   const int tid = threadIdx.x;
   while (true) {
     if (tid == 0) {
       const int t = atomicAdd(next, 1);
       s_p = t < count ? order[t] : -1;
-      s_fail = 0;
     }
     __syncthreads();
     const int p = s_p;
@@ -164,10 +81,10 @@ batched_posv_kernel(const Prob *__restrict__ probs, const int *__restrict__ orde
     const int n = pr.n;
     int fail = 0;
     if (n <= SMALL) {
-      const int lds = n + 1;
+      const int lds = cholb::ld_for(n);
       for (int idx = tid; idx < n * n; idx += BT) sm[idx % n + (idx / n) * lds] = pr.A[idx % n + (long)(idx / n) * pr.lda];
       __syncthreads();
-      fail = chol_smem(sm, lds, n, &s_fail);
+      fail = cholb::chol_smem(sm, lds, n);
       for (int idx = tid; idx < n * n; idx += BT) {
         const int i = idx % n, k = idx / n;
         if (i >= k) pr.A[i + (long)k * pr.lda] = sm[i + k * lds];
@@ -178,12 +95,12 @@ batched_posv_kernel(const Prob *__restrict__ probs, const int *__restrict__ orde
       // panels of PW columns: factor the panel (rows j..n) in shared memory,
       // then update the trailing lower triangle in global memory
       for (int j = 0; j < n && !fail; j += PW) {
-        const int jb = min(PW, n - j), m = n - j, lds = m + 1;
+        const int jb = min(PW, n - j), m = n - j, lds = cholb::ld_for(m);
         for (int idx = tid; idx < m * jb; idx += BT)
           sm[idx % m + (idx / m) * lds] = pr.A[j + idx % m + (long)(j + idx / m) * pr.lda];
         __syncthreads();
         {
-          const int f = chol_panel(sm, lds, m, jb, &s_fail);
+          const int f = cholb::chol_panel(sm, lds, m, jb);
           if (f) fail = j + f;
         }
         for (int idx = tid; idx < m * jb; idx += BT) {
@@ -192,7 +109,7 @@ batched_posv_kernel(const Prob *__restrict__ probs, const int *__restrict__ orde
         }
         if (fail) break;
         // trailing update: A[j+jb.., j+jb..] -= P2 P2^T (lower), P2 = panel rows jb..m
-        if (m > jb) syrk_lower_update(m - jb, jb, sm + jb, lds, pr.A + (j + jb) + (long)(j + jb) * pr.lda, pr.lda);
+        if (m > jb) cholb::syrk_panel(m - jb, m - jb, jb, sm + jb, lds, pr.A + (j + jb) + (long)(j + jb) * pr.lda, pr.lda);
         __syncthreads();
       }
       __syncthreads();
@@ -393,8 +310,8 @@ void batched_posv_dev(const std::vector<Prob> &P, int *info_out, cudaStream_t st
   for (auto &p : P) maxn = std::max(maxn, p.n);
   const int SMALL = tune(kTuneBatchPosvSmall), PW = tune(kTuneBatchPosvPW);
   const int sn = std::min(maxn, SMALL);
-  const size_t sm_bytes = std::max(sizeof(double) * sn * (sn + 1),
-                                   maxn > SMALL ? sizeof(double) * (size_t)(maxn + 1) * PW : (size_t)0);
+  const size_t sm_bytes = std::max(sizeof(double) * sn * cholb::ld_for(sn),
+                                   maxn > SMALL ? sizeof(double) * (size_t)cholb::ld_for(maxn) * PW : (size_t)0);
   static bool configured = false;
   if (!configured) {
     ATLB_CUDA_CHECK(cudaFuncSetAttribute(batched_posv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));

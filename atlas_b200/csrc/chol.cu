@@ -4,77 +4,69 @@
 // Driver: the reference's recursion (src/lapack/ATL_potrfL.c:204-263,
 // ATL_potrfU.c:199-257): factor the leading half, TRSM the off-diagonal block
 // against it, SYRK-update the trailing half (the DMMA GEMM restricted to one
-// triangle), factor the trailing half.  Leaves of <= 64 columns are factored
-// by one CTA in shared memory; the upper case is factored as the transpose
-// of the lower one (U = L^T), so a single leaf kernel serves both.
+// triangle), factor the trailing half.  Leaves of <= 128 columns are factored
+// by one CTA in shared memory (blocked: 16-column panels and register-tiled
+// updates of the trailing triangle); the upper case is factored as the
+// transpose of the lower one (U = L^T), so a single leaf kernel serves both.
 #include <algorithm>
 #include <cmath>
 #include <vector>
 #include "common.cuh"
 #include "kernels.h"
+#include "chol_blocks.cuh"
 
 namespace atlb {
 namespace {
 
-constexpr int CLEAF = 64;
+constexpr int CLEAF = 128;
 
-// Factor the n x n (n <= 64) diagonal block at A in place; first
-// non-positive pivot j lowers *dinfo to ioff + j + 1 and stops the block.
-// Thread (i, g) keeps row i's columns g, g+4, ... of L in registers (the
-// upper case works on the transpose, U = L^T).  Each step needs column j of
-// the partially updated matrix; its owners publish it to a double-buffered
-// shared copy at the end of the previous step, so a step costs one barrier.
+// Factor the n x n (n <= 128) diagonal block at A in place in shared memory
+// (cholb::chol_smem: 16-column panels, the trailing triangle updated on the
+// FP64 tensor cores for double, with 4 x 4 register tiles for float); the
+// upper case is loaded transposed (U = L^T).  A first non-positive pivot j lowers *dinfo to ioff + j + 1; the
+// block is then left partly factored.
 template <typename T>
 __global__ void __launch_bounds__(256)
-potf2_kernel(int n, T *A, long lda, int upper, int *dinfo, int ioff) {
-  static_assert(CLEAF == 64, "4 threads per row, 16 columns each");
-  __shared__ T pcol[2][CLEAF];
-  const int tid = threadIdx.x, i = tid % CLEAF, g = tid / CLEAF;
-  T a[CLEAF / 4];
+potrf_leaf_kernel(int n, T *A, long lda, int upper, int *dinfo, int ioff) {
+  extern __shared__ __align__(16) unsigned char leaf_smem[];
+  T *S = reinterpret_cast<T *>(leaf_smem);
+  const int lds = cholb::ld_for(n);
+  const int nn = n * n, tid = threadIdx.x;
+  for (int base = 0; base < nn; base += 256 * 8) {  // eight loads in flight per thread
+    T v[8];
 #pragma unroll
-  for (int m = 0; m < CLEAF / 4; m++) {
-    const int k = g + 4 * m;
-    a[m] = (i < n && k <= i) ? (upper ? A[k + (long)i * lda] : A[i + (long)k * lda]) : T(0);
+    for (int u = 0; u < 8; u++) {
+      const int idx = base + u * 256 + tid, i = idx % n, k = idx / n;
+      v[u] = (idx < nn && i >= k) ? (upper ? A[k + (long)i * lda] : A[i + (long)k * lda]) : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int idx = base + u * 256 + tid, i = idx % n, k = idx / n;
+      if (idx < nn && i >= k) S[i + k * lds] = v[u];
+    }
   }
-  if (g == 0) pcol[0][i] = a[0];
   __syncthreads();
-#pragma unroll 1
-  for (int j = 0; j < n; j++) {
-    const int b = j & 1;
-    const T djj = pcol[b][j];
-    if (!(djj > T(0))) {
-      if (tid == 0) atomicMin(dinfo, ioff + j + 1);
-      break;  // uniform: every thread read the same pivot
-    }
-    const T d = sqrt(djj), rd = T(1) / d;
-    if (i >= j && i < n) {
-      const T li = i == j ? d : pcol[b][i] * rd;
-#pragma unroll
-      for (int m = 0; m < CLEAF / 4; m++) {
-        const int k = g + 4 * m;
-        if (k == j) a[m] = li;
-        else if (k > j && k <= i) a[m] = fma(-li, pcol[b][k] * rd, a[m]);
-      }
-    }
-    if (g == ((j + 1) & 3) && i > j && i < n) {
-      T v = T(0);
-#pragma unroll
-      for (int m = 0; m < CLEAF / 4; m++)
-        if (g + 4 * m == j + 1) v = a[m];
-      pcol[b ^ 1][i] = v;
-    }
-    __syncthreads();
+  const int fail = cholb::chol_smem(S, lds, n);
+  if (fail && threadIdx.x == 0) atomicMin(dinfo, ioff + fail);
+  for (int idx = tid; idx < nn; idx += 256) {
+    const int i = idx % n, k = idx / n;
+    if (i < k) continue;
+    if (upper) A[k + (long)i * lda] = S[i + k * lds];
+    else A[i + (long)k * lda] = S[i + k * lds];
   }
-  if (i < n) {
-#pragma unroll
-    for (int m = 0; m < CLEAF / 4; m++) {
-      const int k = g + 4 * m;
-      if (k <= i) {
-        if (upper) A[k + (long)i * lda] = a[m];
-        else A[i + (long)k * lda] = a[m];
-      }
-    }
+}
+
+template <typename T>
+void potrf_leaf(int n, T *Ad, long lda, int upper, int *dinfo, int ioff, cudaStream_t st) {
+  const size_t smem = sizeof(T) * (size_t)n * cholb::ld_for(n);
+  static bool configured = false;
+  if (!configured) {
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(potrf_leaf_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(sizeof(T) * CLEAF * cholb::ld_for(CLEAF))));
+    configured = true;
   }
+  potrf_leaf_kernel<T><<<1, 256, smem, st>>>(n, Ad, lda, upper, dinfo, ioff);
+  ATLB_CUDA_CHECK(cudaGetLastError());
 }
 
 void syrk_update(SgemmFn, int upper, int n, int k, const double *X, double *C, long lda,
@@ -105,8 +97,7 @@ void potrf_rec(int upper, int off, int N, T *A, long lda, int *dinfo, cudaStream
   if (N <= 0) return;
   T *Ad = A + off + (long)off * lda;
   if (N <= CLEAF) {
-    potf2_kernel<T><<<1, 256, 0, st>>>(N, Ad, lda, upper, dinfo, off);
-    ATLB_CUDA_CHECK(cudaGetLastError());
+    potrf_leaf<T>(N, Ad, lda, upper, dinfo, off, st);
     return;
   }
   const int Nl = std::max(CLEAF, (N / 2) / CLEAF * CLEAF), Nr = N - Nl;

@@ -307,6 +307,23 @@ __global__ void scale_kernel(int M, int N, double beta, double *C, long ldc, int
   }
 }
 
+// Slices for a split-K GEMM of `tiles` output tiles (too few for the SMs):
+// the smallest count, slices of at least 2 BK, whose CTAs (tiles x slices)
+// fill their waves of nsm within 3 % of the best count -- e.g. 63 tiles take
+// 7 slices (441 CTAs in 3 full waves), not 3 (189 CTAs, a second wave of 41).
+int splitk_count(int tiles, int K, int nsm) {
+  const int smax = std::max(1, std::min(K / (2 * BK), 4 * nsm));
+  auto fill = [&](int s) {
+    const long c = (long)tiles * s;
+    return (double)c / ((double)cdiv(c, (long)nsm) * nsm);
+  };
+  double best = 0.0;
+  for (int s = 1; s <= smax; s++) best = std::max(best, fill(s));
+  for (int s = 1; s <= smax; s++)
+    if (fill(s) >= 0.97 * best) return s;
+  return 1;
+}
+
 template <bool TA, bool TB, int VEC>
 void launch(int M, int N, int K, double alpha, const double *A, long lda, const double *B,
             long ldb, double beta, double *C, long ldc, int tri, cudaStream_t st) {
@@ -321,7 +338,7 @@ void launch(int M, int N, int K, double alpha, const double *A, long lda, const 
   // too few tiles for the 148 SMs and a long K: split K (partials + reduction)
   const int nsm = num_sms();
   int S = 1;
-  if (tune(kTuneSplitK) && tiles * 2 <= nsm && K >= 4 * BK && !no_alloc_active()) S = std::min(cdiv(nsm, tiles), K / (2 * BK));
+  if (tune(kTuneSplitK) && tiles * 2 <= nsm && K >= 4 * BK && !no_alloc_active()) S = splitk_count(tiles, K, nsm);
   if (S > 1) {
     const int kc = cdiv(cdiv(K, S), BK) * BK;
     S = cdiv(K, kc);

@@ -281,25 +281,251 @@ __global__ void extract_v_kernel(int M, int k, const double *P, long ldp, double
   }
 }
 
-// T (k x k upper, ld k) from G = V^T V and tau: T(0:i,i) = -tau_i T(0:i,0:i) G(0:i,i)
+// T (k x k upper, ld k, k <= NBQ_MAX) of the block reflector
+// H(0) H(1) ... H(k-1) = I - V T V^T, from G = V^T V and tau.  ATL_larft's
+// column recurrence T(0:i,i) = -tau_i T(0:i,0:i) G(0:i,i), T(i,i) = tau_i
+// runs on the 16-column diagonal blocks (one warp each, all at once); the
+// blocks are then merged pairwise, 16 -> 32 -> 64 -> 128, with the identity
+// H1 H2 = I - [V1 V2] [T1, -T1 (V1^T V2) T2; 0, T2] [V1 V2]^T, i.e.
+// T12 = -T1 G12 T2 (two small products in shared memory per level).
+// G's strictly upper part is overwritten in place by T's.
+constexpr int LFT_LD = NBQ_MAX + 1;
 __global__ void __launch_bounds__(256) larft_kernel(int k, const double *G, const double *tau, double *T) {
-  extern __shared__ double sT[];  // k x k
-  const int tid = threadIdx.x;
-  for (int idx = tid; idx < k * k; idx += blockDim.x) sT[idx] = 0.0;
+  extern __shared__ double lft_smem[];
+  double *S = lft_smem;                      // k x k, ld LFT_LD: G, then T
+  double *W = lft_smem + NBQ_MAX * LFT_LD;   // products G12 T2 of one level (<= NBQ_MAX^2 / 4 doubles)
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int idx = tid; idx < k * k; idx += 256) {
+    const int r = idx % k, c = idx / k;
+    S[r + c * LFT_LD] = r < c ? G[r + (long)c * k] : 0.0;
+  }
   __syncthreads();
-  for (int i = 0; i < k; i++) {
-    const double ti = tau[i];
-    double val = 0.0;
-    if (tid < i) {
-      for (int q = tid; q < i; q++) val += sT[tid + q * k] * G[q + (long)i * k];
-      val *= -ti;
+  for (int b = warp; b * 16 < k; b += 8) {   // diagonal blocks by the recurrence
+    const int o = b * 16, kb = min(16, k - o);
+    double *B = S + o + o * LFT_LD;
+    for (int i = 0; i < kb; i++) {
+      double val = 0.0;
+      if (lane < i) {
+        for (int q = lane; q < i; q++) val = fma(B[lane + q * LFT_LD], B[q + i * LFT_LD], val);
+        val *= -tau[o + i];
+      }
+      __syncwarp();  // column i of G read by every lane before it is overwritten
+      if (lane < i) B[lane + i * LFT_LD] = val;
+      if (lane == i) B[i + i * LFT_LD] = tau[o + i];
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  for (int h = 16; h < k; h *= 2) {          // merge sibling blocks of order h
+    const int npair = (k + 2 * h - 1) / (2 * h);
+    // W_p = G12 T2 (h x h2): G12 = S[o : o+h, o+h : o+h+h2], T2 upper h2 x h2
+    for (int idx = tid; idx < npair * h * h; idx += 256) {
+      const int p = idx / (h * h), e = idx % (h * h), r = e % h, c = e / h;
+      const int o = 2 * h * p, h2 = min(h, k - o - h);
+      if (h2 <= 0 || c >= h2) continue;
+      const double *G12 = S + o + (o + h) * LFT_LD, *T2 = S + (o + h) + (o + h) * LFT_LD;
+      double v = 0.0;
+      for (int q = 0; q <= c; q++) v = fma(G12[r + q * LFT_LD], T2[q + c * LFT_LD], v);
+      W[p * h * h + r + c * h] = v;
     }
     __syncthreads();
-    if (tid < i) sT[tid + i * k] = val;
-    if (tid == 0) sT[i + i * k] = ti;
+    // T12 = -T1 W_p, T1 upper h x h
+    for (int idx = tid; idx < npair * h * h; idx += 256) {
+      const int p = idx / (h * h), e = idx % (h * h), r = e % h, c = e / h;
+      const int o = 2 * h * p, h2 = min(h, k - o - h);
+      if (h2 <= 0 || c >= h2) continue;
+      const double *T1 = S + o + o * LFT_LD;
+      const double *Wp = W + p * h * h;
+      double v = 0.0;
+      for (int q = r; q < h; q++) v = fma(T1[r + q * LFT_LD], Wp[q + c * h], v);
+      S[(o + r) + (o + h + c) * LFT_LD] = -v;
+    }
     __syncthreads();
   }
-  for (int idx = tid; idx < k * k; idx += blockDim.x) T[idx] = sT[idx];
+  for (int idx = tid; idx < k * k; idx += 256) {
+    const int r = idx % k, c = idx / k;
+    T[idx] = r <= c ? S[r + c * LFT_LD] : 0.0;
+  }
+}
+
+constexpr size_t larft_smem_bytes() { return sizeof(double) * ((size_t)NBQ_MAX * LFT_LD + NBQ_MAX * NBQ_MAX / 4); }
+
+// ---- Applying a leaf's reflectors to the rest of its panel.  The leaf is
+// m x kb (kb <= 32) with V its unit lower trapezoid, C the n2 panel columns
+// on its right (kb + n2 <= NBQ_MAX).  C <- (I - V T V^T)^T C as three
+// streaming passes over the rows, in place of GEMMs whose output (kb x n2)
+// is too small to fill the GPU:
+//   1. qr_leaf_gram_kernel: per-CTA partial sums of V^T [V C] (kb x (kb+n2));
+//   2. qr_leaf_reduce_kernel: the partials summed in a fixed order;
+//   3. qr_leaf_apply_kernel: every CTA forms T from G = V^T V (the column
+//      recurrence) and Y = T^T (V^T C), then C -= V Y for its rows.
+// V is read straight from the factored leaf (unit diagonal and zeros above
+// it applied on the fly).
+constexpr int QL_GRID = 256;         // CTAs of the partial-sum pass (at most)
+constexpr int QL_OUT = 32 * NBQ_MAX; // doubles per partial (kb <= 32 rows of <= NBQ_MAX columns)
+
+__device__ __forceinline__ double leaf_v(const double *L, long lda, int r, int a) {
+  return r > a ? L[r + (long)a * lda] : (r == a ? 1.0 : 0.0);
+}
+
+template <int KB>
+__global__ void __launch_bounds__(256) qr_leaf_gram_kernel(int m, int kb, int ncol, const double *L, long lda,
+                                                           int rpc, double *part) {
+  __shared__ double X[NBQ_MAX][33];  // 32 rows of [V C], column by column
+  constexpr int SB = 256 / KB, NJ = NBQ_MAX / SB;
+  const int tid = threadIdx.x, a = tid % KB, b0 = tid / KB;
+  double acc[NJ];
+#pragma unroll
+  for (int j = 0; j < NJ; j++) acc[j] = 0.0;
+  const int rb = blockIdx.x * rpc, re = min(m, rb + rpc);
+  for (int r0 = rb; r0 < re; r0 += 32) {
+    __syncthreads();
+    double v[NBQ_MAX / 8];  // all of this thread's loads in flight before the stores
+    const int r = r0 + (tid & 31);
+#pragma unroll
+    for (int u = 0; u < NBQ_MAX / 8; u++) {
+      const int c = (tid >> 5) + 8 * u;
+      v[u] = 0.0;
+      if (r < re && c < ncol) v[u] = c < kb ? leaf_v(L, lda, r, c) : L[r + (long)c * lda];
+    }
+#pragma unroll
+    for (int u = 0; u < NBQ_MAX / 8; u++) {
+      const int c = (tid >> 5) + 8 * u;
+      if (c < ncol) X[c][tid & 31] = v[u];
+    }
+    __syncthreads();
+    const int nr = min(32, re - r0);
+    for (int rr = 0; rr < nr; rr++) {
+      const double xa = a < kb ? X[a][rr] : 0.0;
+#pragma unroll
+      for (int j = 0; j < NJ; j++) {
+        const int b = b0 + SB * j;
+        if (b < ncol) acc[j] = fma(xa, X[b][rr], acc[j]);
+      }
+    }
+  }
+  double *P = part + (size_t)blockIdx.x * QL_OUT;
+#pragma unroll
+  for (int j = 0; j < NJ; j++) P[a + (b0 + SB * j) * KB] = acc[j];
+}
+
+// P[o] = sum over g < ngrid of part[g][o], o < nout: eight partial sums per
+// output (warps), combined in a fixed order
+__global__ void __launch_bounds__(256) qr_leaf_reduce_kernel(int ngrid, int nout, const double *part, double *P) {
+  __shared__ double red[8][33];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, o = blockIdx.x * 32 + lane;
+  double v = 0.0;
+  if (o < nout)
+    for (int g = w; g < ngrid; g += 8) v += part[(size_t)g * QL_OUT + o];
+  red[w][lane] = v;
+  __syncthreads();
+  if (w == 0 && o < nout) {
+    double t = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; q++) t += red[q][lane];
+    P[o] = t;
+  }
+}
+
+template <int KB>
+__global__ void __launch_bounds__(256) qr_leaf_apply_kernel(int m, int kb, int n2, double *L, long lda,
+                                                            const double *P, const double *tau) {
+  constexpr int RPT = KB == 8 ? 4 : 2;  // rows per thread
+  __shared__ double sT[KB][KB + 1];
+  __shared__ double sW[KB][NBQ_MAX + 1];  // W = V^T C, then Y = T^T W in its place
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  for (int idx = tid; idx < KB * (kb + n2); idx += 256) {
+    const int a = idx % KB, b = idx / KB;
+    const double v = a < kb ? P[a + b * KB] : 0.0;
+    if (b < kb) sT[a][b] = v;  // G = V^T V for now
+    else sW[a][b - kb] = v;
+  }
+  __syncthreads();
+  if (w == 0) {  // T from G (upper; the recurrence overwrites G's strictly upper part)
+    for (int i = 0; i < kb; i++) {
+      double val = 0.0;
+      if (lane < i) {
+        for (int q = lane; q < i; q++) val = fma(sT[lane][q], sT[q][i], val);
+        val *= -tau[i];
+      }
+      __syncwarp();
+      if (lane < i) sT[lane][i] = val;
+      if (lane == i) sT[i][i] = tau[i];
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  constexpr int NY = KB * NBQ_MAX / 256;  // Y = T^T W: outputs per thread, held until W is read
+  double y[NY];
+#pragma unroll
+  for (int u = 0; u < NY; u++) {
+    const int idx = tid + 256 * u, a = idx % KB, c = idx / KB;
+    double v = 0.0;
+    if (a < kb && c < n2)
+      for (int q = 0; q <= a; q++) v = fma(sT[q][a], sW[q][c], v);
+    y[u] = v;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < NY; u++) {
+    const int idx = tid + 256 * u;
+    sW[idx % KB][idx / KB] = y[u];
+  }
+  __syncthreads();
+  // C -= V Y: 32 lanes x RPT rows by 8 column groups per CTA tile of 32 * RPT rows
+  const int cq = w;
+  for (int rt = blockIdx.x * 32 * RPT; rt < m; rt += gridDim.x * 32 * RPT) {
+    double v[RPT][KB];
+#pragma unroll
+    for (int i = 0; i < RPT; i++) {
+      const int r = rt + lane + 32 * i;
+#pragma unroll
+      for (int a = 0; a < KB; a++) v[i][a] = (r < m && a < kb) ? leaf_v(L, lda, r, a) : 0.0;
+    }
+#pragma unroll 2
+    for (int c = cq; c < n2; c += 8) {
+      double acc[RPT];
+#pragma unroll
+      for (int i = 0; i < RPT; i++) acc[i] = 0.0;
+#pragma unroll
+      for (int a = 0; a < KB; a++) {
+        const double y = sW[a][c];
+#pragma unroll
+        for (int i = 0; i < RPT; i++) acc[i] = fma(v[i][a], y, acc[i]);
+      }
+#pragma unroll
+      for (int i = 0; i < RPT; i++) {
+        const int r = rt + lane + 32 * i;
+        if (r < m) L[r + (long)(kb + c) * lda] -= acc[i];
+      }
+    }
+  }
+}
+
+template <int KB>
+void leaf_apply_t(int m, int kb, int n2, double *L, long lda, const double *tau, double *part, double *P,
+                  cudaStream_t st) {
+  const int ncol = kb + n2;
+  const int rpc = cdiv(cdiv(m, QL_GRID), 32) * 32;
+  const int grid = cdiv(m, rpc);
+  qr_leaf_gram_kernel<KB><<<grid, 256, 0, st>>>(m, kb, ncol, L, lda, rpc, part);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+  const int nout = KB * ncol;
+  qr_leaf_reduce_kernel<<<cdiv(nout, 32), 256, 0, st>>>(grid, nout, part, P);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+  constexpr int RPT = KB == 8 ? 4 : 2;
+  const int agrid = std::min(cdiv(m, 32 * RPT), 2 * num_sms());
+  qr_leaf_apply_kernel<KB><<<agrid, 256, 0, st>>>(m, kb, n2, L, lda, P, tau);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
+
+// the leaf at L (m x kb, factored) applied to the n2 columns on its right
+void leaf_apply(int m, int kb, int n2, double *L, long lda, const double *tau, double *part, double *P,
+                cudaStream_t st) {
+  if (m <= 0 || n2 <= 0 || kb <= 0) return;
+  if (kb <= 8) leaf_apply_t<8>(m, kb, n2, L, lda, tau, part, P, st);
+  else if (kb <= 16) leaf_apply_t<16>(m, kb, n2, L, lda, tau, part, P, st);
+  else leaf_apply_t<32>(m, kb, n2, L, lda, tau, part, P, st);
 }
 
 // C (m x n, ldc) = (I - V T V^T)^T C, V explicit (m x k, ld m), T k x k
@@ -318,14 +544,13 @@ void build_vt(int m, int k, const double *P, long ldp, const double *tau, double
   extract_v_kernel<<<(int)std::min<long>((tot + 255) / 256, 8192), 256, 0, st>>>(m, k, P, ldp, V);
   ATLB_CUDA_CHECK(cudaGetLastError());
   dgemm_dev(kTrans, kNoTrans, k, k, m, 1.0, V, m, V, m, 0.0, G, k, st);
-  size_t sm = sizeof(double) * k * k;
   static bool cfg = false;
   if (!cfg) {
     ATLB_CUDA_CHECK(cudaFuncSetAttribute(larft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)(sizeof(double) * NBQ_MAX * NBQ_MAX)));
+                                         (int)larft_smem_bytes()));
     cfg = true;
   }
-  larft_kernel<<<1, 256, sm, st>>>(k, G, tau, T);
+  larft_kernel<<<1, 256, larft_smem_bytes(), st>>>(k, G, tau, T);
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
 
@@ -382,10 +607,12 @@ void dgeqrf_dev(int M, int N, double *A, long lda, double *tau, cudaStream_t st)
   const int mn = std::min(M, N);
   if (mn <= 0) return;
   const int NBQ = tune(kTuneQrNB);  // the outer panel width (ATL_ilaenv's NB, tuned)
-  // workspace: V (M x NBQ), G and T (NBQ x NBQ each), W (2 x NBQ x N)
-  size_t need = (size_t)M * NBQ + 2 * (size_t)NBQ * NBQ + 2 * (size_t)NBQ * N;
+  // workspace: V (M x NBQ), G and T (NBQ x NBQ each), W (2 x NBQ x N), the
+  // leaf passes' partial sums (QL_GRID x QL_OUT) and their total (QL_OUT)
+  size_t need = (size_t)M * NBQ + 2 * (size_t)NBQ * NBQ + 2 * (size_t)NBQ * N + (size_t)(QL_GRID + 1) * QL_OUT;
   double *ws = (double *)scratch(kSlotWork, sizeof(double) * need);
   double *V = ws, *G = V + (size_t)M * NBQ, *T = G + (size_t)NBQ * NBQ, *W = T + (size_t)NBQ * NBQ;
+  double *part = W + 2 * (size_t)NBQ * N, *Psum = part + (size_t)QL_GRID * QL_OUT;
   for (int j = 0; j < mn; j += NBQ) {
     const int nb = std::min(NBQ, mn - j), m = M - j;
     double *P = A + j + (long)j * lda;
@@ -394,10 +621,7 @@ void dgeqrf_dev(int M, int N, double *A, long lda, double *tau, cudaStream_t st)
       const int leaf = std::min(qr_leaf(m - l), nb - l);
       double *L = P + l + (long)l * lda;
       geqr2_leaf(m - l, leaf, L, lda, tau + j + l, st);
-      if (l + leaf < nb) {
-        build_vt(m - l, leaf, L, lda, tau + j + l, V, G, T, st);
-        larfb_lt(m - l, nb - l - leaf, leaf, V, T, L + (long)leaf * lda, lda, W, st);
-      }
+      if (l + leaf < nb) leaf_apply(m - l, leaf, nb - l - leaf, L, lda, tau + j + l, part, Psum, st);
       l += leaf;
     }
     if (j + nb < N) {

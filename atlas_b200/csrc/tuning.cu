@@ -28,7 +28,7 @@ struct TuneDef {
 };
 const TuneDef kDefs[kNumTune] = {
     {"getrf_nb", 256, 64, 256, 32},           // outer LU block (leaf panels are 32 wide)
-    {"potrf_nb", 256, 64, 1024, 64},          // outer Cholesky block (leaves are 64 wide)
+    {"potrf_nb", 256, 64, 16384, 64},         // outer Cholesky block (leaves are 128 wide; >= N: pure recursion)
     {"dgemm_group", 8, 1, 64, 1},             // DGEMM rasterisation: tile rows sharing B panels
     {"dgemm_splitk", 1, 0, 1, 1},             // split K when the output has too few tiles
     {"lookahead", 1, 0, 1, 1},                // depth-one look-ahead in getrf / potrf
