@@ -156,36 +156,37 @@ __device__ __forceinline__ void dgemm_tile(int M, int N, int K, double alpha, co
   }
   cp_async_wait<0>();
 
-  // epilogue: C fragment row = lane>>2, cols = 2*(lane&3) + {0,1}.  The old
-  // C values of fragment row i+1 are loaded before row i is stored, so the
-  // loads' latencies overlap instead of adding up.
+  // epilogue: C fragment row = lane>>2, cols = 2*(lane&3) + {0,1}.  With
+  // beta != 0 the old C tile is first staged in shared memory (the pipeline
+  // buffers are free now) by one burst of asynchronous copies, so its load
+  // latency is paid once per tile rather than once per fragment row.
   auto ok = [&](int r, int c) {
     return r < M && c < N && !(tri == 1 && r < c) && !(tri == 2 && r > c);
   };
-  double cv[2][4][2];
-  auto load_c = [&](int i, double (&d)[4][2]) {
-    const int r = m0 + wm + i * 8 + fr;
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const int c = n0 + wn + j * 8 + fk * 2 + h;
-        d[j][h] = (beta != 0.0 && ok(r, c)) ? C[r + (long)c * ldc] : 0.0;
-      }
-  };
-  load_c(0, cv[0]);
+  constexpr int CLD = BM + 4;  // staged C: column-major, ld CLD (fits the STAGES pipeline buffers)
+  static_assert(BN * CLD <= STAGES * (Lay<false>::SIZE + Lay<false>::SIZE), "C tile does not fit");
+  double *sC = smem;
+  if (beta != 0.0) {
+    __syncthreads();  // every warp is done with the pipeline buffers
+    for (int idx = tid; idx < BM * BN; idx += THREADS) {
+      const int rr = idx % BM, cc = idx / BM, r = m0 + rr, c = n0 + cc;
+      if (ok(r, c)) cp_async8(sC + rr + cc * CLD, C + r + (long)c * ldc, true);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+  }
 #pragma unroll
   for (int i = 0; i < 8; i++) {
-    if (i + 1 < 8) load_c(i + 1, cv[(i + 1) & 1]);
-    const int r = m0 + wm + i * 8 + fr;
+    const int rr = wm + i * 8 + fr, r = m0 + rr;
 #pragma unroll
     for (int j = 0; j < 4; j++)
 #pragma unroll
       for (int h = 0; h < 2; h++) {
-        const int c = n0 + wn + j * 8 + fk * 2 + h;
+        const int cc = wn + j * 8 + fk * 2 + h, c = n0 + cc;
         if (!ok(r, c)) continue;
         double v = alpha * acc[i][j][h];
-        if (beta != 0.0) v = fma(beta, cv[i & 1][j][h], v);
+        if (beta != 0.0) v = fma(beta, sC[rr + cc * CLD], v);
         C[r + (long)c * ldc] = v;
       }
   }

@@ -603,6 +603,18 @@ void dormqr_dev(int side, int trans, int M, int N, int K, const double *A, long 
   }
 }
 
+// Factor the m x nb panel at P in leaves, each applied to the panel's
+// columns on its right (the reference's recursive panel ATL_geqrr).
+void factor_panel(int m, int nb, double *P, long lda, double *tau, double *part, double *Psum, cudaStream_t st) {
+  for (int l = 0; l < nb;) {
+    const int leaf = std::min(qr_leaf(m - l), nb - l);
+    double *L = P + l + (long)l * lda;
+    geqr2_leaf(m - l, leaf, L, lda, tau + l, st);
+    if (l + leaf < nb) leaf_apply(m - l, leaf, nb - l - leaf, L, lda, tau + l, part, Psum, st);
+    l += leaf;
+  }
+}
+
 void dgeqrf_dev(int M, int N, double *A, long lda, double *tau, cudaStream_t st) {
   const int mn = std::min(M, N);
   if (mn <= 0) return;
@@ -613,22 +625,58 @@ void dgeqrf_dev(int M, int N, double *A, long lda, double *tau, cudaStream_t st)
   double *ws = (double *)scratch(kSlotWork, sizeof(double) * need);
   double *V = ws, *G = V + (size_t)M * NBQ, *T = G + (size_t)NBQ * NBQ, *W = T + (size_t)NBQ * NBQ;
   double *part = W + 2 * (size_t)NBQ * N, *Psum = part + (size_t)QL_GRID * QL_OUT;
-  for (int j = 0; j < mn; j += NBQ) {
-    const int nb = std::min(NBQ, mn - j), m = M - j;
-    double *P = A + j + (long)j * lda;
-    // factor the panel in leaves, applying each leaf to the panel's remaining columns
-    for (int l = 0; l < nb;) {
-      const int leaf = std::min(qr_leaf(m - l), nb - l);
-      double *L = P + l + (long)l * lda;
-      geqr2_leaf(m - l, leaf, L, lda, tau + j + l, st);
-      if (l + leaf < nb) leaf_apply(m - l, leaf, nb - l - leaf, L, lda, tau + j + l, part, Psum, st);
-      l += leaf;
+  if (!lookahead_enabled() || mn <= NBQ) {
+    for (int j = 0; j < mn; j += NBQ) {
+      const int nb = std::min(NBQ, mn - j), m = M - j;
+      double *P = A + j + (long)j * lda;
+      factor_panel(m, nb, P, lda, tau + j, part, Psum, st);
+      if (j + nb < N) {
+        build_vt(m, nb, P, lda, tau + j, V, G, T, st);
+        larfb_lt(m, N - j - nb, nb, V, T, P + (long)nb * lda, lda, W, st);
+      }
     }
-    if (j + nb < N) {
-      build_vt(m, nb, P, lda, tau + j, V, G, T, st);
-      larfb_lt(m, N - j - nb, nb, V, T, P + (long)nb * lda, lda, W, st);
+    return;
+  }
+  // Look-ahead of depth one (as in getrf and potrf): panel k's block
+  // reflector updates panel k+1's columns first; the side stream factors
+  // panel k+1 while the main stream updates the columns right of it.  The
+  // side stream writes only panel k+1 (and its tau), the main stream only
+  // the columns beyond it; the main stream's V is its own copy of panel k.
+  cudaStream_t s1 = side_stream();
+  double *spart, *sPsum;
+  {
+    SideScope side;  // the side stream's own partial-sum buffers
+    spart = (double *)scratch(kSlotWork, sizeof(double) * (size_t)(QL_GRID + 1) * QL_OUT);
+    sPsum = spart + (size_t)QL_GRID * QL_OUT;
+  }
+  factor_panel(M, std::min(NBQ, mn), A, lda, tau, part, Psum, st);
+  int k = 0;
+  for (int j = 0; j < mn; j += NBQ, k++) {
+    const int nb = std::min(NBQ, mn - j), m = M - j, jn = j + nb;
+    if (jn >= N) break;
+    double *P = A + j + (long)j * lda;
+    if (k > 0) ATLB_CUDA_CHECK(cudaStreamWaitEvent(st, side_event(2 + (k & 1)), 0));  // panel k factored
+    build_vt(m, nb, P, lda, tau + j, V, G, T, st);
+    if (jn >= mn) {  // no panel after this one: columns mn..N-1 only
+      larfb_lt(m, N - jn, nb, V, T, P + (long)nb * lda, lda, W, st);
+      break;
+    }
+    const int nbn = std::min(NBQ, mn - jn), rest = N - jn - nbn;
+    larfb_lt(m, nbn, nb, V, T, P + (long)nb * lda, lda, W, st);
+    ATLB_CUDA_CHECK(cudaEventRecord(side_event(k & 1), st));
+    ATLB_CUDA_CHECK(cudaStreamWaitEvent(s1, side_event(k & 1), 0));
+    {
+      SideScope side;
+      factor_panel(M - jn, nbn, A + jn + (long)jn * lda, lda, tau + jn, spart, sPsum, s1);
+      ATLB_CUDA_CHECK(cudaEventRecord(side_event(2 + ((k + 1) & 1)), s1));
+    }
+    if (rest > 0) {
+      const int reserve = tune(kTuneLookaheadReserve);
+      GemmCtaCap cap(reserve > 0 ? std::max(1, num_sms() - reserve) : 0);
+      larfb_lt(m, rest, nb, V, T, P + (long)(nb + nbn) * lda, lda, W, st);
     }
   }
+  ATLB_CUDA_CHECK(cudaStreamWaitEvent(st, side_event(2 + (k & 1)), 0));  // join the last panel
 }
 
 }  // namespace atlb
