@@ -97,6 +97,7 @@ _SIGS = {
     "atlb_dgetrs_adjoint_dev": (_I, [_I, _I, _P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I]),
     "atlb_dgetrf_adjoint_dev": (_I, [_I, _P, _I, _P, _P, _I, _P, _I, _P, _I]),
     "atlb_dsposv": (_I, [_I, _I, _I, _P, _I, _P, _I, _P, _I, _I, _P]),
+    "atlb_mixed_krylov_steps": (_I, []),
     "atlb_dpotrf_adjoint_batched_dev": (_I, [_I, _P, _P, _P, _P, _P, _P, _P]),
     "atlb_dpotrs_adjoint_batched_dev": (_I, [_I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
 }

@@ -67,7 +67,7 @@ enum ScratchSlot {
   kSlotOzA, kSlotOzB, kSlotOzScale, kSlotBatch0, kSlotBatch1, kSlotBatch2,
   kSlotBatch3, kSlotAdj0, kSlotAdj1, kSlotAdj2, kSlotTc0, kSlotTc1, kSlotTrsmW, kSlotTrsvCtl, kSlotLaswp,
   kSlotMixedWL, kSlotMixedWU, kSlotMixedPerm, kSlotGemmSplit, kSlotPermPlan,
-  kSlotQrApply, kSlotExt0, kSlotExt1, kSlotExt2, kSlotExt3, kSlotAdjProbs,
+  kSlotQrApply, kSlotExt0, kSlotExt1, kSlotExt2, kSlotExt3, kSlotAdjProbs, kSlotKrylov, kSlotKrylovH,
   kNumSlots
 };
 

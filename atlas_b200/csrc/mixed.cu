@@ -203,6 +203,59 @@ __global__ void symmetrize_kernel(int uplo, int N, const double *__restrict__ A,
   }
 }
 
+// ---- GMRES-based refinement kernels (FP64 vectors of length N, nrhs columns
+// iterated in lockstep; the Krylov basis V holds vector i of column c at
+// V + (i * nrhs + c) * N).
+
+// Y = sum of the GEMV partials (fixed order)
+__global__ void gemv_sum_kernel(int N, int nrhs, int nchunks, const double *__restrict__ part,
+                                double *__restrict__ Y, long ldy) {
+  const int r = blockIdx.y;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int ch = 0; ch < nchunks; ch++) s += part[((long)ch * nrhs + r) * N + i];
+    Y[i + (long)r * ldy] = s;
+  }
+}
+
+// h[i * nrhs + c] = <V_i[:, c], W[:, c]> for i < gridDim.x, one CTA per (i, c)
+__global__ void __launch_bounds__(256) multidot_kernel(int N, int nrhs, const double *__restrict__ V,
+                                                       const double *__restrict__ W, double *__restrict__ h) {
+  __shared__ double red[8];
+  const int i = blockIdx.x, c = blockIdx.y;
+  const double *v = V + ((long)i * nrhs + c) * N, *w = W + (long)c * N;
+  double s = 0.0;
+  for (int r = threadIdx.x; r < N; r += 256) s = fma(v[r], w[r], s);
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int q = 0; q < 8; q++) t += red[q];
+    h[(long)i * nrhs + c] = t;
+  }
+}
+
+// X[:, c] += sgn * sum_{i < k} V_i[:, c] y[i * nrhs + c]
+__global__ void vcombine_kernel(int N, int nrhs, int k, const double *__restrict__ V, const double *__restrict__ y,
+                                double sgn, double *__restrict__ X, long ldx) {
+  const int c = blockIdx.y;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < N; r += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int i = 0; i < k; i++) s = fma(V[((long)i * nrhs + c) * N + r], y[(long)i * nrhs + c], s);
+    X[r + (long)c * ldx] += sgn * s;
+  }
+}
+
+// Vout[:, c] = W[:, c] / sqrt(nrm2[c]) (zero for a zero norm)
+__global__ void vscale_kernel(int N, int nrhs, const double *__restrict__ W, const double *__restrict__ nrm2,
+                              double *__restrict__ Vout) {
+  const int c = blockIdx.y;
+  const double q = nrm2[c] > 0.0 ? 1.0 / sqrt(nrm2[c]) : 0.0;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < N; r += gridDim.x * blockDim.x)
+    Vout[(long)c * N + r] = W[(long)c * N + r] * q;
+}
+
 bool debug_ir() {
   static int v = -1;
   if (v < 0) { const char *e = getenv("ATLAS_B200_DEBUG_IR"); v = (e && *e && *e != '0') ? 1 : 0; }
@@ -298,6 +351,123 @@ void add_s2d_dev(int M, int N, const float *S, long lds, double *X, long ldx, cu
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
 
+// Y (N x nrhs, ld N) = A X (X: N x nrhs, ld N); part as for dresid_dev
+void dgemv_dev(int N, int nrhs, const double *A, long lda, const double *X, double *Y, double *part,
+               cudaStream_t st) {
+  const int nch = cdiv(N, GV_COLS);
+  dim3 grid(cdiv(N, GV_ROWS), nch);
+  for (int r0 = 0; r0 < nrhs; r0 += 8) {
+    const int nr = std::min(8, nrhs - r0);
+    const double *Xr = X + (long)r0 * N;
+    if (nr <= 1) gemv_partial_kernel<1><<<grid, GV_ROWS, 0, st>>>(N, nr, A, lda, Xr, N, part);
+    else if (nr <= 4) gemv_partial_kernel<4><<<grid, GV_ROWS, 0, st>>>(N, nr, A, lda, Xr, N, part);
+    else gemv_partial_kernel<8><<<grid, GV_ROWS, 0, st>>>(N, nr, A, lda, Xr, N, part);
+    gemv_sum_kernel<<<dim3(std::min(cdiv(N, 256), 64), nr), 256, 0, st>>>(N, nr, nch, part, Y + (long)r0 * N, N);
+  }
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
+
+// One GMRES-IR correction (Carson & Higham, "Accelerating the solution of
+// linear systems by iterative refinement in three precisions", SIAM J. Sci.
+// Comput. 40(2), 2018; on GPUs with a tensor-core LU, Haidar, Tomov,
+// Dongarra & Higham, SC18): X += d, d from GMRES on the left-preconditioned
+// system M^-1 A d = M^-1 R, M = the low-precision factors (`correct` applies
+// M^-1 to a zeroed vector), FP64 Arnoldi with classical Gram-Schmidt
+// repeated once (CGS2), Givens rotations and the small least-squares solve on
+// the host.  Stops when every column's preconditioned residual estimate has
+// dropped by KRYLOV_TAU or after KRYLOV_M steps; returns the steps taken.
+// When u_low * kappa(A) is near or above 1, plain refinement (one M^-1 solve
+// per step) stagnates or diverges while this correction still converges.
+constexpr int KRYLOV_M = 30;
+constexpr int KRYLOV_MAX_RHS = 8;
+constexpr double KRYLOV_TAU = 1e-4;
+
+template <class Correct>
+int gmres_correct(int N, int nrhs, const double *A, long lda, const double *R, long ldr, double *X, long ldx,
+                  Correct correct, double *part, cudaStream_t st) {
+  const int m = KRYLOV_M;
+  const size_t nv = (size_t)N * nrhs;
+  double *V = (double *)scratch(kSlotKrylov, sizeof(double) * (nv * (m + 3) + (size_t)(3 * (m + 1) + m + 1) * nrhs));
+  double *Z = V + nv * (m + 1), *Wv = Z + nv;
+  double *h1 = Wv + nv, *h2 = h1 + (size_t)(m + 1) * nrhs, *nrm = h2 + (size_t)(m + 1) * nrhs;
+  double *y = nrm + nrhs;
+  double *hh = (double *)pinned(kSlotKrylovH, sizeof(double) * (size_t)(3 * (m + 1) + m + 1) * nrhs);
+  double *hh1 = hh, *hh2 = hh1 + (size_t)(m + 1) * nrhs, *hnrm = hh2 + (size_t)(m + 1) * nrhs,
+         *hy = hnrm + nrhs;
+  const dim3 vgrid(std::min(cdiv(N, 256), 148), nrhs);
+  // v0 = M^-1 R / beta
+  ATLB_CUDA_CHECK(cudaMemsetAsync(V, 0, sizeof(double) * nv, st));
+  correct(R, ldr, V, N);
+  multidot_kernel<<<dim3(1, nrhs), 256, 0, st>>>(N, nrhs, V, V, nrm);
+  vscale_kernel<<<vgrid, 256, 0, st>>>(N, nrhs, V, nrm, V);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+  ATLB_CUDA_CHECK(cudaMemcpyAsync(hnrm, nrm, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st));
+  ATLB_CUDA_CHECK(cudaStreamSynchronize(st));
+  std::vector<double> H((size_t)nrhs * (m + 1) * m, 0.0), g((size_t)nrhs * (m + 1), 0.0), cs((size_t)nrhs * m),
+      sn((size_t)nrhs * m), beta(nrhs);
+  auto Hc = [&](int c, int i, int j) -> double & { return H[((size_t)c * (m + 1) + i) * m + j]; };
+  for (int c = 0; c < nrhs; c++) {
+    beta[c] = std::sqrt(std::max(hnrm[c], 0.0));
+    g[(size_t)c * (m + 1)] = beta[c];
+  }
+  int j = 0;
+  while (j < m) {
+    const double *Vj = V + (size_t)j * nv;
+    double *Vn = V + (size_t)(j + 1) * nv;
+    dgemv_dev(N, nrhs, A, lda, Vj, Wv, part, st);                 // A v_j
+    ATLB_CUDA_CHECK(cudaMemsetAsync(Z, 0, sizeof(double) * nv, st));
+    correct(Wv, N, Z, N);                                          // M^-1 A v_j
+    multidot_kernel<<<dim3(j + 1, nrhs), 256, 0, st>>>(N, nrhs, V, Z, h1);
+    vcombine_kernel<<<vgrid, 256, 0, st>>>(N, nrhs, j + 1, V, h1, -1.0, Z, N);
+    multidot_kernel<<<dim3(j + 1, nrhs), 256, 0, st>>>(N, nrhs, V, Z, h2);
+    vcombine_kernel<<<vgrid, 256, 0, st>>>(N, nrhs, j + 1, V, h2, -1.0, Z, N);
+    multidot_kernel<<<dim3(1, nrhs), 256, 0, st>>>(N, nrhs, Z, Z, nrm);
+    vscale_kernel<<<vgrid, 256, 0, st>>>(N, nrhs, Z, nrm, Vn);
+    ATLB_CUDA_CHECK(cudaGetLastError());
+    ATLB_CUDA_CHECK(cudaMemcpyAsync(hh1, h1, sizeof(double) * (size_t)(j + 1) * nrhs, cudaMemcpyDeviceToHost, st));
+    ATLB_CUDA_CHECK(cudaMemcpyAsync(hh2, h2, sizeof(double) * (size_t)(j + 1) * nrhs, cudaMemcpyDeviceToHost, st));
+    ATLB_CUDA_CHECK(cudaMemcpyAsync(hnrm, nrm, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st));
+    ATLB_CUDA_CHECK(cudaStreamSynchronize(st));
+    bool done = true;
+    for (int c = 0; c < nrhs; c++) {
+      double *gc = g.data() + (size_t)c * (m + 1), *csc = cs.data() + (size_t)c * m, *snc = sn.data() + (size_t)c * m;
+      for (int i = 0; i <= j; i++) Hc(c, i, j) = hh1[(size_t)i * nrhs + c] + hh2[(size_t)i * nrhs + c];
+      Hc(c, j + 1, j) = std::sqrt(std::max(hnrm[c], 0.0));
+      for (int i = 0; i < j; i++) {  // previous rotations
+        const double t = csc[i] * Hc(c, i, j) + snc[i] * Hc(c, i + 1, j);
+        Hc(c, i + 1, j) = -snc[i] * Hc(c, i, j) + csc[i] * Hc(c, i + 1, j);
+        Hc(c, i, j) = t;
+      }
+      const double a = Hc(c, j, j), b = Hc(c, j + 1, j), d = std::hypot(a, b);
+      csc[j] = d > 0 ? a / d : 1.0;
+      snc[j] = d > 0 ? b / d : 0.0;
+      Hc(c, j, j) = d;
+      Hc(c, j + 1, j) = 0.0;
+      gc[j + 1] = -snc[j] * gc[j];
+      gc[j] = csc[j] * gc[j];
+      if (!(std::fabs(gc[j + 1]) <= KRYLOV_TAU * beta[c]) && std::isfinite(gc[j + 1])) done = false;
+    }
+    j++;
+    if (debug_ir()) fprintf(stderr, "atlas_b200 gmres: step %d residual estimate %.3e\n", j,
+                            std::fabs(g[j]) / std::max(beta[0], 1e-300));
+    if (done) break;
+  }
+  // y = H(0:j, 0:j)^-1 g(0:j) per column (upper triangular after the rotations)
+  for (int c = 0; c < nrhs; c++) {
+    const double *gc = g.data() + (size_t)c * (m + 1);
+    for (int i = j - 1; i >= 0; i--) {
+      double s = gc[i];
+      for (int k = i + 1; k < j; k++) s -= Hc(c, i, k) * hy[(size_t)k * nrhs + c];
+      const double dii = Hc(c, i, i);
+      hy[(size_t)i * nrhs + c] = (dii != 0.0 && std::isfinite(s)) ? s / dii : 0.0;
+    }
+  }
+  ATLB_CUDA_CHECK(cudaMemcpyAsync(y, hy, sizeof(double) * (size_t)j * nrhs, cudaMemcpyHostToDevice, st));
+  vcombine_kernel<<<vgrid, 256, 0, st>>>(N, nrhs, j, V, y, 1.0, X, ldx);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+  return j;
+}
+
 // Refinement driver shared by the solvers.  `factor(part, nrm)` factors the
 // low precision copy and returns its info; it also leaves ||A||_inf (bits of
 // the double) in *nrm, with part (N * ceil(N/256) doubles) as workspace, so
@@ -305,10 +475,21 @@ void add_s2d_dev(int M, int N, const float *S, long lds, double *X, long ldx, cu
 // `correct(R, ldr, X, ldx)` adds an
 // approximate solution of A D = R to X (R, X FP64 device); `fallback()` runs
 // the FP64 solver.  X is overwritten with the solution.
+//
+// krylov: 0 = plain refinement only; 1 = plain refinement, switching to
+// GMRES-IR corrections (gmres_correct) once a step gains less than a digit;
+// 2 = GMRES-IR corrections from the first step (BF16 factors, whose u * kappa
+// is near 1 already for well-conditioned matrices).  GMRES-IR serves up to
+// KRYLOV_MAX_RHS right-hand sides and gives up after two corrections that
+// fail to halve the backward error, or after KRYLOV_OUTER of them.
+thread_local int tl_krylov_steps = 0;
+constexpr int KRYLOV_OUTER = 12;
+
 template <class Factor, class Correct, class Fallback>
 int refine(int N, int nrhs, const double *A, long lda, const double *B, long ldb, double *X,
            long ldx, int *iter, Factor factor, Correct correct, Fallback fallback, cudaStream_t st,
-           MixedStats *stats) {
+           MixedStats *stats, int krylov) {
+  tl_krylov_steps = 0;
   const int nch = cdiv(N, GV_COLS);
   double *R = (double *)scratch(kSlotMixedR, sizeof(double) * (size_t)N * nrhs);
   double *part = (double *)scratch(kSlotMixedD, sizeof(double) * (size_t)nch * N * 8 + 64);
@@ -327,6 +508,9 @@ int refine(int N, int nrhs, const double *A, long lda, const double *B, long ldb
     for (int r = 0; r < nrhs; r++)
       ATLB_CUDA_CHECK(cudaMemsetAsync(X + (long)r * ldx, 0, sizeof(double) * N, st));
     correct(B, ldb, X, ldx);  // x0
+    bool gm = krylov == 2 && nrhs <= KRYLOV_MAX_RHS;
+    int gm_outer = 0, gm_stall = 0;
+    double prev = INFINITY;
     for (int it = 0; it <= ITERMAX; it++) {
       dresid_dev(N, nrhs, A, lda, X, ldx, B, ldb, R, N, part, red, st);
       ATLB_CUDA_CHECK(cudaMemcpyAsync(hred, red, sizeof(unsigned long long) * 3 * nrhs,
@@ -349,7 +533,16 @@ int refine(int N, int nrhs, const double *A, long lda, const double *B, long ldb
         return 0;
       }
       if (it == ITERMAX || !(worst < 1e300)) break;
-      correct(R, N, X, ldx);
+      if (!gm && krylov == 1 && nrhs <= KRYLOV_MAX_RHS && it >= 1 && worst > 0.1 * prev) gm = true;
+      if (gm && gm_outer > 0 && !(worst <= 0.5 * prev)) gm_stall++;
+      if (gm && (gm_stall >= 2 || gm_outer >= KRYLOV_OUTER)) break;
+      prev = worst;
+      if (gm) {
+        tl_krylov_steps += gmres_correct(N, nrhs, A, lda, R, N, X, ldx, correct, part, st);
+        gm_outer++;
+      } else {
+        correct(R, N, X, ldx);
+      }
     }
     *iter = -(ITERMAX + 1);
   } else {
@@ -459,7 +652,7 @@ int atlb_dsgesv_ex(int N, int NRHS, double *A, int lda, int *ipiv, double *B, in
     return info;
   };
   int info = refine(N, NRHS, dA.d, dA.ld, dB.d, dB.ld, dX.d, dX.ld, iter, factor, correct, fallback,
-                    st, nullptr);
+                    st, nullptr, prec == kPrecBF16 ? 2 : 1);
   stage_out(X, ldx, dX, N, NRHS, st);
   if (fell_back) {
     stage_out(A, lda, dA, N, N, st);
@@ -468,6 +661,8 @@ int atlb_dsgesv_ex(int N, int NRHS, double *A, int lda, int *ipiv, double *B, in
   ATLB_CUDA_CHECK(cudaStreamSynchronize(st));
   return info;
 }
+
+int atlb_mixed_krylov_steps(void) { return tl_krylov_steps; }
 
 int atlb_dsgesv(int N, int NRHS, double *A, int lda, int *ipiv, double *B, int ldb, double *X,
                 int ldx, int prec, int *iter) {
@@ -537,7 +732,7 @@ int atlb_dsposv(int Uplo, int N, int NRHS, double *A, int lda, double *B, int ld
     return info;
   };
   int info = refine(N, NRHS, Af, N, dB.d, dB.ld, dX.d, dX.ld, iter, factor, correct, fallback, st,
-                    nullptr);
+                    nullptr, prec == kPrecBF16 ? 2 : 1);
   stage_out(X, ldx, dX, N, NRHS, st);
   if (fell_back) stage_out(A, lda, dA, N, N, st);
   ATLB_CUDA_CHECK(cudaStreamSynchronize(st));

@@ -668,8 +668,9 @@ def extra_adjoints(torch, AB, dev, stream):
     return out
 
 
-def run_probe(torch, AB, what, n, acol0, b0, x, ipiv, it, hprec, hpiv, dev):
-    """One call of a path between cudaProfilerStart/Stop, after two warm-up calls."""
+def run_probe(torch, AB, what, n, acol0, b0, x, ipiv, it, hprec, hpiv, dev, trace=False):
+    """One call of a path between cudaProfilerStart/Stop, after two warm-up
+    calls; with trace, the call's kernels from a CUPTI trace instead."""
     f64 = torch.float64
     if what in ("dgemm", "ozaki"):
         g = torch.Generator(device=dev)
@@ -697,6 +698,28 @@ def run_probe(torch, AB, what, n, acol0, b0, x, ipiv, it, hprec, hpiv, dev):
         def call():
             A.copy_(acol0)
             AB.atlb_dgetrf_dev(n, n, A, n, ipiv, info)
+    elif what == "potrf":   # dpotrf (lower) of an SPD matrix of order n
+        g = torch.Generator(device=dev)
+        g.manual_seed(5)
+        gm = torch.randn(n, n, dtype=f64, device=dev, generator=g)
+        S = gm @ gm.T / n + torch.eye(n, dtype=f64, device=dev)
+        del gm
+        A = torch.empty_like(S)
+        info = torch.zeros(1, dtype=torch.int32, device=dev)
+
+        def call():
+            A.copy_(S)
+            AB.atlb_dpotrf_dev(122, n, A, n, info)
+    elif what == "geqrf":   # dgeqrf of a 2n x n Gaussian matrix
+        g = torch.Generator(device=dev)
+        g.manual_seed(5)
+        G0 = torch.randn(n, 2 * n, dtype=f64, device=dev, generator=g)   # column-major 2n x n
+        A = torch.empty_like(G0)
+        tau = torch.zeros(n, dtype=f64, device=dev)
+
+        def call():
+            A.copy_(G0)
+            AB.atlb_dgeqrf_dev(2 * n, n, A, 2 * n, tau)
     else:
         a0 = acol0.clone()
 
@@ -707,11 +730,51 @@ def run_probe(torch, AB, what, n, acol0, b0, x, ipiv, it, hprec, hpiv, dev):
     call()
     call()
     torch.cuda.synchronize()
+    if trace:
+        print(json.dumps({"probe": what, "n": n, "trace": cupti_trace(torch, call)}), flush=True)
+        return
     torch.cuda.profiler.start()
     call()
     torch.cuda.synchronize()
     torch.cuda.profiler.stop()
     print(json.dumps({"probe": what, "n": n}), flush=True)
+
+
+def cupti_trace(torch, call):
+    """One call under torch.profiler (CUPTI activity records): the span from
+    the first kernel's start to the last one's end, the time with at least one
+    kernel running, and per stream the kernels' count and device time by name
+    (the copy that resets the input included)."""
+    import re
+    from torch.profiler import profile, ProfilerActivity
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        call()
+        torch.cuda.synchronize()
+    ev = [e for e in prof.events() if e.device_type == torch.autograd.DeviceType.CUDA]
+    ivs = sorted((e.time_range.start, e.time_range.end, e.name) for e in ev)
+    if not ivs:
+        return {}
+    t0, t1 = ivs[0][0], max(e for _, e, _ in ivs)
+    busy, cur_s, cur_e = 0.0, ivs[0][0], ivs[0][1]
+    for s_, e_, _ in ivs[1:]:
+        if s_ > cur_e:
+            busy += cur_e - cur_s
+            cur_s, cur_e = s_, e_
+        else:
+            cur_e = max(cur_e, e_)
+    busy += cur_e - cur_s
+    agg = {}
+    for s_, e_, name in ivs:
+        k = re.split(r"\((?!\d)", name.replace("(anonymous namespace)::", "").replace("atlb::", "")
+                     .replace("void ", ""))[0][:70]
+        a = agg.setdefault(k, [0, 0.0])
+        a[0] += 1
+        a[1] += e_ - s_
+    top = sorted(agg.items(), key=lambda kv: -kv[1][1])
+    return {"span_us": round(t1 - t0, 1), "busy_us": round(busy, 1),
+            "kernel_us_total": round(sum(v[1] for _, v in top), 1),
+            "kernels": [{"name": k, "launches": v[0], "us": round(v[1], 1), "avg_us": round(v[1] / v[0], 2)}
+                        for k, v in top[:16]]}
 
 
 def main():
@@ -724,9 +787,12 @@ def main():
     ap.add_argument("--n", type=int, default=N_DEFAULT, help="matrix order (default 8192; smaller for profiling)")
     ap.add_argument("--skip-e2e", action="store_true", help="omit the host-buffer leg (profiling)")
     ap.add_argument("--skip-extras", action="store_true", help="only the headline and FP64 solves (profiling)")
-    ap.add_argument("--probe", choices=["dgemm", "getrf", "mixed", "ozaki", "tcgemm"],
+    ap.add_argument("--probe", choices=["dgemm", "getrf", "potrf", "geqrf", "mixed", "ozaki", "tcgemm"],
                     help="profiling aid: warm up, then run ONE call of the named path at order --n between "
                          "cudaProfilerStart/Stop (ncu --profile-from-start off) and exit")
+    ap.add_argument("--trace", action="store_true",
+                    help="with --probe: print the call's kernels (CUPTI trace: device time per kernel name, "
+                         "span, busy time) instead of bracketing it for ncu")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     n = args.n
@@ -765,7 +831,7 @@ def main():
     it = np.zeros(1, dtype=np.int32)
     _, hprec, hpiv = HEADLINE
     if args.probe:
-        return run_probe(torch, AB, args.probe, n, acol0, b0, x, ipiv, it, hprec, hpiv, dev)
+        return run_probe(torch, AB, args.probe, n, acol0, b0, x, ipiv, it, hprec, hpiv, dev, args.trace)
 
     fallbacks = [0]
 

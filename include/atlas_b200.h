@@ -262,11 +262,17 @@ int atlb_dormqr_dev(int Side, int Trans, int M, int N, int K, const double *A, i
  * success; otherwise the FP64 solver runs, A/ipiv hold its factors and *iter
  * < 0 (-3: FP32 factorization broke down, -31: no convergence).  Returns
  * info (0, > 0 singular / not positive definite, < 0 bad argument).  Host or
- * device pointers; synchronous. */
+ * device pointers; synchronous.  Refinement steps are plain (one solve with
+ * the low-precision factors) until a step gains less than a digit; from
+ * then on -- and from the first step for BF16 (prec 2) -- each step is a
+ * GMRES-IR correction: FP64 GMRES on the system preconditioned by the
+ * low-precision factors (up to 8 right-hand sides). */
 int atlb_dsgesv(int N, int NRHS, double *A, int lda, int *ipiv, double *B, int ldb, double *X,
                 int ldx, int prec, int *iter);
 int atlb_dsposv(int Uplo, int N, int NRHS, double *A, int lda, double *B, int ldb, double *X,
                 int ldx, int prec, int *iter);
+/* GMRES steps (Arnoldi vectors) of the calling thread's last mixed solve. */
+int atlb_mixed_krylov_steps(void);
 /* atlb_dsgesv with a choice of factorization: pivoting 0 = partial pivoting
  * (as atlb_dsgesv), 1 = random butterfly transformation U^T A V of the
  * matrix followed by LU without pivoting (no column-by-column pivot search;

@@ -138,3 +138,53 @@ def test_dsgesv_rbt_matrix_without_pivot_needs(gpu):
     ipiv = np.zeros(n, dtype=np.int32)
     assert AB.atlb_dsgesv_ex(n, 1, a0.copy(order="F"), n, ipiv, b0, n, x, n, 3, 1, it) == 0
     assert np.all(bwd_err(a0, x, b0) <= n * 2.0 ** -53)
+
+
+@pytest.mark.parametrize("n", [1024, 3000])
+def test_dsgesv_bf16_converges_by_gmres_ir(gpu, n):
+    """BF16 factors leave u_bf16 * kappa * growth near 1 even at kappa = 1e2,
+    where plain refinement stalls: the GMRES-IR corrections (FP64 GMRES
+    preconditioned by the BF16 factors) still reach N * 2^-53 without the FP64
+    fallback, and A and B stay unchanged."""
+    a0 = kappa_matrix(n, 1e2, 31 + n)
+    b0 = np.asfortranarray(np.random.default_rng(7).uniform(-1, 1, (n, 1)))
+    a, b = a0.copy(order="F"), b0.copy(order="F")
+    x = np.zeros((n, 1), order="F")
+    ipiv = np.zeros(n, dtype=np.int32)
+    it = np.zeros(1, dtype=np.int32)
+    assert AB.atlb_dsgesv(n, 1, a, n, ipiv, b, n, x, n, 2, it) == 0
+    assert it[0] >= 0, f"no convergence (iter={it[0]})"
+    assert AB.atlb_mixed_krylov_steps() > 0
+    assert np.all(bwd_err(a0, x, b0) <= n * 2.0 ** -53)
+    assert np.array_equal(a, a0) and np.array_equal(b, b0)
+
+
+@pytest.mark.parametrize("prec", [0, 3])
+def test_dsgesv_kappa_1e7_switches_to_gmres_ir(gpu, prec):
+    """At kappa = 1e7 (u_fp32 * kappa near 1) a plain refinement step gains
+    less than a digit; the solver then takes GMRES-IR corrections and still
+    converges without the FP64 fallback, on 3 right-hand sides at once."""
+    n, nrhs = 1500, 3
+    a0 = kappa_matrix(n, 1e7, 77 + prec)
+    b0 = np.asfortranarray(np.random.default_rng(8).uniform(-1, 1, (n, nrhs)))
+    x = np.zeros((n, nrhs), order="F")
+    ipiv = np.zeros(n, dtype=np.int32)
+    it = np.zeros(1, dtype=np.int32)
+    assert AB.atlb_dsgesv(n, nrhs, a0.copy(order="F"), n, ipiv, b0.copy(order="F"), n, x, n, prec, it) == 0
+    assert it[0] >= 0, f"no convergence (iter={it[0]})"
+    assert AB.atlb_mixed_krylov_steps() > 0
+    assert np.all(bwd_err(a0, x, b0) <= n * 2.0 ** -53)
+
+
+def test_dsposv_bf16_gmres_ir(gpu):
+    n = 1200
+    rng = np.random.default_rng(12)
+    q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    a0 = np.asfortranarray((q * np.logspace(0, -2, n)) @ q.T)
+    a0 = np.asfortranarray(0.5 * (a0 + a0.T))
+    b0 = np.asfortranarray(rng.uniform(-1, 1, (n, 2)))
+    x = np.zeros((n, 2), order="F")
+    it = np.zeros(1, dtype=np.int32)
+    assert AB.atlb_dsposv(AB.CblasLower, n, 2, a0.copy(order="F"), n, b0.copy(order="F"), n, x, n, 2, it) == 0
+    assert it[0] >= 0, f"no convergence (iter={it[0]})"
+    assert np.all(bwd_err(a0, x, b0) <= n * 2.0 ** -53)
