@@ -477,13 +477,23 @@ int gmres_correct(int N, int nrhs, const double *A, long lda, const double *R, l
 // the FP64 solver.  X is overwritten with the solution.
 //
 // krylov: 0 = plain refinement only; 1 = plain refinement, switching to
-// GMRES-IR corrections (gmres_correct) once a step gains less than a digit;
-// 2 = GMRES-IR corrections from the first step (BF16 factors, whose u * kappa
-// is near 1 already for well-conditioned matrices).  GMRES-IR serves up to
-// KRYLOV_MAX_RHS right-hand sides and gives up after two corrections that
-// fail to halve the backward error, or after KRYLOV_OUTER of them.
+// GMRES-IR corrections (gmres_correct) once a step fails to halve the
+// backward error (a plain step and a GMRES step cost about the same -- one
+// product with A, one solve with the factors -- so plain steps are kept
+// while they converge); 2 = GMRES-IR corrections from the first step.
+// GMRES-IR serves up to KRYLOV_MAX_RHS right-hand sides and gives up (FP64
+// fallback) after a correction that fails to halve the backward error, or
+// after KRYLOV_OUTER of them.
 thread_local int tl_krylov_steps = 0;
 constexpr int KRYLOV_OUTER = 12;
+
+// the refinement mode for a factorization precision: the tunable, with its
+// automatic setting (1) taking GMRES-IR from the start for BF16 factors, whose
+// u * kappa * growth is near 1 already for well-conditioned matrices
+int krylov_mode(int prec) {
+  const int k = tune(kTuneMixedKrylov);
+  return (k == 1 && prec == kPrecBF16) ? 2 : k;
+}
 
 template <class Factor, class Correct, class Fallback>
 int refine(int N, int nrhs, const double *A, long lda, const double *B, long ldb, double *X,
@@ -509,7 +519,7 @@ int refine(int N, int nrhs, const double *A, long lda, const double *B, long ldb
       ATLB_CUDA_CHECK(cudaMemsetAsync(X + (long)r * ldx, 0, sizeof(double) * N, st));
     correct(B, ldb, X, ldx);  // x0
     bool gm = krylov == 2 && nrhs <= KRYLOV_MAX_RHS;
-    int gm_outer = 0, gm_stall = 0;
+    int gm_outer = 0, gm_stall = 0;  // GMRES-IR corrections taken / that failed to halve the error
     double prev = INFINITY;
     for (int it = 0; it <= ITERMAX; it++) {
       dresid_dev(N, nrhs, A, lda, X, ldx, B, ldb, R, N, part, red, st);
@@ -533,9 +543,9 @@ int refine(int N, int nrhs, const double *A, long lda, const double *B, long ldb
         return 0;
       }
       if (it == ITERMAX || !(worst < 1e300)) break;
-      if (!gm && krylov == 1 && nrhs <= KRYLOV_MAX_RHS && it >= 1 && worst > 0.1 * prev) gm = true;
+      if (!gm && krylov == 1 && nrhs <= KRYLOV_MAX_RHS && it >= 1 && !(worst <= 0.5 * prev)) gm = true;
       if (gm && gm_outer > 0 && !(worst <= 0.5 * prev)) gm_stall++;
-      if (gm && (gm_stall >= 2 || gm_outer >= KRYLOV_OUTER)) break;
+      if (gm && (gm_stall >= 1 || gm_outer >= KRYLOV_OUTER)) break;
       prev = worst;
       if (gm) {
         tl_krylov_steps += gmres_correct(N, nrhs, A, lda, R, N, X, ldx, correct, part, st);
@@ -652,7 +662,7 @@ int atlb_dsgesv_ex(int N, int NRHS, double *A, int lda, int *ipiv, double *B, in
     return info;
   };
   int info = refine(N, NRHS, dA.d, dA.ld, dB.d, dB.ld, dX.d, dX.ld, iter, factor, correct, fallback,
-                    st, nullptr, prec == kPrecBF16 ? 2 : 1);
+                    st, nullptr, krylov_mode(prec));
   stage_out(X, ldx, dX, N, NRHS, st);
   if (fell_back) {
     stage_out(A, lda, dA, N, N, st);
@@ -732,7 +742,7 @@ int atlb_dsposv(int Uplo, int N, int NRHS, double *A, int lda, double *B, int ld
     return info;
   };
   int info = refine(N, NRHS, Af, N, dB.d, dB.ld, dX.d, dX.ld, iter, factor, correct, fallback, st,
-                    nullptr, prec == kPrecBF16 ? 2 : 1);
+                    nullptr, krylov_mode(prec));
   stage_out(X, ldx, dX, N, NRHS, st);
   if (fell_back) stage_out(A, lda, dA, N, N, st);
   ATLB_CUDA_CHECK(cudaStreamSynchronize(st));

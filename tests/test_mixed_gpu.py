@@ -160,20 +160,29 @@ def test_dsgesv_bf16_converges_by_gmres_ir(gpu, n):
 
 
 @pytest.mark.parametrize("prec", [0, 3])
-def test_dsgesv_kappa_1e7_switches_to_gmres_ir(gpu, prec):
-    """At kappa = 1e7 (u_fp32 * kappa near 1) a plain refinement step gains
-    less than a digit; the solver then takes GMRES-IR corrections and still
-    converges without the FP64 fallback, on 3 right-hand sides at once."""
+def test_dsgesv_kappa_1e6_gmres_ir_corrections(gpu, prec):
+    """mixed_krylov = 2: every refinement step is a GMRES-IR correction (FP64
+    GMRES preconditioned by the FP32 factors); at kappa = 1e6 it converges on
+    3 right-hand sides at once, in fewer outer steps than plain refinement
+    (mixed_krylov = 0) takes, to the same criterion."""
     n, nrhs = 1500, 3
-    a0 = kappa_matrix(n, 1e7, 77 + prec)
+    a0 = kappa_matrix(n, 1e6, 77 + prec)
     b0 = np.asfortranarray(np.random.default_rng(8).uniform(-1, 1, (n, nrhs)))
-    x = np.zeros((n, nrhs), order="F")
-    ipiv = np.zeros(n, dtype=np.int32)
-    it = np.zeros(1, dtype=np.int32)
-    assert AB.atlb_dsgesv(n, nrhs, a0.copy(order="F"), n, ipiv, b0.copy(order="F"), n, x, n, prec, it) == 0
-    assert it[0] >= 0, f"no convergence (iter={it[0]})"
-    assert AB.atlb_mixed_krylov_steps() > 0
-    assert np.all(bwd_err(a0, x, b0) <= n * 2.0 ** -53)
+    steps = {}
+    try:
+        for mode in (2, 0):
+            assert AB.atlb_tune_set("mixed_krylov", mode) == mode
+            x = np.zeros((n, nrhs), order="F")
+            ipiv = np.zeros(n, dtype=np.int32)
+            it = np.zeros(1, dtype=np.int32)
+            assert AB.atlb_dsgesv(n, nrhs, a0.copy(order="F"), n, ipiv, b0.copy(order="F"), n, x, n, prec, it) == 0
+            assert it[0] >= 0, f"mode {mode}: no convergence (iter={it[0]})"
+            assert np.all(bwd_err(a0, x, b0) <= n * 2.0 ** -53)
+            steps[mode] = (int(it[0]), AB.atlb_mixed_krylov_steps())
+    finally:
+        AB.atlb_tune_set("mixed_krylov", 1)
+    assert steps[2][1] > 0 and steps[0][1] == 0
+    assert steps[2][0] <= steps[0][0]
 
 
 def test_dsposv_bf16_gmres_ir(gpu):

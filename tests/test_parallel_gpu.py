@@ -54,3 +54,31 @@ def test_sharded_posv_batched_one_rank(gpu):
         x = Bs[i].t()
         r = (A0[i] @ x - B0[i].t()).abs().max().item()
         assert r <= 1e-10 * A0[i].abs().max().item() * max(1.0, x.abs().max().item()), (i, r)
+
+
+@pytest.mark.parametrize("world", [2, 3, 4])
+@pytest.mark.parametrize("slices", [0, 7])
+def test_column_slabs_through_the_gpu_kernels(gpu, world, slices):
+    """Every rank's slab of a sharded DGEMM, run one after another on this GPU
+    through the GEMM each rank would call (DMMA or Ozaki), assembles the full
+    product: the slab offsets, widths and leading dimensions are right for
+    world sizes the pool cannot give as separate GPUs."""
+    import torch
+    import atlas_b200 as AB
+    m, n, k = 257, 1000, 300
+    g = torch.Generator(device="cuda")
+    g.manual_seed(11 + world)
+    A = torch.rand(m, k, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    B = torch.rand(k, n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    C = torch.rand(m, n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    a_store = A.t().contiguous()
+    out = C.clone()
+    for r, (s, w) in enumerate(PAR.column_slabs(n, world)):
+        b_slab = B[:, s:s + w].t().contiguous()
+        c_slab = C[:, s:s + w].t().contiguous()
+        PAR._default_gemm(111, 111, m, w, k, 0.5, a_store, m, b_slab, k, -1.0, c_slab, m, slices=slices)
+        assert AB.atlb_sync() == 0
+        out[:, s:s + w] = c_slab.t()
+    ref = 0.5 * A @ B - C
+    err = ((out - ref).abs().max() / ref.abs().max()).item()
+    assert err < (1e-14 if slices == 0 else 1e-12), err
