@@ -19,32 +19,35 @@ namespace {
 
 constexpr int BM = 128, BN = 128, BK = 16, THREADS = 256, STAGES = 4, PAD = 4;
 
-// Shared-memory layout of one operand tile.  "o" is the outer index (m for A,
-// n for B), "k" the reduction index.  KC = the operand is k-contiguous in
-// global memory (A transposed, B not transposed); otherwise o-contiguous.
-template <bool KC> struct Lay;
-template <> struct Lay<false> {
-  static constexpr int LD = BM + PAD;  // 132 doubles: conflict-free fragments
+// Shared-memory layout of one operand tile of BO (outer) x BK.  "o" is the
+// outer index (m for A, n for B), "k" the reduction index.  KC = the operand
+// is k-contiguous in global memory (A transposed, B not transposed);
+// otherwise o-contiguous.
+template <bool KC, int BO> struct Lay;
+template <int BO> struct Lay<false, BO> {
+  static constexpr int LD = BO + PAD;  // 132 / 68 doubles (4 mod 16): conflict-free fragments
   static constexpr int SIZE = BK * LD;
   __device__ static __forceinline__ int at(int o, int k) { return k * LD + o; }
 };
-template <> struct Lay<true> {
+template <int BO> struct Lay<true, BO> {
   static constexpr int LD = BK + PAD;  // 20 doubles
-  static constexpr int SIZE = BM * LD;
+  static constexpr int SIZE = BO * LD;
   __device__ static __forceinline__ int at(int o, int k) { return o * LD + k; }
 };
 
-// Issue the cp.async copies of one BMxBK tile (o0.., k0..) of an operand.
-template <bool KC, int VEC>
+// Issue the cp.async copies of one BO x BK tile (o0.., k0..) of an operand.
+template <bool KC, int VEC, int BO>
 __device__ __forceinline__ void load_tile(double *s, const double *X, long ld, int o0, int k0,
                                           int O, int K, int tid) {
+  using L = Lay<KC, BO>;
+  constexpr int N16 = BO * BK / 2 / THREADS, N8 = BO * BK / THREADS;  // copies per thread
   if (!KC) {
     if (VEC == 2) {
 #pragma unroll
-      for (int i = 0; i < 4; i++) {
-        int c = tid + THREADS * i, k = c >> 6, o = (c & 63) * 2;
+      for (int i = 0; i < N16; i++) {
+        int c = tid + THREADS * i, k = c / (BO / 2), o = (c % (BO / 2)) * 2;
         int go = o0 + o, gk = k0 + k;
-        double *d = s + Lay<false>::at(o, k);
+        double *d = s + L::at(o, k);
         const double *g = X + go + (long)gk * ld;
         if (gk < K && go + 1 < O) cp_async16(d, g, true);
         else {
@@ -55,20 +58,20 @@ __device__ __forceinline__ void load_tile(double *s, const double *X, long ld, i
       }
     } else {
 #pragma unroll
-      for (int i = 0; i < 8; i++) {
-        int c = tid + THREADS * i, k = c >> 7, o = c & 127;
+      for (int i = 0; i < N8; i++) {
+        int c = tid + THREADS * i, k = c / BO, o = c % BO;
         int go = o0 + o, gk = k0 + k;
         bool p = gk < K && go < O;
-        cp_async8(s + Lay<false>::at(o, k), p ? X + go + (long)gk * ld : X, p);
+        cp_async8(s + L::at(o, k), p ? X + go + (long)gk * ld : X, p);
       }
     }
   } else {
     if (VEC == 2) {
 #pragma unroll
-      for (int i = 0; i < 4; i++) {
+      for (int i = 0; i < N16; i++) {
         int c = tid + THREADS * i, o = c >> 3, k = (c & 7) * 2;
         int go = o0 + o, gk = k0 + k;
-        double *d = s + Lay<true>::at(o, k);
+        double *d = s + L::at(o, k);
         const double *g = X + gk + (long)go * ld;
         if (go < O && gk + 1 < K) cp_async16(d, g, true);
         else {
@@ -79,15 +82,31 @@ __device__ __forceinline__ void load_tile(double *s, const double *X, long ld, i
       }
     } else {
 #pragma unroll
-      for (int i = 0; i < 8; i++) {
+      for (int i = 0; i < N8; i++) {
         int c = tid + THREADS * i, o = c >> 4, k = c & 15;
         int go = o0 + o, gk = k0 + k;
         bool p = go < O && gk < K;
-        cp_async8(s + Lay<true>::at(o, k), p ? X + gk + (long)go * ld : X, p);
+        cp_async8(s + L::at(o, k), p ? X + gk + (long)go * ld : X, p);
       }
     }
   }
 }
+
+// Tile shapes.  BNT = 128: 128 x 128 tiles, 4 stages, one CTA per SM (the
+// long-K GEMMs).  BNT = 64: 128 x 64 tiles, 3 stages, two CTAs per SM, so
+// that one CTA's epilogue (the old C tile in and the new one out) overlaps
+// the other's main loop -- the short-K trailing updates of the
+// factorizations (K = 128..256), where a 128 x 128 tile spends a large part
+// of its time in the epilogue.
+template <int BNT> struct TileCfg {
+  static constexpr int STG = BNT == 128 ? STAGES : 3;
+  static constexpr int MINB = BNT == 128 ? 1 : 2;
+  static constexpr int WARPS_N = BNT / 32, WARPS_M = 8 / WARPS_N;
+  static constexpr int WMT = BM / WARPS_M, MI = WMT / 8;  // warp tile: WMT x 32 = MI x 4 fragments
+  template <bool TA, bool TB>
+  static constexpr int smem_doubles() { return STG * (Lay<TA, BM>::SIZE + Lay<!TB, BNT>::SIZE); }
+};
+constexpr int SMALL_K = 256;  // K up to this uses the 128 x 64 tiles
 
 __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
   asm volatile(
@@ -96,60 +115,62 @@ __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
       : "d"(a), "d"(b));
 }
 
-// One 128x128 tile of C = alpha*op(A)*op(B) + beta*C (column-major) at
+// One BM x BNT tile of C = alpha*op(A)*op(B) + beta*C (column-major) at
 // (m0, n0).  tri: 0 full, 1 lower (store row >= col), 2 upper (row <= col).
-template <bool TA, bool TB, int VEC>
+template <bool TA, bool TB, int VEC, int BNT = BN>
 __device__ __forceinline__ void dgemm_tile(int M, int N, int K, double alpha, const double *__restrict__ A,
                                            long lda, const double *__restrict__ B, long ldb, double beta,
                                            double *__restrict__ C, long ldc, int tri, int m0, int n0,
                                            double *smem) {
-  using LA = Lay<TA>;   // A k-contiguous when transposed
-  using LB = Lay<!TB>;  // B k-contiguous when not transposed
+  using CF = TileCfg<BNT>;
+  constexpr int STG = CF::STG, MI = CF::MI;
+  using LA = Lay<TA, BM>;     // A k-contiguous when transposed
+  using LB = Lay<!TB, BNT>;   // B k-contiguous when not transposed
   double *sA = smem;
-  double *sB = smem + STAGES * LA::SIZE;
+  double *sB = smem + STG * LA::SIZE;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = (warp & 1) * 64, wn = (warp >> 1) * 32;
+  const int wm = (warp % CF::WARPS_M) * CF::WMT, wn = (warp / CF::WARPS_M) * 32;
 
-  double acc[8][4][2];
+  double acc[MI][4][2];
 #pragma unroll
-  for (int i = 0; i < 8; i++)
+  for (int i = 0; i < MI; i++)
 #pragma unroll
     for (int j = 0; j < 4; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
 
   const int KT = (K + BK - 1) / BK;
 #pragma unroll
-  for (int s = 0; s < STAGES - 1; s++) {
+  for (int s = 0; s < STG - 1; s++) {
     if (s < KT) {
-      load_tile<TA, VEC>(sA + s * LA::SIZE, A, lda, m0, s * BK, M, K, tid);
-      load_tile<!TB, VEC>(sB + s * LB::SIZE, B, ldb, n0, s * BK, N, K, tid);
+      load_tile<TA, VEC, BM>(sA + s * LA::SIZE, A, lda, m0, s * BK, M, K, tid);
+      load_tile<!TB, VEC, BNT>(sB + s * LB::SIZE, B, ldb, n0, s * BK, N, K, tid);
     }
     cp_async_commit();
   }
 
   const int fr = lane >> 2, fk = lane & 3;
   for (int kt = 0; kt < KT; kt++) {
-    cp_async_wait<STAGES - 2>();
+    cp_async_wait<STG - 2>();
     __syncthreads();
     {
-      int nk = kt + STAGES - 1;
+      int nk = kt + STG - 1;
       if (nk < KT) {
-        int st = nk % STAGES;
-        load_tile<TA, VEC>(sA + st * LA::SIZE, A, lda, m0, nk * BK, M, K, tid);
-        load_tile<!TB, VEC>(sB + st * LB::SIZE, B, ldb, n0, nk * BK, N, K, tid);
+        int st = nk % STG;
+        load_tile<TA, VEC, BM>(sA + st * LA::SIZE, A, lda, m0, nk * BK, M, K, tid);
+        load_tile<!TB, VEC, BNT>(sB + st * LB::SIZE, B, ldb, n0, nk * BK, N, K, tid);
       }
       cp_async_commit();
     }
-    const double *a_s = sA + (kt % STAGES) * LA::SIZE;
-    const double *b_s = sB + (kt % STAGES) * LB::SIZE;
+    const double *a_s = sA + (kt % STG) * LA::SIZE;
+    const double *b_s = sB + (kt % STG) * LB::SIZE;
 #pragma unroll
     for (int kk = 0; kk < BK; kk += 4) {
-      double a[8], b[4];
+      double a[MI], b[4];
 #pragma unroll
-      for (int i = 0; i < 8; i++) a[i] = a_s[LA::at(wm + i * 8 + fr, kk + fk)];
+      for (int i = 0; i < MI; i++) a[i] = a_s[LA::at(wm + i * 8 + fr, kk + fk)];
 #pragma unroll
       for (int j = 0; j < 4; j++) b[j] = b_s[LB::at(wn + j * 8 + fr, kk + fk)];
 #pragma unroll
-      for (int i = 0; i < 8; i++)
+      for (int i = 0; i < MI; i++)
 #pragma unroll
         for (int j = 0; j < 4; j++) dmma(acc[i][j], a[i], b[j]);
     }
@@ -163,12 +184,12 @@ __device__ __forceinline__ void dgemm_tile(int M, int N, int K, double alpha, co
   auto ok = [&](int r, int c) {
     return r < M && c < N && !(tri == 1 && r < c) && !(tri == 2 && r > c);
   };
-  constexpr int CLD = BM + 4;  // staged C: column-major, ld CLD (fits the STAGES pipeline buffers)
-  static_assert(BN * CLD <= STAGES * (Lay<false>::SIZE + Lay<false>::SIZE), "C tile does not fit");
+  constexpr int CLD = BM + 4;  // staged C: column-major, ld CLD (fits the pipeline buffers)
+  static_assert(BNT * CLD <= STG * (Lay<false, BM>::SIZE + Lay<false, BNT>::SIZE), "C tile does not fit");
   double *sC = smem;
   if (beta != 0.0) {
     __syncthreads();  // every warp is done with the pipeline buffers
-    for (int idx = tid; idx < BM * BN; idx += THREADS) {
+    for (int idx = tid; idx < BM * BNT; idx += THREADS) {
       const int rr = idx % BM, cc = idx / BM, r = m0 + rr, c = n0 + cc;
       if (ok(r, c)) cp_async8(sC + rr + cc * CLD, C + r + (long)c * ldc, true);
     }
@@ -177,7 +198,7 @@ __device__ __forceinline__ void dgemm_tile(int M, int N, int K, double alpha, co
     __syncthreads();
   }
 #pragma unroll
-  for (int i = 0; i < 8; i++) {
+  for (int i = 0; i < MI; i++) {
     const int rr = wm + i * 8 + fr, r = m0 + rr;
 #pragma unroll
     for (int j = 0; j < 4; j++)
@@ -192,22 +213,22 @@ __device__ __forceinline__ void dgemm_tile(int M, int N, int K, double alpha, co
   }
 }
 
-template <bool TA, bool TB, int VEC>
-__global__ void __launch_bounds__(THREADS, 1)
+template <bool TA, bool TB, int VEC, int BNT>
+__global__ void __launch_bounds__(THREADS, TileCfg<BNT>::MINB)
 dgemm_dmma_kernel(int M, int N, int K, double alpha, const double *__restrict__ A, long lda,
                   const double *__restrict__ B, long ldb, double beta, double *__restrict__ C,
                   long ldc, int tri, int G) {
   extern __shared__ __align__(16) double smem[];
-  const int tiles_m = (M + BM - 1) / BM, tiles_n = (N + BN - 1) / BN;
+  const int tiles_m = (M + BM - 1) / BM, tiles_n = (N + BNT - 1) / BNT;
   // grouped rasterisation: G tile-rows share B panels in L2
   const int bid = blockIdx.x;
   const int per_group = G * tiles_n, group = bid / per_group;
   const int first_m = group * G, gsz = min(tiles_m - first_m, G);
   const int tm = first_m + (bid % per_group) % gsz, tn = (bid % per_group) / gsz;
-  const int m0 = tm * BM, n0 = tn * BN;
+  const int m0 = tm * BM, n0 = tn * BNT;
   if (tri == 1 && m0 + BM - 1 < n0) return;
-  if (tri == 2 && m0 > n0 + BN - 1) return;
-  dgemm_tile<TA, TB, VEC>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, tri, m0, n0, smem);
+  if (tri == 2 && m0 > n0 + BNT - 1) return;
+  dgemm_tile<TA, TB, VEC, BNT>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, tri, m0, n0, smem);
 }
 
 // The same GEMM on a capped number of CTAs, each walking tiles t, t + grid,
@@ -328,11 +349,17 @@ int splitk_count(int tiles, int K, int nsm) {
 template <bool TA, bool TB, int VEC>
 void launch(int M, int N, int K, double alpha, const double *A, long lda, const double *B,
             long ldb, double beta, double *C, long ldc, int tri, cudaStream_t st) {
-  constexpr int smem = STAGES * (Lay<TA>::SIZE + Lay<!TB>::SIZE) * (int)sizeof(double);
+  constexpr int smem = TileCfg<BN>::template smem_doubles<TA, TB>() * (int)sizeof(double);
+  constexpr int smem_s = TileCfg<64>::template smem_doubles<TA, TB>() * (int)sizeof(double);
   static bool configured = false;
   if (!configured) {
-    ATLB_CUDA_CHECK(cudaFuncSetAttribute(dgemm_dmma_kernel<TA, TB, VEC>,
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(dgemm_dmma_kernel<TA, TB, VEC, BN>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(dgemm_dmma_kernel<TA, TB, VEC, 64>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem_s));
+    // the largest shared-memory carveout, so that two of these CTAs fit on an SM
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(dgemm_dmma_kernel<TA, TB, VEC, 64>,
+                                         cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     configured = true;
   }
   int tiles = cdiv(M, BM) * cdiv(N, BN);
@@ -372,8 +399,13 @@ void launch(int M, int N, int K, double alpha, const double *A, long lda, const 
     ATLB_CUDA_CHECK(cudaGetLastError());
     return;
   }
-  dgemm_dmma_kernel<TA, TB, VEC><<<tiles, THREADS, smem, st>>>(M, N, K, alpha, A, lda, B, ldb,
-                                                              beta, C, ldc, tri, tune(kTuneGemmGroup));
+  if (K <= SMALL_K) {
+    dgemm_dmma_kernel<TA, TB, VEC, 64><<<cdiv(M, BM) * cdiv(N, 64), THREADS, smem_s, st>>>(
+        M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, tri, tune(kTuneGemmGroup));
+  } else {
+    dgemm_dmma_kernel<TA, TB, VEC, BN><<<tiles, THREADS, smem, st>>>(M, N, K, alpha, A, lda, B, ldb,
+                                                                     beta, C, ldc, tri, tune(kTuneGemmGroup));
+  }
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
 
@@ -409,7 +441,7 @@ namespace {
 template <bool TA, bool TB, int VEC>
 void launch_grouped(const GemmProb *probs, const int *order, const int *tile_start, int count,
                     int *next, cudaStream_t st) {
-  constexpr int smem = STAGES * (Lay<TA>::SIZE + Lay<!TB>::SIZE) * (int)sizeof(double);
+  constexpr int smem = TileCfg<BN>::template smem_doubles<TA, TB>() * (int)sizeof(double);
   static bool configured = false;
   if (!configured) {
     ATLB_CUDA_CHECK(cudaFuncSetAttribute(dgemm_grouped_kernel<TA, TB, VEC>,

@@ -29,7 +29,7 @@ namespace atlb {
 namespace {
 
 constexpr int QT = 512;
-constexpr int NBQ_MAX = 128;  // largest outer panel width (the trailing update's K)
+constexpr int NBQ_MAX = 128;  // widest panel factored in one piece (wider panels: two halves)
 
 template <int NB>
 struct QPub {
@@ -281,7 +281,7 @@ __global__ void extract_v_kernel(int M, int k, const double *P, long ldp, double
   }
 }
 
-// T (k x k upper, ld k, k <= NBQ_MAX) of the block reflector
+// T (k x k upper, ld ldt, k <= NBQ_MAX) of the block reflector
 // H(0) H(1) ... H(k-1) = I - V T V^T, from G = V^T V and tau.  ATL_larft's
 // column recurrence T(0:i,i) = -tau_i T(0:i,0:i) G(0:i,i), T(i,i) = tau_i
 // runs on the 16-column diagonal blocks (one warp each, all at once); the
@@ -290,14 +290,15 @@ __global__ void extract_v_kernel(int M, int k, const double *P, long ldp, double
 // T12 = -T1 G12 T2 (two small products in shared memory per level).
 // G's strictly upper part is overwritten in place by T's.
 constexpr int LFT_LD = NBQ_MAX + 1;
-__global__ void __launch_bounds__(256) larft_kernel(int k, const double *G, const double *tau, double *T) {
+__global__ void __launch_bounds__(256) larft_kernel(int k, const double *G, long ldg, const double *tau, double *T,
+                                                    long ldt) {
   extern __shared__ double lft_smem[];
   double *S = lft_smem;                      // k x k, ld LFT_LD: G, then T
   double *W = lft_smem + NBQ_MAX * LFT_LD;   // products G12 T2 of one level (<= NBQ_MAX^2 / 4 doubles)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int idx = tid; idx < k * k; idx += 256) {
     const int r = idx % k, c = idx / k;
-    S[r + c * LFT_LD] = r < c ? G[r + (long)c * k] : 0.0;
+    S[r + c * LFT_LD] = r < c ? G[r + (long)c * ldg] : 0.0;
   }
   __syncthreads();
   for (int b = warp; b * 16 < k; b += 8) {   // diagonal blocks by the recurrence
@@ -344,7 +345,7 @@ __global__ void __launch_bounds__(256) larft_kernel(int k, const double *G, cons
   }
   for (int idx = tid; idx < k * k; idx += 256) {
     const int r = idx % k, c = idx / k;
-    T[idx] = r <= c ? S[r + c * LFT_LD] : 0.0;
+    T[r + (long)c * ldt] = r <= c ? S[r + c * LFT_LD] : 0.0;
   }
 }
 
@@ -538,8 +539,13 @@ void larfb_lt(int m, int n, int k, const double *V, const double *T, double *C, 
   dgemm_dev(kNoTrans, kNoTrans, m, n, k, -1.0, V, m, W2, k, 1.0, C, ldc, st);
 }
 
+// V (m x k, explicit unit lower trapezoid of the factored panel at P),
+// G = V^T V and T (k x k, ld k) of its block reflector.  k <= NBQ_MAX: one
+// larft_kernel; k <= 2 NBQ_MAX (a panel of two halves): T of each half by
+// larft_kernel, then T12 = -T1 (G12 T2) by two GEMMs (the same merge
+// identity as inside larft_kernel), tmp holding G12 T2 (NBQ_MAX^2 doubles).
 void build_vt(int m, int k, const double *P, long ldp, const double *tau, double *V, double *G,
-              double *T, cudaStream_t st) {
+              double *T, double *tmp, cudaStream_t st) {
   long tot = (long)m * k;
   extract_v_kernel<<<(int)std::min<long>((tot + 255) / 256, 8192), 256, 0, st>>>(m, k, P, ldp, V);
   ATLB_CUDA_CHECK(cudaGetLastError());
@@ -550,8 +556,19 @@ void build_vt(int m, int k, const double *P, long ldp, const double *tau, double
                                          (int)larft_smem_bytes()));
     cfg = true;
   }
-  larft_kernel<<<1, 256, larft_smem_bytes(), st>>>(k, G, tau, T);
+  if (k <= NBQ_MAX) {
+    larft_kernel<<<1, 256, larft_smem_bytes(), st>>>(k, G, k, tau, T, k);
+    ATLB_CUDA_CHECK(cudaGetLastError());
+    return;
+  }
+  const int k1 = NBQ_MAX, k2 = k - k1;
+  double *T2 = T + k1 + (long)k1 * k;
+  larft_kernel<<<1, 256, larft_smem_bytes(), st>>>(k1, G, k, tau, T, k);
+  larft_kernel<<<1, 256, larft_smem_bytes(), st>>>(k2, G + k1 + (long)k1 * k, k, tau + k1, T2, k);
   ATLB_CUDA_CHECK(cudaGetLastError());
+  ATLB_CUDA_CHECK(cudaMemset2DAsync(T + k1, sizeof(double) * k, 0, sizeof(double) * k2, k1, st));  // T21 = 0
+  dgemm_dev(kNoTrans, kNoTrans, k1, k2, k2, 1.0, G + (long)k1 * k, k, T2, k, 0.0, tmp, k1, st);
+  dgemm_dev(kNoTrans, kNoTrans, k1, k2, k1, -1.0, T, k, tmp, k1, 0.0, T + (long)k1 * k, k, st);
 }
 
 // Apply the block reflector H = I - V T V^T (V explicit, len x k) or its
@@ -587,9 +604,10 @@ void dormqr_dev(int side, int trans, int M, int N, int K, const double *A, long 
   const int NBQ = tune(kTuneQrNB);
   const int nq = side == kLeft ? M : N;   // order of Q
   const int other = side == kLeft ? N : M;
-  size_t need = (size_t)nq * NBQ + 2 * (size_t)NBQ * NBQ + 2 * (size_t)NBQ * other;
+  size_t need = (size_t)nq * NBQ + 2 * (size_t)NBQ * NBQ + 2 * (size_t)NBQ * other + (size_t)NBQ_MAX * NBQ_MAX;
   double *ws = (double *)scratch(kSlotQrApply, sizeof(double) * need);
   double *V = ws, *G = V + (size_t)nq * NBQ, *T = G + (size_t)NBQ * NBQ, *W = T + (size_t)NBQ * NBQ;
+  double *tmp = W + 2 * (size_t)NBQ * other;
   const int nblk = cdiv(K, NBQ);
   // Q C = H0 (H1 (... C)): last block first; Q^T C: first block first (Left).
   // C Q = ((C H0) H1) ...: first block first; C Q^T: last block first (Right).
@@ -597,20 +615,53 @@ void dormqr_dev(int side, int trans, int M, int N, int K, const double *A, long 
   for (int t = 0; t < nblk; t++) {
     const int b = forward ? t : nblk - 1 - t;
     const int j = b * NBQ, kb = std::min(NBQ, K - j), len = nq - j;
-    build_vt(len, kb, A + j + (long)j * lda, lda, tau + j, V, G, T, st);
+    build_vt(len, kb, A + j + (long)j * lda, lda, tau + j, V, G, T, tmp, st);
     if (side == kLeft) larfb_gen(kLeft, trans, len, other, kb, V, T, C + j, ldc, W, st);
     else larfb_gen(kRight, trans, len, other, kb, V, T, C + (long)j * ldc, ldc, W, st);
   }
 }
 
-// Factor the m x nb panel at P in leaves, each applied to the panel's
-// columns on its right (the reference's recursive panel ATL_geqrr).
-void factor_panel(int m, int nb, double *P, long lda, double *tau, double *part, double *Psum, cudaStream_t st) {
+// Workspace of one stream's share of the factorization: V (M x NBQ), G and
+// T (NBQ x NBQ), W (2 x NBQ x ncol), tmp (NBQ_MAX^2), the leaf passes'
+// partial sums (QL_GRID x QL_OUT) and their total (QL_OUT).
+struct QrWork {
+  double *V, *G, *T, *W, *tmp, *part, *Psum;
+};
+size_t qr_work_doubles(int M, int NBQ, int ncol) {
+  return (size_t)M * NBQ + 2 * (size_t)NBQ * NBQ + 2 * (size_t)NBQ * ncol + (size_t)NBQ_MAX * NBQ_MAX +
+         (size_t)(QL_GRID + 1) * QL_OUT;
+}
+QrWork qr_work(double *ws, int M, int NBQ, int ncol) {
+  QrWork w;
+  w.V = ws;
+  w.G = w.V + (size_t)M * NBQ;
+  w.T = w.G + (size_t)NBQ * NBQ;
+  w.W = w.T + (size_t)NBQ * NBQ;
+  w.tmp = w.W + 2 * (size_t)NBQ * ncol;
+  w.part = w.tmp + (size_t)NBQ_MAX * NBQ_MAX;
+  w.Psum = w.part + (size_t)QL_GRID * QL_OUT;
+  return w;
+}
+
+// Factor the m x nb panel at P.  Up to NBQ_MAX columns: leaves, each applied
+// to the panel's columns on its right (the reference's recursive panel
+// ATL_geqrr).  Wider (up to 2 NBQ_MAX): the left half so, its block
+// reflector applied to the right half (larfb, K = NBQ_MAX), then the right
+// half -- one more level of the same recursion.
+void factor_panel(int m, int nb, double *P, long lda, double *tau, const QrWork &w, cudaStream_t st) {
+  if (nb > NBQ_MAX) {
+    const int h = NBQ_MAX;
+    factor_panel(m, h, P, lda, tau, w, st);
+    build_vt(m, h, P, lda, tau, w.V, w.G, w.T, w.tmp, st);
+    larfb_lt(m, nb - h, h, w.V, w.T, P + (long)h * lda, lda, w.W, st);
+    factor_panel(m - h, nb - h, P + h + (long)h * lda, lda, tau + h, w, st);
+    return;
+  }
   for (int l = 0; l < nb;) {
     const int leaf = std::min(qr_leaf(m - l), nb - l);
     double *L = P + l + (long)l * lda;
     geqr2_leaf(m - l, leaf, L, lda, tau + l, st);
-    if (l + leaf < nb) leaf_apply(m - l, leaf, nb - l - leaf, L, lda, tau + l, part, Psum, st);
+    if (l + leaf < nb) leaf_apply(m - l, leaf, nb - l - leaf, L, lda, tau + l, w.part, w.Psum, st);
     l += leaf;
   }
 }
@@ -618,21 +669,17 @@ void factor_panel(int m, int nb, double *P, long lda, double *tau, double *part,
 void dgeqrf_dev(int M, int N, double *A, long lda, double *tau, cudaStream_t st) {
   const int mn = std::min(M, N);
   if (mn <= 0) return;
-  const int NBQ = tune(kTuneQrNB);  // the outer panel width (ATL_ilaenv's NB, tuned)
-  // workspace: V (M x NBQ), G and T (NBQ x NBQ each), W (2 x NBQ x N), the
-  // leaf passes' partial sums (QL_GRID x QL_OUT) and their total (QL_OUT)
-  size_t need = (size_t)M * NBQ + 2 * (size_t)NBQ * NBQ + 2 * (size_t)NBQ * N + (size_t)(QL_GRID + 1) * QL_OUT;
-  double *ws = (double *)scratch(kSlotWork, sizeof(double) * need);
-  double *V = ws, *G = V + (size_t)M * NBQ, *T = G + (size_t)NBQ * NBQ, *W = T + (size_t)NBQ * NBQ;
-  double *part = W + 2 * (size_t)NBQ * N, *Psum = part + (size_t)QL_GRID * QL_OUT;
+  const int NBQ = tune(kTuneQrNB);  // the outer panel width (ATL_ilaenv's NB, tuned; <= 2 NBQ_MAX)
+  double *ws = (double *)scratch(kSlotWork, sizeof(double) * qr_work_doubles(M, NBQ, N));
+  const QrWork w = qr_work(ws, M, NBQ, N);
   if (!lookahead_enabled() || mn <= NBQ) {
     for (int j = 0; j < mn; j += NBQ) {
       const int nb = std::min(NBQ, mn - j), m = M - j;
       double *P = A + j + (long)j * lda;
-      factor_panel(m, nb, P, lda, tau + j, part, Psum, st);
+      factor_panel(m, nb, P, lda, tau + j, w, st);
       if (j + nb < N) {
-        build_vt(m, nb, P, lda, tau + j, V, G, T, st);
-        larfb_lt(m, N - j - nb, nb, V, T, P + (long)nb * lda, lda, W, st);
+        build_vt(m, nb, P, lda, tau + j, w.V, w.G, w.T, w.tmp, st);
+        larfb_lt(m, N - j - nb, nb, w.V, w.T, P + (long)nb * lda, lda, w.W, st);
       }
     }
     return;
@@ -641,39 +688,40 @@ void dgeqrf_dev(int M, int N, double *A, long lda, double *tau, cudaStream_t st)
   // reflector updates panel k+1's columns first; the side stream factors
   // panel k+1 while the main stream updates the columns right of it.  The
   // side stream writes only panel k+1 (and its tau), the main stream only
-  // the columns beyond it; the main stream's V is its own copy of panel k.
+  // the columns beyond it; the main stream's V is its own copy of panel k,
+  // and the side stream has its own workspace (SideScope).
   cudaStream_t s1 = side_stream();
-  double *spart, *sPsum;
+  QrWork sw;
   {
-    SideScope side;  // the side stream's own partial-sum buffers
-    spart = (double *)scratch(kSlotWork, sizeof(double) * (size_t)(QL_GRID + 1) * QL_OUT);
-    sPsum = spart + (size_t)QL_GRID * QL_OUT;
+    SideScope side;
+    double *sws = (double *)scratch(kSlotWork, sizeof(double) * qr_work_doubles(M, NBQ, NBQ));
+    sw = qr_work(sws, M, NBQ, NBQ);
   }
-  factor_panel(M, std::min(NBQ, mn), A, lda, tau, part, Psum, st);
+  factor_panel(M, std::min(NBQ, mn), A, lda, tau, w, st);
   int k = 0;
   for (int j = 0; j < mn; j += NBQ, k++) {
     const int nb = std::min(NBQ, mn - j), m = M - j, jn = j + nb;
     if (jn >= N) break;
     double *P = A + j + (long)j * lda;
     if (k > 0) ATLB_CUDA_CHECK(cudaStreamWaitEvent(st, side_event(2 + (k & 1)), 0));  // panel k factored
-    build_vt(m, nb, P, lda, tau + j, V, G, T, st);
+    build_vt(m, nb, P, lda, tau + j, w.V, w.G, w.T, w.tmp, st);
     if (jn >= mn) {  // no panel after this one: columns mn..N-1 only
-      larfb_lt(m, N - jn, nb, V, T, P + (long)nb * lda, lda, W, st);
+      larfb_lt(m, N - jn, nb, w.V, w.T, P + (long)nb * lda, lda, w.W, st);
       break;
     }
     const int nbn = std::min(NBQ, mn - jn), rest = N - jn - nbn;
-    larfb_lt(m, nbn, nb, V, T, P + (long)nb * lda, lda, W, st);
+    larfb_lt(m, nbn, nb, w.V, w.T, P + (long)nb * lda, lda, w.W, st);
     ATLB_CUDA_CHECK(cudaEventRecord(side_event(k & 1), st));
     ATLB_CUDA_CHECK(cudaStreamWaitEvent(s1, side_event(k & 1), 0));
     {
       SideScope side;
-      factor_panel(M - jn, nbn, A + jn + (long)jn * lda, lda, tau + jn, spart, sPsum, s1);
+      factor_panel(M - jn, nbn, A + jn + (long)jn * lda, lda, tau + jn, sw, s1);
       ATLB_CUDA_CHECK(cudaEventRecord(side_event(2 + ((k + 1) & 1)), s1));
     }
     if (rest > 0) {
       const int reserve = tune(kTuneLookaheadReserve);
       GemmCtaCap cap(reserve > 0 ? std::max(1, num_sms() - reserve) : 0);
-      larfb_lt(m, rest, nb, V, T, P + (long)(nb + nbn) * lda, lda, W, st);
+      larfb_lt(m, rest, nb, w.V, w.T, P + (long)(nb + nbn) * lda, lda, w.W, st);
     }
   }
   ATLB_CUDA_CHECK(cudaStreamWaitEvent(st, side_event(2 + (k & 1)), 0));  // join the last panel

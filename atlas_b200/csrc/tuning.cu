@@ -35,7 +35,7 @@ const TuneDef kDefs[kNumTune] = {
     {"mixed_tc_min_work_log2", 31, 16, 40, 1},  // mixed solvers: M*N*K below 2^x runs on FP32 FMA
     {"lookahead_reserve_sms", 0, 0, 96, 1},   // SMs the trailing-update DGEMM leaves to the look-ahead panel
     {"sgetrf_nb", 256, 64, 256, 32},          // outer LU block of the FP32 factorization (mixed solvers)
-    {"qr_nb", 128, 32, 128, 32},              // QR panel width (ilaenv's NB for geqrf)
+    {"qr_nb", 128, 32, 256, 32},              // QR panel width (ilaenv's NB for geqrf; > 128: two halves)
     {"batch_posv_small", 96, 32, 128, 16},    // batched Cholesky: orders <= this factor whole in shared memory
     {"batch_posv_pw", 32, 16, 64, 16},        // batched Cholesky: panel width above that order
     {"batch_getrf_smem", 160, 64, 160, 16},   // batched LU: orders <= this factor whole in shared memory

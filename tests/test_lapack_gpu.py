@@ -261,3 +261,34 @@ def test_geqrf_vs_reference_lapack_golden(gpu):
         assert info == info_ref == 0, f"geqrf case {i}"
         assert GL.close(qr, qr_ref, 1e-10), f"geqrf case {i}"
         assert GL.close(tau[:min(m, n)], tau_ref, 1e-10), f"geqrf case {i}"
+
+
+@pytest.mark.parametrize("nb", [64, 256])
+@pytest.mark.parametrize("la", [0, 1])
+def test_geqrf_panel_widths_vs_oracle(gpu, orc, nb, la):
+    """qr_nb = 256 factors each panel as two 128-column halves (the left
+    half's block reflector applied to the right half in between, T built
+    from the two halves' T); with and without look-ahead the result matches
+    the oracle as with the default width, and so does Q applied by dormqr."""
+    m, n = 1100, 700
+    a0 = orc.normal((m, n), 97)
+    try:
+        assert AB.atlb_tune_set("qr_nb", nb) == nb
+        assert AB.atlb_tune_set("lookahead", la) == la
+        a = a0.copy(order="F")
+        tau = np.zeros(n)
+        assert AB.clapack_dgeqrf(CM, m, n, a, m, tau) == 0
+        qr, rtau = orc.dgeqrf(a0.copy(order="F"))
+        np.testing.assert_allclose(tau, rtau, rtol=1e-9, atol=1e-11)
+        np.testing.assert_allclose(np.triu(a), np.triu(qr), rtol=1e-9, atol=1e-10)
+        np.testing.assert_allclose(np.tril(a, -1), np.tril(qr, -1), rtol=1e-8, atol=1e-10)
+        assert orc.resid_qr(a0, a.copy(order="F"), tau) <= 100.0
+        # Q^T A = R through the blocked apply at the same width
+        c = a0.copy(order="F")
+        assert AB.ATL_dormqr(AB.CblasLeft, AB.CblasTrans, m, n, n, a, m, tau, c, m, None, 0) == 0
+        r = np.triu(a)[:n]
+        np.testing.assert_allclose(c[:n], r, rtol=1e-9, atol=1e-9 * np.abs(r).max())
+        assert np.abs(c[n:]).max() <= 1e-9 * np.abs(r).max()
+    finally:
+        AB.atlb_tune_set("qr_nb", 128)
+        AB.atlb_tune_set("lookahead", 1)
