@@ -12,9 +12,13 @@
 // already in registers.  The block is then solved by one product with the
 // inverse of its 128 x 128 diagonal block (computed once per factor by
 // trsv_inverse_dev, loaded into shared memory before any wait) and
-// published.  Every wait on a flag is bounded: after ~1 s the kernel records
-// an error in *err and stops waiting (the result is then wrong but the GPU
-// is released).  The launcher clears the ticket counter and the flags before
+// published.  In FP32 the block just before is not awaited through its flag:
+// its x also goes out as (value, epoch) 64-bit words, each written by one
+// single-copy-atomic store, and the next block polls those words directly --
+// one round trip to L2 on the chain instead of fence, flag and data load.
+// Every wait is bounded: after ~1 s the kernel records an error in *err and
+// stops waiting (the result is then wrong but the GPU is released).  The
+// launcher clears the ticket counter, the flags and the tagged words before
 // each launch.
 #include <algorithm>
 #include "common.cuh"
@@ -25,7 +29,9 @@ namespace {
 
 constexpr int BS = 64;       // rows of a diagonal block (W's blocks)
 constexpr int CB = 2 * BS;   // rows of one CTA's block
-constexpr int TT = 256;      // threads: two per row of the CTA's block
+constexpr int TT = 512;      // threads: four per row of the CTA's block
+constexpr int NQ = TT / CB;  // parts a row's dot products are split into
+constexpr int PART = CB / NQ;  // columns of a solved block per thread
 
 __device__ __forceinline__ uint64_t gtimer() {
   uint64_t t;
@@ -42,12 +48,13 @@ __device__ __forceinline__ int ld_acquire(const int *p) {
 template <typename T, int NR>
 __global__ void __launch_bounds__(TT, 1)
 trsv_kernel(int n, int nrhs, const T *__restrict__ Tp, long tr, long tc, int lower,
-            const T *__restrict__ W, T *X, long ldx, int *counter, int *flags, int epoch, int *err) {
+            const T *__restrict__ W, T *X, long ldx, int *counter, int *flags, int epoch, int *err,
+            unsigned long long *xt) {
   extern __shared__ __align__(16) unsigned char trsv_smem[];
   T(*sW)[CB + 1] = reinterpret_cast<T(*)[CB + 1]>(trsv_smem);   // [CB]: the inverted diagonal block
   T(*sxd)[CB][NR] = reinterpret_cast<T(*)[CB][NR]>(sW + CB);    // x of a solved block, double-buffered
   T(*sb)[NR] = reinterpret_cast<T(*)[NR]>(sxd + 2);             // this block's b
-  T(*sacc)[CB][NR] = reinterpret_cast<T(*)[CB][NR]>(sb + CB);   // [2]: the two halves' sums
+  T(*sacc)[CB][NR] = reinterpret_cast<T(*)[CB][NR]>(sb + CB);   // [NQ]: the parts' sums
   __shared__ int s_bi, s_ready;
   const int tid = threadIdx.x, lane = tid & 31, nb = (n + CB - 1) / CB;
   if (tid == 0) {
@@ -71,13 +78,13 @@ trsv_kernel(int n, int nrhs, const T *__restrict__ Tp, long tr, long tc, int low
     const int rr = idx % CB, q = idx / CB;
     sb[rr][q] = (rr < rows && q < nrhs) ? X[r0 + rr + (long)q * ldx] : T(0);
   }
-  // thread (row, half): row of this block, columns half*64 .. +63 of every solved block
-  const int row = tid % CB, half = tid / CB;
+  // thread (row, part): row of this block, columns part*PART .. +PART-1 of every solved block
+  const int row = tid % CB, part = tid / CB;
   const T *trow = Tp + (long)(r0 + row) * tr;
   const int ndep = lower ? bi : nb - 1 - bi;
-  T acc[NR];
+  T acc[NR], acc2[NR];  // even and odd columns: two independent FMA chains
 #pragma unroll
-  for (int q = 0; q < NR; q++) acc[q] = T(0);
+  for (int q = 0; q < NR; q++) acc[q] = acc2[q] = T(0);
   auto wait_flag = [&](int bj) {
     const uint64_t t0 = gtimer();
     while (ld_acquire(flags + bj) != epoch) {
@@ -110,20 +117,24 @@ trsv_kernel(int n, int nrhs, const T *__restrict__ Tp, long tr, long tc, int low
     const int nr = s_ready;
     for (int e = 0; e < nr; e++, d++) {
       const int bj = lower ? d : nb - 1 - d;
-      const int c0 = bj * CB + half * BS, cols = min(BS, n - c0);
-      // all 64 matrix loads in flight at once, issued before the barrier: a
-      // CTA far down the triangle streams many blocks, and this stream (not
-      // the chain of solves) bounds it when fewer loads are in flight
-      T tv[BS];
+      const int c0 = bj * CB + part * PART, cols = min(PART, n - c0);
+      // all of this thread's matrix loads in flight at once, issued before
+      // the barrier: a CTA far down the triangle streams many blocks, and
+      // this stream (not the chain of solves) bounds it when fewer loads
+      // are in flight
+      T tv[PART];
 #pragma unroll
-      for (int k = 0; k < BS; k++) tv[k] = (row < rows && k < cols) ? trow[(long)(c0 + k) * tc] : T(0);
+      for (int k = 0; k < PART; k++) tv[k] = (row < rows && k < cols) ? trow[(long)(c0 + k) * tc] : T(0);
       load_x(bj, buf);
       __syncthreads();
-      const T(*xs)[NR] = sxd[buf] + half * BS;
+      const T(*xs)[NR] = sxd[buf] + part * PART;
 #pragma unroll
-      for (int k = 0; k < BS; k++)
+      for (int k = 0; k < PART; k += 2)
 #pragma unroll
-        for (int q = 0; q < NR; q++) acc[q] = fma(tv[k], xs[k][q], acc[q]);
+        for (int q = 0; q < NR; q++) {
+          acc[q] = fma(tv[k], xs[k][q], acc[q]);
+          acc2[q] = fma(tv[k + 1], xs[k + 1][q], acc2[q]);
+        }
       buf ^= 1;
     }
     __syncthreads();  // s_ready is read by every thread before it is rewritten
@@ -131,45 +142,87 @@ trsv_kernel(int n, int nrhs, const T *__restrict__ Tp, long tr, long tc, int low
   // 2. the block just before this one: its matrix values first, then the wait
   if (ndep > 0) {
     const int bj = lower ? ndep - 1 : nb - ndep;
-    const int c0 = bj * CB + half * BS, cols = min(BS, n - c0);
-    T tv[BS];
+    const int c0 = bj * CB + part * PART, cols = min(PART, n - c0);
+    T tv[PART];
 #pragma unroll
-    for (int k = 0; k < BS; k++) tv[k] = (row < rows && k < cols) ? trow[(long)(c0 + k) * tc] : T(0);
-    if (tid == 0) wait_flag(bj);
-    __syncthreads();
-    load_x(bj, buf);
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < BS; k++)
-#pragma unroll
-      for (int q = 0; q < NR; q++) acc[q] = fma(tv[k], sxd[buf][half * BS + k][q], acc[q]);
-  }
-#pragma unroll
-  for (int q = 0; q < NR; q++) sacc[half][row][q] = acc[q];
-  __syncthreads();
-  for (int idx = tid; idx < CB * NR; idx += TT) {
-    const int rr = idx % CB, q = idx / CB;
-    sb[rr][q] -= sacc[0][rr][q] + sacc[1][rr][q];
-  }
-  __syncthreads();
-  // 3. x = inv(T_bb) b: thread (row, half) sums over half of the columns
-  {
-    T v[NR];
-#pragma unroll
-    for (int q = 0; q < NR; q++) v[q] = T(0);
-#pragma unroll 16
-    for (int c = half * BS; c < half * BS + BS; c++) {
-      const T w = sW[row][c];
-#pragma unroll
-      for (int q = 0; q < NR; q++) v[q] = fma(w, sb[c][q], v[q]);
+    for (int k = 0; k < PART; k++) tv[k] = (row < rows && k < cols) ? trow[(long)(c0 + k) * tc] : T(0);
+    if constexpr (sizeof(T) == 4) {
+      // FP32: x arrives as (value, epoch) 64-bit words, each written by one
+      // single-copy-atomic store, so a word whose tag is current carries its
+      // value: one round trip to L2 instead of flag, fence and data
+      const uint64_t t0 = gtimer();
+      while (true) {
+        bool ok = true;
+        for (int idx = tid; idx < CB * NR; idx += TT) {
+          const int cc = idx % CB, q = idx / CB;
+          T v = T(0);
+          if (bj * CB + cc < n && q < nrhs) {
+            const unsigned long long w = __ldcg(xt + (long)(bj * CB + cc) * NR + q);
+            ok = ok && (int)(w >> 32) == epoch;
+            v = __uint_as_float((unsigned)(w & 0xffffffffu));
+          }
+          sxd[buf][cc][q] = v;
+        }
+        if (__syncthreads_and(ok)) break;
+        if (gtimer() - t0 > 1000000000ull) {  // bounded: record and go on (the result is then wrong)
+          if (tid == 0) atomicExch(err, 1);
+          break;
+        }
+      }
+    } else {
+      if (tid == 0) wait_flag(bj);
+      __syncthreads();
+      load_x(bj, buf);
+      __syncthreads();
     }
 #pragma unroll
-    for (int q = 0; q < NR; q++) sacc[half][row][q] = v[q];
+    for (int k = 0; k < PART; k += 2)
+#pragma unroll
+      for (int q = 0; q < NR; q++) {
+        acc[q] = fma(tv[k], sxd[buf][part * PART + k][q], acc[q]);
+        acc2[q] = fma(tv[k + 1], sxd[buf][part * PART + k + 1][q], acc2[q]);
+      }
+  }
+#pragma unroll
+  for (int q = 0; q < NR; q++) sacc[part][row][q] = acc[q] + acc2[q];
+  __syncthreads();
+  for (int idx = tid; idx < CB * NR; idx += TT) {
+    const int rr = idx % CB, q = idx / CB;
+    T t = T(0);
+#pragma unroll
+    for (int p = 0; p < NQ; p++) t += sacc[p][rr][q];
+    sb[rr][q] -= t;
+  }
+  __syncthreads();
+  // 3. x = inv(T_bb) b: thread (row, part) sums over a quarter of the columns
+  {
+    T v[NR], v2[NR];
+#pragma unroll
+    for (int q = 0; q < NR; q++) v[q] = v2[q] = T(0);
+#pragma unroll
+    for (int c = part * PART; c < part * PART + PART; c += 2) {
+      const T w = sW[row][c], w2 = sW[row][c + 1];
+#pragma unroll
+      for (int q = 0; q < NR; q++) {
+        v[q] = fma(w, sb[c][q], v[q]);
+        v2[q] = fma(w2, sb[c + 1][q], v2[q]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < NR; q++) sacc[part][row][q] = v[q] + v2[q];
   }
   __syncthreads();
   for (int idx = tid; idx < CB * NR; idx += TT) {
     const int rr = idx % CB, q = idx / CB;
-    if (rr < rows && q < nrhs) X[r0 + rr + (long)q * ldx] = sacc[0][rr][q] + sacc[1][rr][q];
+    T t = T(0);
+#pragma unroll
+    for (int p = 0; p < NQ; p++) t += sacc[p][rr][q];
+    if (rr < rows && q < nrhs) {
+      X[r0 + rr + (long)q * ldx] = t;
+      if constexpr (sizeof(T) == 4)
+        xt[(long)(r0 + rr) * NR + q] =
+            ((unsigned long long)(unsigned)epoch << 32) | (unsigned long long)__float_as_uint((float)t);
+    }
   }
   __syncthreads();
   if (tid == 0) {  // the barrier orders every thread's x stores before this release
@@ -298,13 +351,16 @@ void trsv_w_dev(int uplo, int trans, int n, int nrhs, const T *A, long lda, cons
   const long tstr = tr ? lda : 1, tcol = tr ? 1 : lda;  // effective T(i,k) = A[i*tstr + k*tcol]
   const int lower = (uplo == kLower) != tr;
   const int nb = cdiv(n, CB);
-  // workspace: ticket counter, error word, flags
-  int *ctl = (int *)scratch(kSlotTrsvCtl, sizeof(int) * (nb + 64));
+  // workspace: ticket counter, error word, flags, and (FP32) the tagged copy
+  // of x, 8 words per row
+  const size_t nctl = (size_t)cdiv(nb + 64, 2) * 2, ntag = sizeof(T) == 4 ? (size_t)nb * CB * 8 : 0;
+  int *ctl = (int *)scratch(kSlotTrsvCtl, sizeof(int) * nctl + sizeof(unsigned long long) * ntag);
   const int epoch = 1;
   int *counter = ctl, *err = ctl + 1, *flags = ctl + 64;
-  ATLB_CUDA_CHECK(cudaMemsetAsync(ctl, 0, sizeof(int) * (nb + 64), st));  // counter, flags
+  unsigned long long *xt = (unsigned long long *)(ctl + nctl);
+  ATLB_CUDA_CHECK(cudaMemsetAsync(ctl, 0, sizeof(int) * nctl + sizeof(unsigned long long) * ntag, st));
   // sW, sxd, sb, sacc (trsv_kernel's layout), for the largest NR
-  constexpr int smem = (CB * (CB + 1) + (2 * CB + CB + 2 * CB) * 8) * (int)sizeof(T);
+  constexpr int smem = (CB * (CB + 1) + (2 * CB + CB + NQ * CB) * 8) * (int)sizeof(T);
   static bool configured = false;
   if (!configured) {
     ATLB_CUDA_CHECK(cudaFuncSetAttribute(trsv_kernel<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -312,9 +368,12 @@ void trsv_w_dev(int uplo, int trans, int n, int nrhs, const T *A, long lda, cons
     ATLB_CUDA_CHECK(cudaFuncSetAttribute(trsv_kernel<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     configured = true;
   }
-  if (nrhs == 1) trsv_kernel<T, 1><<<nb, TT, smem, st>>>(n, nrhs, A, tstr, tcol, lower, W, B, ldb, counter, flags, epoch, err);
-  else if (nrhs <= 4) trsv_kernel<T, 4><<<nb, TT, smem, st>>>(n, nrhs, A, tstr, tcol, lower, W, B, ldb, counter, flags, epoch, err);
-  else trsv_kernel<T, 8><<<nb, TT, smem, st>>>(n, nrhs, A, tstr, tcol, lower, W, B, ldb, counter, flags, epoch, err);
+  if (nrhs == 1)
+    trsv_kernel<T, 1><<<nb, TT, smem, st>>>(n, nrhs, A, tstr, tcol, lower, W, B, ldb, counter, flags, epoch, err, xt);
+  else if (nrhs <= 4)
+    trsv_kernel<T, 4><<<nb, TT, smem, st>>>(n, nrhs, A, tstr, tcol, lower, W, B, ldb, counter, flags, epoch, err, xt);
+  else
+    trsv_kernel<T, 8><<<nb, TT, smem, st>>>(n, nrhs, A, tstr, tcol, lower, W, B, ldb, counter, flags, epoch, err, xt);
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
 template void trsv_w_dev<double>(int, int, int, int, const double *, long, const double *, double *, long,
