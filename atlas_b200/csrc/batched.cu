@@ -6,11 +6,13 @@
 // One persistent launch per batch: CTAs pull problem indices from an atomic
 // counter over a work list sorted by decreasing size (largest first, so the
 // tail of the launch is made of small problems), and each problem is handled
-// entirely by one CTA.  Size buckets pick the code path: a matrix of order
-// <= 96 is factored with the whole matrix in shared memory; larger ones
-// (up to 256) in 32-column panels staged in shared memory with the trailing
-// update written back to global memory (L2-resident at these sizes).
-// Nothing waits on another CTA, so the launch cannot stall.
+// entirely by one CTA.  Cholesky: orders up to batch_posv_small are factored
+// with the whole matrix in shared memory, larger ones (up to 256) in panels
+// of batch_posv_pw columns staged in shared memory with the trailing update
+// written back to global memory (L2-resident at these sizes).  LU: 16-column
+// pivoted panels in shared memory, the trailing update on the FP64 tensor
+// cores in global memory.  The solves run in blocks of 16 rows.  Nothing
+// waits on another CTA, so the launch cannot stall.
 #include <algorithm>
 #include <cfloat>
 #include <climits>
@@ -27,9 +29,9 @@ namespace {
 
 constexpr int BT = 256;       // threads per CTA
 constexpr int MAXN = 256;
-// Size buckets (tunable, tuning.cu): orders up to batch_posv_small (Cholesky)
-// / batch_getrf_smem (LU) are factored whole in shared memory, larger ones in
-// panels of batch_posv_pw columns.
+// Size buckets of the Cholesky path (tunable, tuning.cu): orders up to
+// batch_posv_small are factored whole in shared memory, larger ones in panels
+// of batch_posv_pw columns.
 
 struct Prob {
   double *A;
@@ -40,26 +42,60 @@ struct Prob {
 
 // ---------------------------------------------------------------- Cholesky
 
-// forward then backward substitution with L (lower, in shared memory or
-// global, ld = ldl) for nrhs columns of B (global)
-__device__ void chol_solve(const double *L, int ldl, int n, double *B, int ldb, int nrhs) {
+// Triangular solve of one right-hand side held in shared memory (b, n <=
+// MAXN) with T in shared or global memory (ld ldt): op(T) x = b, op(T)
+// lower (forward) or upper (backward) triangular, T itself read transposed
+// when trans.  Blocks of 16 rows: warp 0 solves a block's 16 x 16 diagonal
+// part (x_c by shuffle), then every thread subtracts the block's
+// contribution from one remaining row -- two barriers per block instead of
+// two per row.
+__device__ void tri_solve_smem(const double *T, long ldt, int n, double *b, bool lower, bool unit, bool trans) {
   const int tid = threadIdx.x;
+  auto at = [&](int i, int c) { return trans ? T[c + (long)i * ldt] : T[i + (long)c * ldt]; };
+  const int nblk = (n + 15) / 16;
+  for (int t = 0; t < nblk; t++) {
+    const int b0 = lower ? 16 * t : 16 * (nblk - 1 - t), bs = min(16, n - b0);
+    if (tid < 32) {
+      const int i = tid;
+      double x = i < bs ? b[b0 + i] : 0.0;
+      if (lower) {
+        for (int c = 0; c < bs; c++) {
+          if (!unit && i == c) x = x / at(b0 + c, b0 + c);
+          const double xc = __shfl_sync(0xffffffffu, x, c);
+          if (i > c && i < bs) x = fma(-at(b0 + i, b0 + c), xc, x);
+        }
+      } else {
+        for (int c = bs - 1; c >= 0; c--) {
+          if (!unit && i == c) x = x / at(b0 + c, b0 + c);
+          const double xc = __shfl_sync(0xffffffffu, x, c);
+          if (i < c) x = fma(-at(b0 + i, b0 + c), xc, x);
+        }
+      }
+      if (i < bs) b[b0 + i] = x;
+    }
+    __syncthreads();
+    const int r0 = lower ? b0 + bs : 0, r1 = lower ? n : b0;
+    for (int i = r0 + tid; i < r1; i += BT) {
+      double acc = b[i];
+      for (int c = 0; c < bs; c++) acc = fma(-at(i, b0 + c), b[b0 + c], acc);
+      b[i] = acc;
+    }
+    __syncthreads();
+  }
+}
+
+// A = L L^T: forward then backward substitution for nrhs columns of B
+// (global), L lower in shared or global memory (ld ldl)
+__device__ void chol_solve(const double *L, int ldl, int n, double *B, int ldb, int nrhs) {
+  __shared__ double sbv[MAXN];
   for (int r = 0; r < nrhs; r++) {
-    double *b = B + (long)r * ldb;
-    for (int j = 0; j < n; j++) {  // L y = b
-      const double yj = b[j] / L[j + (long)j * ldl];
-      __syncthreads();
-      if (tid == 0) b[j] = yj;
-      for (int i = j + 1 + tid; i < n; i += BT) b[i] = fma(-L[i + (long)j * ldl], yj, b[i]);
-      __syncthreads();
-    }
-    for (int j = n - 1; j >= 0; j--) {  // L^T x = y
-      const double xj = b[j] / L[j + (long)j * ldl];
-      __syncthreads();
-      if (tid == 0) b[j] = xj;
-      for (int i = tid; i < j; i += BT) b[i] = fma(-L[j + (long)i * ldl], xj, b[i]);
-      __syncthreads();
-    }
+    double *bg = B + (long)r * ldb;
+    for (int i = threadIdx.x; i < n; i += BT) sbv[i] = bg[i];
+    __syncthreads();
+    tri_solve_smem(L, ldl, n, sbv, true, false, false);   // L y = b
+    tri_solve_smem(L, ldl, n, sbv, false, false, true);   // L^T x = y
+    for (int i = threadIdx.x; i < n; i += BT) bg[i] = sbv[i];
+    __syncthreads();
   }
 }
 
@@ -122,52 +158,136 @@ batched_posv_kernel(const Prob *__restrict__ probs, const int *__restrict__ orde
 
 // ---------------------------------------------------------------- LU
 
-// partial-pivoting LU of the n x n matrix in shared memory (ld lds); ipiv
-// 0-based; returns the first zero pivot (1-based) or 0.  Pivot rule as
-// ATL_getf2: first maximal |a| (ties to the lowest row index).
-__device__ int lu_smem(double *s, int lds, int n, int *ipiv, double *wv, int *wi) {
+// Blocked LU with partial pivoting of one problem by one CTA, the matrix in
+// place in global memory (L2-resident at these orders), ATL_getrfC's
+// right-looking step on panels of LPW columns:
+//   1. the panel (rows j..n-1) is staged in shared memory and factored there
+//      column by column: arg-max with the first maximum on ties
+//      (cblas_idamax / ATL_getf2), the interchange inside the panel, the
+//      scaling (by the reciprocal when the pivot is a normal number), the
+//      rank-1 update of the panel's columns right of it;
+//   2. the panel goes back, ipiv[j + c] = j + its pivot row;
+//   3. the panel's interchanges, composed into one row permutation, move
+//      the rows of every column outside the panel (LAPACK's laswp on the
+//      left and right parts) in one gather / scatter pass;
+//   4. U12 = L11^-1 A12 (one thread per column) into global memory and a
+//      shared copy;
+//   5. A22 -= L21 U12 on the FP64 tensor cores (mma.m8n8k4), L21 and U12
+//      from shared memory, A22 read and written in global memory.
+// Returns the first zero pivot (1-based) or 0; the factorization completes
+// either way (LAPACK getrf semantics).
+constexpr int LPW = 16;              // panel width
+constexpr int LU_LDP = cholb::ld_for(MAXN);  // panel ld (rows of the panel, <= MAXN)
+constexpr int LU_LDU = LPW + 4;      // U12 copy, stored U(q, k) at k * LU_LDU + q
+constexpr int LU_CHUNK = 64;         // columns per gather / scatter pass of the interchanges
+
+struct LuSmem {
+  double P[LU_LDP * LPW];
+  double U[MAXN * LU_LDU];
+  double stage[2 * LPW * LU_CHUNK];
+  double wv[BT / 32];
+  int wi[BT / 32];
+  int piv[LPW];
+  int who[MAXN];
+  int src[2 * LPW], dst[2 * LPW];
+  int nmove, fail;
+};
+
+// C (mt x nt, global, ldc) -= P (mt x kb, shared, ld lds) U (kb x nt, shared,
+// U(q, k) at k * ldu + q), kb <= LPW: each warp owns a 16 x 32 part of every
+// 64 x 64 block of C (2 x 4 tiles of 8 x 8), accumulators started from C
+__device__ void lu_update_dmma(int mt, int nt, int kb, const double *P, int lds, const double *U, int ldu,
+                               double *C, long ldc) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+  const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
+  for (int ib = 0; ib < mt; ib += 64)
+    for (int kb0 = 0; kb0 < nt; kb0 += 64) {
+      const int r0 = ib + wr, c0 = kb0 + wc;
+      if (r0 >= mt || c0 >= nt) continue;  // warp-uniform
+      double acc[2][4][2];
+#pragma unroll
+      for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++)
+#pragma unroll
+          for (int e = 0; e < 2; e++) {
+            const int i = r0 + 8 * a + g, k = c0 + 8 * b + 2 * t + e;
+            acc[a][b][e] = (i < mt && k < nt) ? C[i + (long)k * ldc] : 0.0;
+          }
+#pragma unroll
+      for (int q = 0; q < LPW; q += 4) {
+        const int qq = q + t;
+        double av[2], bv[4];
+#pragma unroll
+        for (int a = 0; a < 2; a++) {
+          const int i = r0 + 8 * a + g;
+          av[a] = (i < mt && qq < kb) ? -P[i + qq * lds] : 0.0;
+        }
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+          const int k = c0 + 8 * b + g;
+          bv[b] = (k < nt && qq < kb) ? U[k * ldu + qq] : 0.0;
+        }
+#pragma unroll
+        for (int a = 0; a < 2; a++)
+#pragma unroll
+          for (int b = 0; b < 4; b++) cholb::dmma_8x8x4(acc[a][b], av[a], bv[b]);
+      }
+#pragma unroll
+      for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++)
+#pragma unroll
+          for (int e = 0; e < 2; e++) {
+            const int i = r0 + 8 * a + g, k = c0 + 8 * b + 2 * t + e;
+            if (i < mt && k < nt) C[i + (long)k * ldc] = acc[a][b][e];
+          }
+    }
+}
+
+// step 1: partial-pivoting LU of the m x jb panel in shared memory; S.piv[c]
+// = panel-relative pivot row of column c; returns the first zero pivot
+// (1-based, panel-relative) or 0
+__device__ int lu_panel(LuSmem &S, int m, int jb) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double *P = S.P;
   int fail = 0;
-  for (int j = 0; j < n; j++) {
+  for (int c = 0; c < jb; c++) {
     double v = -1.0;
     int vi = INT_MAX;
-    for (int i = j + tid; i < n; i += BT) {
-      const double t = fabs(s[i + j * lds]);
-      if (t > v) { v = t; vi = i; }
+    for (int i = c + tid; i < m; i += BT) {
+      const double a = fabs(P[i + c * LU_LDP]);
+      if (a > v) { v = a; vi = i; }   // NaN never wins
     }
     for (int o = 16; o; o >>= 1) {
       const double ov = __shfl_xor_sync(0xffffffffu, v, o);
       const int oi = __shfl_xor_sync(0xffffffffu, vi, o);
       if (ov > v || (ov == v && oi < vi)) { v = ov; vi = oi; }
     }
-    if (lane == 0) { wv[warp] = v; wi[warp] = vi; }
+    if (lane == 0) { S.wv[warp] = v; S.wi[warp] = vi; }
     __syncthreads();
     double best = -1.0;
     int p = INT_MAX;
     for (int w = 0; w < BT / 32; w++)
-      if (wv[w] > best || (wv[w] == best && wi[w] < p)) { best = wv[w]; p = wi[w]; }
-    if (best <= 0.0) p = j;
-    if (tid == 0) ipiv[j] = p;
-    if (p != j)
-      for (int c = tid; c < n; c += BT) {
-        const double t = s[j + c * lds];
-        s[j + c * lds] = s[p + c * lds];
-        s[p + c * lds] = t;
-      }
+      if (S.wv[w] > best || (S.wv[w] == best && S.wi[w] < p)) { best = S.wv[w]; p = S.wi[w]; }
+    if (!(best > 0.0)) p = c;  // zero (or NaN) column: no interchange
+    if (tid == 0) S.piv[c] = p;
+    if (p != c && tid < jb) {
+      const double t0 = P[c + tid * LU_LDP];
+      P[c + tid * LU_LDP] = P[p + tid * LU_LDP];
+      P[p + tid * LU_LDP] = t0;
+    }
     __syncthreads();
-    const double piv = s[j + j * lds];
+    const double piv = P[c + c * LU_LDP];
     if (piv == 0.0) {
-      if (!fail) fail = j + 1;
+      if (!fail) fail = c + 1;
     } else {
       const double r = 1.0 / piv;
       const bool use_r = fabs(piv) >= DBL_MIN;
-      for (int i = j + 1 + tid; i < n; i += BT) s[i + j * lds] = use_r ? s[i + j * lds] * r : s[i + j * lds] / piv;
-      __syncthreads();
-      // rank-1 update: 16 x 16 threads, rows tx + 16 a, columns ty + 16 b
-      const int tx = tid % 16, ty = tid / 16;
-      for (int k = j + 1 + ty; k < n; k += 16) {
-        const double u = s[j + k * lds];
-        for (int i = j + 1 + tx; i < n; i += 16) s[i + k * lds] = fma(-s[i + j * lds], u, s[i + k * lds]);
+      for (int i = c + 1 + tid; i < m; i += BT) {
+        const double l = use_r ? P[i + c * LU_LDP] * r : P[i + c * LU_LDP] / piv;
+        P[i + c * LU_LDP] = l;
+        for (int k = c + 1; k < jb; k++) P[i + k * LU_LDP] = fma(-l, P[c + k * LU_LDP], P[i + k * LU_LDP]);
       }
     }
     __syncthreads();
@@ -175,13 +295,102 @@ __device__ int lu_smem(double *s, int lds, int n, int *ipiv, double *wv, int *wi
   return fail;
 }
 
+__device__ int lu_blocked(const Prob &pr, LuSmem &S) {
+  const int tid = threadIdx.x, n = pr.n;
+  double *A = pr.A;
+  const long lda = pr.lda;
+  if (tid == 0) S.fail = 0;
+  for (int j = 0; j < n; j += LPW) {
+    const int jb = min(LPW, n - j), m = n - j, nt = n - j - jb;
+    for (int idx = tid; idx < m * jb; idx += BT) {
+      const int i = idx % m, c = idx / m;
+      S.P[i + c * LU_LDP] = A[(j + i) + (long)(j + c) * lda];
+    }
+    __syncthreads();
+    const int f = lu_panel(S, m, jb);
+    if (tid == 0 && f && !S.fail) S.fail = j + f;
+    for (int idx = tid; idx < m * jb; idx += BT) {
+      const int i = idx % m, c = idx / m;
+      A[(j + i) + (long)(j + c) * lda] = S.P[i + c * LU_LDP];
+    }
+    if (tid < jb) pr.ipiv[j + tid] = j + S.piv[tid];
+    // the panel's interchanges as one row permutation: who[r] = the panel
+    // row whose content ends at row r (panel-relative)
+    for (int r = tid; r < m; r += BT) S.who[r] = r;
+    __syncthreads();
+    if (tid == 0) {
+      for (int c = 0; c < jb; c++) {
+        const int p = S.piv[c];
+        const int t0 = S.who[c];
+        S.who[c] = S.who[p];
+        S.who[p] = t0;
+      }
+      int cnt = 0;
+      for (int c = 0; c < jb; c++) {  // moved rows: the first jb rows and the pivot rows
+        if (S.who[c] != c) { S.dst[cnt] = c; S.src[cnt] = S.who[c]; cnt++; }
+        const int p = S.piv[c];
+        if (p >= jb && S.who[p] != p) {
+          bool seen = false;
+          for (int q = 0; q < cnt; q++) seen = seen || S.dst[q] == p;
+          if (!seen) { S.dst[cnt] = p; S.src[cnt] = S.who[p]; cnt++; }
+        }
+      }
+      S.nmove = cnt;
+    }
+    __syncthreads();
+    const int nmove = S.nmove;
+    if (nmove > 0) {  // gather / scatter over the columns outside the panel, LU_CHUNK at a time
+      const int nout = n - jb;
+      for (int c0 = 0; c0 < nout; c0 += LU_CHUNK) {
+        const int cw = min(LU_CHUNK, nout - c0);
+        for (int e = tid; e < nmove * cw; e += BT) {
+          const int q = e % nmove, cc = c0 + e / nmove, col = cc < j ? cc : cc + jb;
+          S.stage[e] = A[(j + S.src[q]) + (long)col * lda];
+        }
+        __syncthreads();
+        for (int e = tid; e < nmove * cw; e += BT) {
+          const int q = e % nmove, cc = c0 + e / nmove, col = cc < j ? cc : cc + jb;
+          A[(j + S.dst[q]) + (long)col * lda] = S.stage[e];
+        }
+        __syncthreads();
+      }
+    }
+    if (nt > 0) {
+      // U12 = L11^-1 A12, one thread per column
+      for (int k = tid; k < nt; k += BT) {
+        double x[LPW];
+        double *col = A + j + (long)(j + jb + k) * lda;
+#pragma unroll
+        for (int q = 0; q < LPW; q++) x[q] = q < jb ? col[q] : 0.0;
+#pragma unroll
+        for (int q = 0; q < LPW; q++) {
+          if (q >= jb) continue;
+#pragma unroll
+          for (int r = q + 1; r < LPW; r++)
+            if (r < jb) x[r] = fma(-S.P[r + q * LU_LDP], x[q], x[r]);
+        }
+#pragma unroll
+        for (int q = 0; q < LPW; q++)
+          if (q < jb) {
+            col[q] = x[q];
+            S.U[k * LU_LDU + q] = x[q];
+          }
+      }
+      __syncthreads();
+      if (m > jb) lu_update_dmma(m - jb, nt, jb, S.P + jb, LU_LDP, S.U, LU_LDU, A + (j + jb) + (long)(j + jb) * lda, lda);
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  return S.fail;
+}
+
 __global__ void __launch_bounds__(BT)
 batched_getrf_kernel(const Prob *__restrict__ probs, const int *__restrict__ order, int count,
-                     int *__restrict__ next, int sm_max, int *__restrict__ info) {
+                     int *__restrict__ next, int *__restrict__ info) {
   extern __shared__ __align__(16) double sm[];
+  LuSmem &S = *reinterpret_cast<LuSmem *>(sm);
   __shared__ int s_p;
-  __shared__ double wv[BT / 32];
-  __shared__ int wi[BT / 32];
   const int tid = threadIdx.x;
   while (true) {
     if (tid == 0) {
@@ -192,26 +401,19 @@ batched_getrf_kernel(const Prob *__restrict__ probs, const int *__restrict__ ord
     const int p = s_p;
     if (p < 0) return;
     const Prob pr = probs[p];
-    const int n = pr.n;
-    int fail;
-    if (n <= sm_max) {  // the whole matrix in shared memory
-      const int lds = n + 1;
-      for (int idx = tid; idx < n * n; idx += BT) sm[idx % n + (idx / n) * lds] = pr.A[idx % n + (long)(idx / n) * pr.lda];
-      __syncthreads();
-      fail = lu_smem(sm, lds, n, pr.ipiv, wv, wi);
-      for (int idx = tid; idx < n * n; idx += BT) pr.A[idx % n + (long)(idx / n) * pr.lda] = sm[idx % n + (idx / n) * lds];
-    } else {  // in place in global memory (L2-resident at these orders)
-      fail = lu_smem(pr.A, pr.lda, n, pr.ipiv, wv, wi);
-    }
+    const int fail = lu_blocked(pr, S);
     if (tid == 0) info[p] = fail;
     __syncthreads();
   }
 }
 
+// P A = L U solves, one right-hand side at a time in shared memory: the
+// interchanges in order, then the blocked unit-lower and upper solves
 __global__ void __launch_bounds__(BT)
 batched_getrs_kernel(const Prob *__restrict__ probs, const int *__restrict__ order, int count,
                      int *__restrict__ next, const int *__restrict__ info) {
   __shared__ int s_p;
+  __shared__ double sbv[MAXN];
   const int tid = threadIdx.x;
   while (true) {
     if (tid == 0) {
@@ -224,29 +426,20 @@ batched_getrs_kernel(const Prob *__restrict__ probs, const int *__restrict__ ord
     const Prob pr = probs[p];
     if (info[p] == 0) {
       const int n = pr.n;
-      const int *ipiv = pr.ipiv;
-      const double *L = pr.A;
       for (int r = 0; r < pr.nrhs; r++) {
-        double *b = pr.B + (long)r * pr.ldb;
+        double *bg = pr.B + (long)r * pr.ldb;
+        for (int i = tid; i < n; i += BT) sbv[i] = bg[i];
+        __syncthreads();
         if (tid == 0)
           for (int k = 0; k < n; k++) {
-            const int q = ipiv[k];
-            if (q != k) { const double t = b[k]; b[k] = b[q]; b[q] = t; }
+            const int q = pr.ipiv[k];
+            if (q != k) { const double t0 = sbv[k]; sbv[k] = sbv[q]; sbv[q] = t0; }
           }
         __syncthreads();
-        for (int j = 0; j < n; j++) {  // unit lower
-          const double yj = b[j];
-          __syncthreads();
-          for (int i = j + 1 + tid; i < n; i += BT) b[i] = fma(-L[i + (long)j * pr.lda], yj, b[i]);
-          __syncthreads();
-        }
-        for (int j = n - 1; j >= 0; j--) {  // upper
-          const double xj = b[j] / L[j + (long)j * pr.lda];
-          __syncthreads();
-          if (tid == 0) b[j] = xj;
-          for (int i = tid; i < j; i += BT) b[i] = fma(-L[i + (long)j * pr.lda], xj, b[i]);
-          __syncthreads();
-        }
+        tri_solve_smem(pr.A, pr.lda, n, sbv, true, true, false);    // L y = P b
+        tri_solve_smem(pr.A, pr.lda, n, sbv, false, false, false);  // U x = y
+        for (int i = tid; i < n; i += BT) bg[i] = sbv[i];
+        __syncthreads();
       }
     }
     __syncthreads();
@@ -337,20 +530,19 @@ void batched_gesv_dev(const std::vector<Prob> &P, bool solve, int *info_out, cud
   BatchBufs b = prepare(P, kSlotBatch0);
   int maxn = 0;
   for (auto &p : P) maxn = std::max(maxn, p.n);
+  const size_t smb = sizeof(LuSmem);
   static bool configured = false;
   if (!configured) {
-    ATLB_CUDA_CHECK(cudaFuncSetAttribute(batched_getrf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024));
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(batched_getrf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smb));
     configured = true;
   }
-  const int sm_max = std::min(maxn, tune(kTuneBatchGetrfSmem));  // FP64 in shared memory: 206 KB at 160
-  const size_t smb = sizeof(double) * (size_t)sm_max * (sm_max + 1);
   const std::vector<unsigned long long> key = {0xBA7C0002ull + (solve ? 1 : 0),
       (unsigned long long)tune_generation(), (unsigned long long)count, (unsigned long long)maxn,
       (unsigned long long)(uintptr_t)b.d, (unsigned long long)(uintptr_t)b.h,
       (unsigned long long)(uintptr_t)info_out, (unsigned long long)(uintptr_t)st};
   run_graph(key, st, [&]() {
     enqueue_upload(b, st);
-    batched_getrf_kernel<<<grid_size(smb), BT, smb, st>>>(b.probs, b.order, count, b.next, sm_max, b.info);
+    batched_getrf_kernel<<<grid_size(smb), BT, smb, st>>>(b.probs, b.order, count, b.next, b.info);
     ATLB_CUDA_CHECK(cudaGetLastError());
     if (solve) {
       ATLB_CUDA_CHECK(cudaMemsetAsync(b.next, 0, sizeof(int), st));

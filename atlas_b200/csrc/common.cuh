@@ -77,7 +77,7 @@ inline int cdiv(long a, long b) { return (int)((a + b - 1) / b); }
 enum TuneParam {
   kTuneGetrfNB = 0, kTunePotrfNB, kTuneGemmGroup, kTuneSplitK, kTuneLookahead, kTuneTcMinWorkLog2,
   kTuneLookaheadReserve, kTuneSgetrfNB, kTuneQrNB, kTuneBatchPosvSmall, kTuneBatchPosvPW,
-  kTuneBatchGetrfSmem, kTuneMixedKrylov, kNumTune
+  kTuneMixedKrylov, kNumTune
 };
 int tune(int p);
 int tune_generation();  // bumps whenever a parameter changes (part of graph keys)

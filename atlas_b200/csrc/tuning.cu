@@ -38,7 +38,6 @@ const TuneDef kDefs[kNumTune] = {
     {"qr_nb", 128, 32, 256, 32},              // QR panel width (ilaenv's NB for geqrf; > 128: two halves)
     {"batch_posv_small", 96, 32, 128, 16},    // batched Cholesky: orders <= this factor whole in shared memory
     {"batch_posv_pw", 32, 16, 64, 16},        // batched Cholesky: panel width above that order
-    {"batch_getrf_smem", 160, 64, 160, 16},   // batched LU: orders <= this factor whole in shared memory
     {"mixed_krylov", 1, 0, 2, 1},             // mixed solvers: 0 plain refinement, 1 GMRES-IR once plain stalls
                                               // (from the start for BF16), 2 GMRES-IR from the start
 };

@@ -520,6 +520,19 @@ def extra_batched(torch, AB, dev, stream):
                                                                     ptrs(rh), ns, one, info), 1))
     batch_ms = min(ts[2:])
     flop = float(np.sum(2.0 / 3.0 * ns.astype(np.float64) ** 3 + 2.0 * ns.astype(np.float64) ** 2))
+    # the factorization alone (the batched getrf configuration)
+    tg = []
+    for rep in range(4):
+        for w, a in zip(work, A0s):
+            w.copy_(a)
+        tg.append(timed(torch, stream, lambda: AB.atlb_dgetrf_batched(count, ns, ptrs(work), ns, ptrs(piv), info), 1))
+    getrf_ms = min(tg[2:])
+    getrf_flop = float(np.sum(2.0 / 3.0 * ns.astype(np.float64) ** 3))
+    res["getrf_10k"] = {"ms_one_launch": getrf_ms, "gflops": getrf_flop / getrf_ms / 1e6,
+                        "all_info_zero": bool((info == 0).all()), "entry": "atlb_dgetrf_batched",
+                        "timing": "CUDA events around the call (upload, launch, info back), graph replay"}
+    for w, a in zip(work, A0s):
+        w.copy_(a)
 
     def loop2():
         for i in range(sample):

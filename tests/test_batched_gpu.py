@@ -170,3 +170,33 @@ def test_batched_getrf_only_matches_oracle(gpu):
             ref, rpiv, _ = O.dgetrf(a0s[i].copy(order="F"))
             np.testing.assert_array_equal(Ps[i].cpu().numpy(), rpiv)
             assert np.abs(As[i].cpu().numpy().T - ref).max() < 1e-12
+
+
+def test_batched_getrf_ties_and_zero_columns_match_oracle(gpu):
+    """Pivot ties (entries in {-2..2}: many equal |values| per column, the
+    first maximum wins) and exactly-zero columns (info = first zero pivot,
+    1-based; the factorization completes, as ATL_getf2 does), on sizes that
+    cross the 16-column panels of the batched LU."""
+    import torch
+    ns = [8, 17, 33, 64, 100, 130, 200, 256]
+    As, Ps, a0s, zero_col = [], [], [], []
+    for k, n in enumerate(ns):
+        a = np.asfortranarray(np.round(4.0 * O.gegen(n, n, n, 40 + k)[:n, :n]))
+        zc = -1
+        if k % 2:          # an exactly-zero column past the first panel
+            zc = min(n - 1, 16 + 3 * k)
+            a[:, zc] = 0.0
+        zero_col.append(zc)
+        a0s.append(a)
+        As.append(torch.tensor(np.ascontiguousarray(a.T), device="cuda"))
+        Ps.append(torch.zeros(n, dtype=torch.int32, device="cuda"))
+    info = np.zeros(len(ns), dtype=np.int32)
+    assert AB.atlb_dgetrf_batched(len(ns), _int_array(ns), _ptr_array(As), _int_array(ns), _ptr_array(Ps),
+                                  info) == 0
+    for i, n in enumerate(ns):
+        ref, rpiv, rinfo = O.dgetrf(a0s[i].copy(order="F"))
+        assert info[i] == rinfo, (n, info[i], rinfo)
+        if zero_col[i] >= 0:
+            assert rinfo > 0
+        np.testing.assert_array_equal(Ps[i].cpu().numpy(), rpiv)
+        assert np.abs(As[i].cpu().numpy().T - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max())

@@ -13,7 +13,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 INT_MIN = -2 ** 31
 NAMES = ["getrf_nb", "potrf_nb", "dgemm_group", "dgemm_splitk", "lookahead", "mixed_tc_min_work_log2",
          "lookahead_reserve_sms", "sgetrf_nb", "qr_nb", "batch_posv_small", "batch_posv_pw",
-         "batch_getrf_smem", "mixed_krylov"]
+         "mixed_krylov"]
 
 
 def _run(code, **env):
@@ -53,7 +53,7 @@ def test_set_clamps_and_rounds_to_the_step(atl):
 def test_defaults_without_a_file():
     out = _run("import atlas_b200 as AB; AB.lib(); "
                "print(*[AB.atlb_tune_get(n) for n in %r])" % NAMES, ATLAS_B200_TUNE_FILE="none")
-    assert [int(v) for v in out.split()] == [256, 256, 8, 1, 1, 31, 0, 256, 128, 96, 32, 160, 1]
+    assert [int(v) for v in out.split()] == [256, 256, 8, 1, 1, 31, 0, 256, 128, 96, 32, 1]
 
 
 def test_file_is_read_on_first_use(tmp_path):
