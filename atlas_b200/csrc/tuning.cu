@@ -36,8 +36,8 @@ const TuneDef kDefs[kNumTune] = {
     {"lookahead_reserve_sms", 0, 0, 96, 1},   // SMs the trailing-update DGEMM leaves to the look-ahead panel
     {"sgetrf_nb", 256, 64, 256, 32},          // outer LU block of the FP32 factorization (mixed solvers)
     {"qr_nb", 128, 32, 256, 32},              // QR panel width (ilaenv's NB for geqrf; > 128: two halves)
-    {"batch_posv_small", 96, 32, 128, 16},    // batched Cholesky: orders <= this factor whole in shared memory
-    {"batch_posv_pw", 32, 16, 64, 16},        // batched Cholesky: panel width above that order
+    {"batch_posv_small", 64, 32, 128, 16},    // batched Cholesky: orders <= this factor whole in shared memory
+    {"batch_posv_pw", 16, 16, 64, 16},        // batched Cholesky: panel width above that order
     {"mixed_krylov", 1, 0, 2, 1},             // mixed solvers: 0 plain refinement, 1 GMRES-IR once plain stalls
                                               // (from the start for BF16), 2 GMRES-IR from the start
 };

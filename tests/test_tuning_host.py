@@ -53,7 +53,7 @@ def test_set_clamps_and_rounds_to_the_step(atl):
 def test_defaults_without_a_file():
     out = _run("import atlas_b200 as AB; AB.lib(); "
                "print(*[AB.atlb_tune_get(n) for n in %r])" % NAMES, ATLAS_B200_TUNE_FILE="none")
-    assert [int(v) for v in out.split()] == [256, 256, 8, 1, 1, 31, 0, 256, 128, 96, 32, 1]
+    assert [int(v) for v in out.split()] == [256, 256, 8, 1, 1, 31, 0, 256, 128, 64, 16, 1]
 
 
 def test_file_is_read_on_first_use(tmp_path):
