@@ -107,6 +107,10 @@ template <int BNT> struct TileCfg {
   static constexpr int smem_doubles() { return STG * (Lay<TA, BM>::SIZE + Lay<!TB, BNT>::SIZE); }
 };
 constexpr int SMALL_K = 256;  // K up to this uses the 128 x 64 tiles
+// the grouped (batched) GEMM's tile width: its problems are small (K <= 512,
+// M, N from 16), where the narrower tile wastes less on padding and two CTAs
+// per SM overlap their epilogues
+constexpr int GROUPED_BN = 64;
 
 __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
   asm volatile(
@@ -256,8 +260,8 @@ dgemm_capped_kernel(int M, int N, int K, double alpha, const double *__restrict_
 // Grouped (batched, uneven) GEMM: a persistent grid walks the 128x128 tiles
 // of all problems; tile t belongs to problem order[p] where tile_start[p] <= t
 // < tile_start[p+1] (problems sorted by decreasing size on the host).
-template <bool TA, bool TB, int VEC>
-__global__ void __launch_bounds__(THREADS, 1)
+template <bool TA, bool TB, int VEC, int BNT>
+__global__ void __launch_bounds__(THREADS, TileCfg<BNT>::MINB)
 dgemm_grouped_kernel(const GemmProb *__restrict__ probs, const int *__restrict__ order,
                      const int *__restrict__ tile_start, int count, int *__restrict__ next) {
   extern __shared__ __align__(16) double smem[];
@@ -274,10 +278,10 @@ dgemm_grouped_kernel(const GemmProb *__restrict__ probs, const int *__restrict__
       if (tile_start[mid] <= t) lo = mid; else hi = mid - 1;
     }
     const GemmProb pr = probs[order[lo]];
-    const int local = t - tile_start[lo], tiles_n = (pr.N + BN - 1) / BN;
-    const int m0 = (local / tiles_n) * BM, n0 = (local % tiles_n) * BN;
-    dgemm_tile<TA, TB, VEC>(pr.M, pr.N, pr.K, pr.alpha, pr.A, pr.lda, pr.B, pr.ldb, pr.beta, pr.C,
-                            pr.ldc, 0, m0, n0, smem);
+    const int local = t - tile_start[lo], tiles_n = (pr.N + BNT - 1) / BNT;
+    const int m0 = (local / tiles_n) * BM, n0 = (local % tiles_n) * BNT;
+    dgemm_tile<TA, TB, VEC, BNT>(pr.M, pr.N, pr.K, pr.alpha, pr.A, pr.lda, pr.B, pr.ldb, pr.beta, pr.C,
+                                 pr.ldc, 0, m0, n0, smem);
     __syncthreads();  // shared memory is reused by the next tile
   }
 }
@@ -441,14 +445,17 @@ namespace {
 template <bool TA, bool TB, int VEC>
 void launch_grouped(const GemmProb *probs, const int *order, const int *tile_start, int count,
                     int *next, cudaStream_t st) {
-  constexpr int smem = TileCfg<BN>::template smem_doubles<TA, TB>() * (int)sizeof(double);
+  constexpr int smem = TileCfg<GROUPED_BN>::template smem_doubles<TA, TB>() * (int)sizeof(double);
   static bool configured = false;
   if (!configured) {
-    ATLB_CUDA_CHECK(cudaFuncSetAttribute(dgemm_grouped_kernel<TA, TB, VEC>,
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(dgemm_grouped_kernel<TA, TB, VEC, GROUPED_BN>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(dgemm_grouped_kernel<TA, TB, VEC, GROUPED_BN>,
+                                         cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     configured = true;
   }
-  dgemm_grouped_kernel<TA, TB, VEC><<<num_sms(), THREADS, smem, st>>>(probs, order, tile_start, count, next);
+  dgemm_grouped_kernel<TA, TB, VEC, GROUPED_BN><<<num_sms() * TileCfg<GROUPED_BN>::MINB, THREADS, smem, st>>>(
+      probs, order, tile_start, count, next);
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
 
@@ -464,7 +471,7 @@ void dgemm_grouped_dev(int ta, int tb, const GemmProb *hp, int count, cudaStream
   bool v2 = true;
   for (int i = 0; i < count; i++) {
     const GemmProb &p = hp[order[i]];
-    ts[i + 1] = ts[i] + ((p.M > 0 && p.N > 0) ? cdiv(p.M, BM) * cdiv(p.N, BN) : 0);
+    ts[i + 1] = ts[i] + ((p.M > 0 && p.N > 0) ? cdiv(p.M, BM) * cdiv(p.N, GROUPED_BN) : 0);
     v2 = v2 && al16(p.A, p.lda) && al16(p.B, p.ldb);
   }
   const size_t bytes = sizeof(GemmProb) * count + sizeof(int) * (2 * count + 1 + 16);
