@@ -149,44 +149,58 @@ void potrf_dev(int uplo, int N, T *A, long lda, int *dinfo, cudaStream_t st, Sge
         }
       }
     } else {
-      // Look-ahead of depth one (as in getrf): after the main stream's TRSM
-      // of block column k, the side stream updates and factors diagonal
-      // block k+1 while the main stream updates the rest of the trailing
-      // matrix (disjoint writes).
+      // Look-ahead of depth one.  The side stream owns the chain of diagonal
+      // blocks: once the main stream's wide update by block column k-1 is in
+      // (it covers diagonal block k+1), the side stream updates diagonal
+      // block k+1 by block column k, factors it, and -- once the main stream
+      // has updated block column k+1 below the diagonal by block column k --
+      // solves that block column (TRSM).  The main stream does that narrow
+      // update first, then the wide update of the rest of the trailing
+      // matrix, which overlaps the side stream's chain, so the TRSM is off
+      // the main stream.  Writes never overlap: diagonal block k+1 and block
+      // column k+1 below it (side), the trailing matrix beyond block column
+      // k+1 (main), block column k+1 below the diagonal (main's narrow
+      // update, ordered before the side's TRSM by an event).  Events:
+      // 0/1 narrow update k done, 2/3 block column k solved, 4/5 wide
+      // update k done.
       cudaStream_t s1 = side_stream();
+      auto blk = [&](int k) { return A + (long)k * NBO + (long)k * NBO * lda; };  // diagonal block k
+      auto trsm_col = [&](int k, cudaStream_t s) {  // block column k below its diagonal block
+        const int j = k * NBO, jb = std::min(NBO, N - j), nr = N - j - jb;
+        if (nr <= 0) return;
+        T *Ad = blk(k);
+        if (!up) trsm_dev<T>(kRight, kLower, kTrans, kNonUnit, nr, jb, T(1), Ad, lda, Ad + jb, lda, s, gemm);
+        else trsm_dev<T>(kLeft, kUpper, kTrans, kNonUnit, jb, nr, T(1), Ad, lda, Ad + (long)jb * lda, lda, s, gemm);
+      };
       potrf_rec<T>(up, 0, std::min(NBO, N), A, lda, dinfo, st, gemm);
+      trsm_col(0, st);
+      ATLB_CUDA_CHECK(cudaEventRecord(side_event(0), st));
+      ATLB_CUDA_CHECK(cudaStreamWaitEvent(s1, side_event(0), 0));  // block column 0 solved
       for (int k = 0; k < nblk - 1; k++) {
         const int j = k * NBO, jb = std::min(NBO, N - j), jn = j + jb, nr = N - jn;
         const int jbn = std::min(NBO, nr), nrest = nr - jbn;
-        T *Ad = A + j + (long)j * lda, *Dn = A + jn + (long)jn * lda;
-        if (k > 0) ATLB_CUDA_CHECK(cudaStreamWaitEvent(st, side_event(2 + (k & 1)), 0));  // block k factored
-        T *P;  // the TRSM'd block column (lower) / block row (upper) of block k
-        if (!up) {
-          P = Ad + jb;
-          trsm_dev<T>(kRight, kLower, kTrans, kNonUnit, nr, jb, T(1), Ad, lda, P, lda, st, gemm);
-        } else {
-          P = Ad + (long)jb * lda;
-          trsm_dev<T>(kLeft, kUpper, kTrans, kNonUnit, jb, nr, T(1), Ad, lda, P, lda, st, gemm);
+        T *Ad = blk(k), *Dn = A + jn + (long)jn * lda;
+        const T *P = up ? Ad + (long)jb * lda : Ad + jb;  // block column (row) k, solved
+        if (k > 0) ATLB_CUDA_CHECK(cudaStreamWaitEvent(st, side_event(2 + (k & 1)), 0));  // block column k solved
+        if (nrest > 0) {  // narrow update: block column k+1 below its diagonal block
+          if (!up) offdiag_update(gemm, kNoTrans, kTrans, nrest, jbn, jb, P + jbn, P, Dn + jbn, lda, st);
+          else offdiag_update(gemm, kTrans, kNoTrans, jbn, nrest, jb, P, P + (long)jbn * lda, Dn + (long)jbn * lda, lda, st);
         }
         ATLB_CUDA_CHECK(cudaEventRecord(side_event(k & 1), st));
-        ATLB_CUDA_CHECK(cudaStreamWaitEvent(s1, side_event(k & 1), 0));
         {
           SideScope side;
+          if (k > 0) ATLB_CUDA_CHECK(cudaStreamWaitEvent(s1, side_event(4 + ((k - 1) & 1)), 0));  // wide update k-1 in
           syrk_update(gemm, up, jbn, jb, P, Dn, lda, s1);   // diagonal block k+1
           potrf_rec<T>(up, jn, jbn, A, lda, dinfo, s1, gemm);
+          ATLB_CUDA_CHECK(cudaStreamWaitEvent(s1, side_event(k & 1), 0));  // its block column updated
+          trsm_col(k + 1, s1);
           ATLB_CUDA_CHECK(cudaEventRecord(side_event(2 + ((k + 1) & 1)), s1));
         }
-        if (nrest > 0) {
-          if (!up) {
-            const T *Pn = P, *Pr = P + jbn;          // rows of block k+1 / below it
-            offdiag_update(gemm, kNoTrans, kTrans, nrest, jbn, jb, Pr, Pn, Dn + jbn, lda, st);
-            syrk_update(gemm, 0, nrest, jb, Pr, Dn + jbn + (long)jbn * lda, lda, st);
-          } else {
-            const T *Pn = P, *Pr = P + (long)jbn * lda;  // columns of block k+1 / right of it
-            offdiag_update(gemm, kTrans, kNoTrans, jbn, nrest, jb, Pn, Pr, Dn + (long)jbn * lda, lda, st);
-            syrk_update(gemm, 1, nrest, jb, Pr, Dn + jbn + (long)jbn * lda, lda, st);
-          }
+        if (nrest > 0) {  // wide update: the trailing matrix beyond block column k+1
+          if (!up) syrk_update(gemm, 0, nrest, jb, P + jbn, Dn + jbn + (long)jbn * lda, lda, st);
+          else syrk_update(gemm, 1, nrest, jb, P + (long)jbn * lda, Dn + jbn + (long)jbn * lda, lda, st);
         }
+        ATLB_CUDA_CHECK(cudaEventRecord(side_event(4 + (k & 1)), st));
       }
       ATLB_CUDA_CHECK(cudaStreamWaitEvent(st, side_event(2 + ((nblk - 1) & 1)), 0));  // join
     }

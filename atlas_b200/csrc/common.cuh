@@ -40,7 +40,7 @@ void *pinned(int slot, size_t bytes);
 // thread, scratch() and pinned() hand out a second set of buffers, so work
 // enqueued on the two streams never shares a workspace.
 cudaStream_t side_stream();
-cudaEvent_t side_event(int i);  // four reusable events per thread (i < 4)
+cudaEvent_t side_event(int i);  // eight reusable events per thread (i < 8)
 struct SideScope {
   SideScope();
   ~SideScope();

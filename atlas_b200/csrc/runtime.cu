@@ -22,7 +22,7 @@ struct ThreadState {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   cudaStream_t side = nullptr;
-  cudaEvent_t events[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t events[8] = {};
   Buf dev[2 * kNumSlots];   // second half: buffers of work on the side stream
   Buf host[2 * kNumSlots];
   ~ThreadState() {
