@@ -215,7 +215,7 @@ void potrs_dev(int uplo, int N, int NRHS, const T *A, long lda, T *B, long ldb, 
                SgemmFn gemm) {
   // ATL_potrs column-major (src/lapack/ATL_potrs.c:41-60)
   if (N <= 0 || NRHS <= 0) return;
-  if (NRHS <= 8) {  // few right-hand sides: one-launch blocked solves
+  if (NRHS <= kTrsvMaxRhs) {  // few right-hand sides: blocked solves, one launch per 8 columns
     if (uplo == kUpper) {
       trsv_dev<T>(kUpper, kTrans, kNonUnit, N, NRHS, A, lda, B, ldb, st);
       trsv_dev<T>(kUpper, kNoTrans, kNonUnit, N, NRHS, A, lda, B, ldb, st);

@@ -67,7 +67,10 @@ void trsm_impl(int side, int uplo, int trans, int diag, int M, int N, T alpha, c
 // (n x n), block b stored dense 64x64 column-major at W + b*4096.
 template <typename T>
 void trinv_dev(int n, const T *Tp, long tr, long tc, int lower, int unit, T *W, cudaStream_t st);
-// op(A) X = B (Left side) for nrhs <= 8 in one launch.
+// op(A) X = B (Left side): one launch per 8 right-hand sides, the inverted
+// diagonal blocks computed once.  getrs / potrs take this path up to
+// kTrsvMaxRhs right-hand sides, the recursive TRSM above.
+constexpr int kTrsvMaxRhs = 32;
 template <typename T>
 void trsv_dev(int uplo, int trans, int diag, int n, int nrhs, const T *A, long lda, T *B, long ldb,
               cudaStream_t st);

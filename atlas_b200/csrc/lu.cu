@@ -1066,7 +1066,7 @@ void getrs_dev(int trans, int N, int NRHS, const T *A, long lda, const int *ipiv
                cudaStream_t st, SgemmFn gemm) {
   // ATL_getrs column-major (src/lapack/ATL_getrs.c:34-50)
   if (N <= 0 || NRHS <= 0) return;
-  if (NRHS <= 8) {  // few right-hand sides: one-launch blocked solves
+  if (NRHS <= kTrsvMaxRhs) {  // few right-hand sides: blocked solves, one launch per 8 columns
     if (trans == kNoTrans) {
       laswp_dev<T>(NRHS, B, ldb, 0, N, ipiv, 1, st);
       trsv_dev<T>(kLower, kNoTrans, kUnit, N, NRHS, A, lda, B, ldb, st);

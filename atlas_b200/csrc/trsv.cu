@@ -329,14 +329,16 @@ void trsv_inverse_dev(int uplo, int trans, int diag, int n, const T *A, long lda
 template void trsv_inverse_dev<double>(int, int, int, int, const double *, long, double *, cudaStream_t);
 template void trsv_inverse_dev<float>(int, int, int, int, const float *, long, float *, cudaStream_t);
 
-// Solve op(A) X = B in place for nrhs <= 8 right-hand sides (Left side only).
+// Solve op(A) X = B in place (Left side only): the inverted diagonal blocks
+// once, then one launch per 8 right-hand sides.
 template <typename T>
 void trsv_dev(int uplo, int trans, int diag, int n, int nrhs, const T *A, long lda, T *B, long ldb,
               cudaStream_t st) {
   if (n <= 0 || nrhs <= 0) return;
   T *W = (T *)scratch(kSlotTrsmW, sizeof(T) * trsv_w_elems(n));
   trsv_inverse_dev<T>(uplo, trans, diag, n, A, lda, W, st);
-  trsv_w_dev<T>(uplo, trans, n, nrhs, A, lda, W, B, ldb, st);
+  for (int c0 = 0; c0 < nrhs; c0 += 8)
+    trsv_w_dev<T>(uplo, trans, n, std::min(8, nrhs - c0), A, lda, W, B + (long)c0 * ldb, ldb, st);
 }
 template void trsv_dev<double>(int, int, int, int, int, const double *, long, double *, long, cudaStream_t);
 template void trsv_dev<float>(int, int, int, int, int, const float *, long, float *, long, cudaStream_t);
