@@ -296,9 +296,18 @@ __global__ void __launch_bounds__(256) larft_kernel(int k, const double *G, long
   double *S = lft_smem;                      // k x k, ld LFT_LD: G, then T
   double *W = lft_smem + NBQ_MAX * LFT_LD;   // products G12 T2 of one level (<= NBQ_MAX^2 / 4 doubles)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int idx = tid; idx < k * k; idx += 256) {
-    const int r = idx % k, c = idx / k;
-    S[r + c * LFT_LD] = r < c ? G[r + (long)c * ldg] : 0.0;
+  for (int base = 0; base < k * k; base += 256 * 8) {  // eight loads in flight per thread
+    double v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int idx = base + u * 256 + tid, r = idx % k, c = idx / k;
+      v[u] = (idx < k * k && r < c) ? G[r + (long)c * ldg] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int idx = base + u * 256 + tid;
+      if (idx < k * k) S[idx % k + (idx / k) * LFT_LD] = v[u];
+    }
   }
   __syncthreads();
   for (int b = warp; b * 16 < k; b += 8) {   // diagonal blocks by the recurrence
@@ -435,11 +444,21 @@ __global__ void __launch_bounds__(256) qr_leaf_apply_kernel(int m, int kb, int n
   __shared__ double sT[KB][KB + 1];
   __shared__ double sW[KB][NBQ_MAX + 1];  // W = V^T C, then Y = T^T W in its place
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  for (int idx = tid; idx < KB * (kb + n2); idx += 256) {
-    const int a = idx % KB, b = idx / KB;
-    const double v = a < kb ? P[a + b * KB] : 0.0;
-    if (b < kb) sT[a][b] = v;  // G = V^T V for now
-    else sW[a][b - kb] = v;
+  for (int base = 0; base < KB * (kb + n2); base += 256 * 8) {  // eight loads in flight per thread
+    const int tot = KB * (kb + n2);
+    double v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int idx = base + u * 256 + tid, a = idx % KB;
+      v[u] = (idx < tot && a < kb) ? P[idx] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int idx = base + u * 256 + tid, a = idx % KB, b = idx / KB;
+      if (idx >= tot) continue;
+      if (b < kb) sT[a][b] = v[u];  // G = V^T V for now
+      else sW[a][b - kb] = v[u];
+    }
   }
   __syncthreads();
   if (w == 0) {  // T from G (upper; the recurrence overwrites G's strictly upper part)
