@@ -40,6 +40,26 @@ struct Prob {
   int n, lda, ldb, nrhs;
 };
 
+// dst (rows x cols, ld ldd, shared memory) = src (ld lds, global), eight
+// loads in flight per thread before their stores (a plain strided loop would
+// wait for each load in turn)
+__device__ __forceinline__ void stage_tile(double *dst, int ldd, const double *src, long lds, int rows, int cols) {
+  const int tot = rows * cols, tid = threadIdx.x;
+  for (int base = 0; base < tot; base += BT * 8) {
+    double v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int idx = base + u * BT + tid;
+      v[u] = idx < tot ? src[idx % rows + (long)(idx / rows) * lds] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int idx = base + u * BT + tid;
+      if (idx < tot) dst[idx % rows + (idx / rows) * ldd] = v[u];
+    }
+  }
+}
+
 // ---------------------------------------------------------------- Cholesky
 
 // Triangular solve of one right-hand side held in shared memory (b, n <=
@@ -118,7 +138,7 @@ batched_posv_kernel(const Prob *__restrict__ probs, const int *__restrict__ orde
     int fail = 0;
     if (n <= SMALL) {
       const int lds = cholb::ld_for(n);
-      for (int idx = tid; idx < n * n; idx += BT) sm[idx % n + (idx / n) * lds] = pr.A[idx % n + (long)(idx / n) * pr.lda];
+      stage_tile(sm, lds, pr.A, pr.lda, n, n);
       __syncthreads();
       fail = cholb::chol_smem(sm, lds, n);
       for (int idx = tid; idx < n * n; idx += BT) {
@@ -132,8 +152,7 @@ batched_posv_kernel(const Prob *__restrict__ probs, const int *__restrict__ orde
       // then update the trailing lower triangle in global memory
       for (int j = 0; j < n && !fail; j += PW) {
         const int jb = min(PW, n - j), m = n - j, lds = cholb::ld_for(m);
-        for (int idx = tid; idx < m * jb; idx += BT)
-          sm[idx % m + (idx / m) * lds] = pr.A[j + idx % m + (long)(j + idx / m) * pr.lda];
+        stage_tile(sm, lds, pr.A + j + (long)j * pr.lda, pr.lda, m, jb);
         __syncthreads();
         {
           const int f = cholb::chol_panel(sm, lds, m, jb);
@@ -302,10 +321,7 @@ __device__ int lu_blocked(const Prob &pr, LuSmem &S) {
   if (tid == 0) S.fail = 0;
   for (int j = 0; j < n; j += LPW) {
     const int jb = min(LPW, n - j), m = n - j, nt = n - j - jb;
-    for (int idx = tid; idx < m * jb; idx += BT) {
-      const int i = idx % m, c = idx / m;
-      S.P[i + c * LU_LDP] = A[(j + i) + (long)(j + c) * lda];
-    }
+    stage_tile(S.P, LU_LDP, A + j + (long)j * lda, lda, m, jb);
     __syncthreads();
     const int f = lu_panel(S, m, jb);
     if (tid == 0 && f && !S.fail) S.fail = j + f;

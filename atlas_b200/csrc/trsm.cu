@@ -668,9 +668,18 @@ trsm_llu_small_kernel(int m, int n, const T *__restrict__ L, long lda, T *B, lon
   T(*sL)[33] = reinterpret_cast<T(*)[33]>(sX + LLU_MAX);                  // [32]: one tile of L
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int c0 = blockIdx.x * LLU_COLS, nc = min(LLU_COLS, n - c0);
-  for (int idx = tid; idx < LLU_MAX * LLU_COLS; idx += 256) {
-    const int r = idx % LLU_MAX, c = idx / LLU_MAX;
-    sX[r][c] = (r < m && c < nc) ? B[r + (long)(c0 + c) * ldb] : T(0);
+  for (int base = 0; base < LLU_MAX * LLU_COLS; base += 256 * 8) {  // eight loads in flight per thread
+    T v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int idx = base + u * 256 + tid, r = idx % LLU_MAX, c = idx / LLU_MAX;
+      v[u] = (r < m && c < nc) ? B[r + (long)(c0 + c) * ldb] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int idx = base + u * 256 + tid;
+      sX[idx % LLU_MAX][idx / LLU_MAX] = v[u];
+    }
   }
   const int nblk = (m + 31) / 32;
   const int rr = tid % 32, cq = tid / 32;  // update: row rr of the block, columns 4 cq .. 4 cq + 3
