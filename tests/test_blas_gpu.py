@@ -1,6 +1,6 @@
 """Parity of the GPU level-3 BLAS with the reference: the reference's own C
 BLAS outputs (tests/golden/ref_blas.npz) and the oracle, through the C ABI
-with host buffers (the drop-in path), judged by bin/l3blastst.c's residual
+with host buffers (the drop-in path), checked by bin/l3blastst.c's residual
 (< 50) plus an elementwise tolerance, with the lda gaps checked for stray
 writes (ATL_gechkgap)."""
 import os
