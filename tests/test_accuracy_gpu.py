@@ -23,6 +23,7 @@ def _factors(n, seed):
 
 @pytest.mark.parametrize("n,nrhs,trans", [(1000, 1, NOTRANS), (4096, 1, NOTRANS), (4096, 3, NOTRANS),
                                           (4096, 8, NOTRANS), (3000, 1, TRANS), (2500, 12, NOTRANS),
+                                          (2048, 29, TRANS), (1500, 32, NOTRANS), (1500, 33, NOTRANS),
                                           (8192, 1, NOTRANS)])
 def test_getrs_matches_substitution(gpu, n, nrhs, trans):
     import scipy.linalg as sl

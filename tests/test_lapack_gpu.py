@@ -135,6 +135,22 @@ def test_potrf_not_spd_info(gpu, orc, bad):
 
 
 @pytest.mark.parametrize("uplo", [121, 122])
+@pytest.mark.parametrize("r", [13, 32, 40])
+def test_potrs_many_rhs(gpu, orc, uplo, r):
+    """13 and 32 right-hand sides take the one-launch solves in chunks of 8
+    columns, 40 the recursive TRSM: the same solution either way."""
+    n = 700
+    a0 = orc.spd_matrix(n, 31)
+    xt = orc.uniform((n, r), 32)
+    f = a0.copy(order="F")
+    assert AB.clapack_dpotrf(CM, uplo, n, f, n) == 0
+    x = np.array(a0 @ xt, order="F")
+    assert AB.clapack_dpotrs(CM, uplo, n, r, f, n, x, n) == 0
+    assert orc.resid_slv(a0, x, xt) <= 100.0
+    np.testing.assert_allclose(x, xt, rtol=1e-9, atol=1e-9)
+
+
+@pytest.mark.parametrize("uplo", [121, 122])
 def test_potrs_posv(gpu, orc, uplo):
     n, r = 300, 4
     a0 = orc.spd_matrix(n, 21)
