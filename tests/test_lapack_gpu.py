@@ -279,6 +279,36 @@ def test_geqrf_vs_reference_lapack_golden(gpu):
         assert GL.close(tau[:min(m, n)], tau_ref, 1e-10), f"geqrf case {i}"
 
 
+@pytest.mark.parametrize("m,n", [(300, 900), (900, 300), (257, 385), (129, 129), (640, 129)])
+def test_geqrf_lookahead_shapes_vs_oracle(gpu, orc, m, n):
+    """Wide, tall and ragged shapes through the look-ahead driver: the last
+    panel narrower than the others, a wide matrix whose columns beyond
+    min(m, n) get only the block reflectors, a single extra column."""
+    a0 = orc.normal((m, n), 3 * m + n)
+    a = a0.copy(order="F")
+    tau = np.zeros(min(m, n))
+    assert AB.clapack_dgeqrf(CM, m, n, a, m, tau) == 0
+    qr, rtau = orc.dgeqrf(a0.copy(order="F"))
+    np.testing.assert_allclose(tau, rtau, rtol=1e-9, atol=1e-11)
+    np.testing.assert_allclose(np.triu(a), np.triu(qr), rtol=1e-9, atol=1e-10)
+    np.testing.assert_allclose(np.tril(a, -1), np.tril(qr, -1), rtol=1e-8, atol=1e-10)
+    assert orc.resid_qr(a0, a.copy(order="F"), tau) <= 100.0
+
+
+@pytest.mark.parametrize("n", [129, 300, 513])
+@pytest.mark.parametrize("uplo", [121, 122])
+def test_potrf_lookahead_sizes_vs_oracle(gpu, orc, n, uplo):
+    """Orders just past one, two and four 128-column blocks through the
+    Cholesky look-ahead (the last block narrow), both triangles."""
+    a0 = orc.spd_matrix(n, 7 * n)
+    a = a0.copy(order="F")
+    assert AB.clapack_dpotrf(CM, uplo, n, a, n) == 0
+    f = a0.copy(order="F")
+    assert orc.dpotrf(uplo, f) == 0
+    tri = np.triu if uplo == 121 else np.tril
+    np.testing.assert_allclose(tri(a), tri(f), rtol=1e-10, atol=1e-11)
+
+
 @pytest.mark.parametrize("nb", [64, 256])
 @pytest.mark.parametrize("la", [0, 1])
 def test_geqrf_panel_widths_vs_oracle(gpu, orc, nb, la):
