@@ -121,7 +121,13 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 // the stage's B tile, into MS accumulators side by side in TMEM (MS * BN
 // columns); a 256 x 256 tile moves half the operand bytes per product of a
 // 128 x 256 one.
-template <int KIND, int BN, int STAGES, int EPI, int MS = 1>
+//
+// SPLIT (TF32 only): each operand row holds two planes of K elements, the
+// TF32 high parts at columns [0, K) and the TF32 remainders at [K, 2K).  A
+// stage carries both planes of A and of B, and each k-step issues the three
+// products hi*hi, lo*hi and hi*lo into the one accumulator: the operands
+// cross L2 once per plane instead of once per product.
+template <int KIND, int BN, int STAGES, int EPI, int MS = 1, int SPLIT = 0>
 __global__ void __launch_bounds__(THREADS, 1)
 tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                int M, int N, int K, EpiParams ep, int *err) {
@@ -130,7 +136,11 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   constexpr int BMT = BM * MS;  // rows of the CTA's tile
   static_assert(MS * BN <= 512, "TMEM holds 512 columns");
-  constexpr int A_BYTES = BMT * SLAB, B_BYTES = BN * SLAB, STAGE = A_BYTES + B_BYTES;
+  static_assert(!SPLIT || KIND == kKindTF32, "split operands are TF32 pairs");
+  constexpr int NP = SPLIT ? 2 : 1;  // planes per operand
+  constexpr int NPROD = SPLIT ? 3 : 1;
+  // stage: A plane 0 [, A plane 1], B plane 0 [, B plane 1], each 1024-byte aligned
+  constexpr int A_BYTES = BMT * SLAB, B_BYTES = BN * SLAB, STAGE = NP * (A_BYTES + B_BYTES);
   uint64_t *bars = (uint64_t *)(smem + STAGES * STAGE);
   uint32_t *tmem_slot = (uint32_t *)(bars + 2 * STAGES + 1);
   const uint32_t sbase = smem_u32(smem);
@@ -175,8 +185,12 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       const uint32_t ph = (kb / STAGES) & 1;
       if (kb >= STAGES && !mbar_wait(bar_empty + 8 * s, ph ^ 1, TO)) { atomicExch(err, 1); break; }
       mbar_expect_tx(bar_full + 8 * s, STAGE);
-      tma_load_2d(sbase + s * STAGE, &tmA, kb * KPS, m0, bar_full + 8 * s);
-      tma_load_2d(sbase + s * STAGE + A_BYTES, &tmB, kb * KPS, n0, bar_full + 8 * s);
+#pragma unroll
+      for (int p = 0; p < NP; p++) {
+        tma_load_2d(sbase + s * STAGE + p * A_BYTES, &tmA, p * K + kb * KPS, m0, bar_full + 8 * s);
+        tma_load_2d(sbase + s * STAGE + NP * A_BYTES + p * B_BYTES, &tmB, p * K + kb * KPS, n0,
+                    bar_full + 8 * s);
+      }
     }
   } else if (warp == 1 && lane == 0) {
     // MMA issuer
@@ -187,13 +201,17 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       const uint32_t ph = (kb / STAGES) & 1;
       if (!mbar_wait(bar_full + 8 * s, ph, TO)) { atomicExch(err, 2); ok = false; break; }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t a_addr = sbase + s * STAGE, b_addr = a_addr + A_BYTES;
+      const uint32_t a_addr = sbase + s * STAGE, b_addr = a_addr + NP * A_BYTES;
 #pragma unroll
       for (int k = 0; k < KPS / KPM; k++) {
 #pragma unroll
-        for (int ms = 0; ms < MS; ms++)
-          mma_issue<KIND>(tmem + ms * BN, smem_desc(a_addr + ms * BM * SLAB + k * 32), smem_desc(b_addr + k * 32),
-                          idesc, (kb > 0 || k > 0) ? 1u : 0u);
+        for (int q = 0; q < NPROD; q++) {  // planes of (A, B): (0, 0), then (1, 0), (0, 1)
+          const uint32_t pa = q == 1 ? A_BYTES : 0, pb = q == 2 ? B_BYTES : 0;
+#pragma unroll
+          for (int ms = 0; ms < MS; ms++)
+            mma_issue<KIND>(tmem + ms * BN, smem_desc(a_addr + pa + ms * BM * SLAB + k * 32),
+                            smem_desc(b_addr + pb + k * 32), idesc, (kb > 0 || k > 0 || q > 0) ? 1u : 0u);
+        }
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                    ::"r"(bar_empty + 8 * s) : "memory");
@@ -319,17 +337,19 @@ int *err_flag() {
   return d;
 }
 
-template <int KIND, int BN, int STAGES, int EPI, int MS = 1>
+// SPLIT: A and B rows hold two K-element planes (K a multiple of 32)
+template <int KIND, int BN, int STAGES, int EPI, int MS = 1, int SPLIT = 0>
 void launch_t(const void *A, long lda, const void *B, long ldb, int M, int N, int K,
               const EpiParams &ep, cudaStream_t st) {
+  constexpr int NP = SPLIT ? 2 : 1;
   CUtensorMap ma, mb;
-  if (!make_map(&ma, KIND, A, M, K, lda, BM * MS) || !make_map(&mb, KIND, B, N, K, ldb, BN)) {
+  if (!make_map(&ma, KIND, A, M, NP * K, lda, BM * MS) || !make_map(&mb, KIND, B, N, NP * K, ldb, BN)) {
     fprintf(stderr, "atlas_b200: tensor-map encoding failed (alignment)\n");
     set_cuda_error(cudaErrorInvalidValue);
     return;
   }
-  constexpr int smem = STAGES * (BM * MS + BN) * SLAB + 1024 + (2 * STAGES + 2) * 8 + 16;
-  auto kern = tc_gemm_kernel<KIND, BN, STAGES, EPI, MS>;
+  constexpr int smem = STAGES * NP * (BM * MS + BN) * SLAB + 1024 + (2 * STAGES + 2) * 8 + 16;
+  auto kern = tc_gemm_kernel<KIND, BN, STAGES, EPI, MS, SPLIT>;
   static bool configured = false;
   if (!configured) {
     ATLB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -355,6 +375,17 @@ void tc_gemm(int kind, int epi, const void *A, long lda, const void *B, long ldb
     // per product of 128 x 128 tiles
     if (epi == kEpiF64Acc) launch_t<kKindI8, 256, 3, kEpiF64Acc, 2>(A, lda, B, ldb, M, N, K, ep, st);
   }
+}
+
+// The split-TF32 product of two-plane operands (rows of 2 * ldk elements,
+// ldk a multiple of 32).
+void tc_gemm_split(const float *A2, const float *B2, long ldk, int M, int N, const EpiParams &ep,
+                   cudaStream_t st) {
+  if (M <= 0 || N <= 0) return;
+  // 128 x 64 tiles, 2 stages of both planes (96 KB): two CTAs per SM, so one
+  // CTA's epilogue runs under the other's products, and each CTA retires
+  // after one tile, which keeps SMs turning over for the look-ahead stream
+  launch_t<kKindTF32, 64, 2, kEpiF32, 1, 1>(A2, 2 * ldk, B2, 2 * ldk, M, N, (int)ldk, ep, st);
 }
 
 int read_and_clear_error(cudaStream_t st) {
@@ -406,18 +437,16 @@ __global__ void to_kmajor_kernel(int rows, int K, const float *__restrict__ X, l
   }
 }
 
-// 3xTF32: op(X) -> rows of [p0 | p1 | p2] K-blocks (each ldk wide) where
-// block q holds the TF32-rounded high part (pat bit q = 0) or the
-// TF32-rounded remainder x - hi(x) (bit q = 1).  A uses [hi lo hi], B uses
-// [hi hi lo], so one GEMM over K' = 3*ldk sums hi*hi + lo*hi + hi*lo, the
-// FP32-accurate product (the lo*lo term is below FP32 rounding).
+// 3xTF32: op(X) -> rows of two K-planes, each ldk wide: the TF32-rounded
+// high part hi(x) at [0, ldk) and the TF32-rounded remainder x - hi(x) at
+// [ldk, 2 ldk).  The split GEMM sums hi*hi + lo*hi + hi*lo, the FP32-accurate
+// product (the lo*lo term is below FP32 rounding).
 struct SplitOperand {
   int rows, K;
   const float *X;
   long ld;
   int rcontig;  // X(r, k) at r + k*ld (else k + r*ld)
   float *out;
-  int pat;
 };
 // Both operands of one GEMM in one launch: CTAs with blockIdx.y < ya convert
 // A's 32 x 32 tiles, the others B's.  Each thread's four loads are issued
@@ -453,9 +482,9 @@ to_kmajor_split_kernel(SplitOperand opa, SplitOperand opb, int ya, long ldk) {
       asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(x));
       const float rem = x - __uint_as_float(hi);
       asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(rem));
-      float *o = op.out + (long)r * 3 * ldk + k;
-#pragma unroll
-      for (int e = 0; e < 3; e++) o[e * ldk] = __uint_as_float(((op.pat >> e) & 1) ? lo : hi);
+      float *o = op.out + (long)r * 2 * ldk + k;
+      o[0] = __uint_as_float(hi);
+      o[ldk] = __uint_as_float(lo);
     }
   }
 }
@@ -469,21 +498,21 @@ void sgemm_tf32x3(int ta, int tb, int M, int N, int K, float alpha, const float 
     sgemm_dev(ta, tb, M, N, 0, alpha, A, lda, B, ldb, beta, C, ldc, st, tri);
     return;
   }
-  // each K-block padded to a whole 32-element TMA slab so the three blocks line up
+  // each K-plane padded to a whole 32-element TMA slab so the two planes line up
   const long ldk = (long)cdiv(K, 32) * 32;
-  const size_t abytes = (size_t)M * 3 * ldk * 4, bbytes = (size_t)N * 3 * ldk * 4;
+  const size_t abytes = (size_t)M * 2 * ldk * 4, bbytes = (size_t)N * 2 * ldk * 4;
   unsigned char *buf = (unsigned char *)scratch(kSlotTc0, abytes + bbytes + 256);
   float *Ak = (float *)buf;
   float *Bk = (float *)(buf + ((abytes + 255) / 256) * 256);
   if (ldk != K) {  // zero the K padding once per call
     ATLB_CUDA_CHECK(cudaMemsetAsync(buf, 0, abytes + bbytes + 256, st));
   }
-  const SplitOperand opa = {M, K, A, lda, ta == kNoTrans, Ak, 0b010};
-  const SplitOperand opb = {N, K, B, ldb, tb != kNoTrans, Bk, 0b100};
+  const SplitOperand opa = {M, K, A, lda, ta == kNoTrans, Ak};
+  const SplitOperand opb = {N, K, B, ldb, tb != kNoTrans, Bk};
   const int ya = cdiv(M, 32);
   to_kmajor_split_kernel<<<dim3(cdiv(K, 32), ya + cdiv(N, 32)), dim3(32, 8), 0, st>>>(opa, opb, ya, ldk);
   ATLB_CUDA_CHECK(cudaGetLastError());
-  tc_gemm(kKindTF32, kEpiF32, Ak, 3 * ldk, Bk, 3 * ldk, M, N, (int)(3 * ldk), ep, st);
+  tc_gemm_split(Ak, Bk, ldk, M, N, ep, st);
 }
 
 template <int KIND>

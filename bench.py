@@ -266,8 +266,9 @@ def peak_tf32_tflops():
 def headline_roofline(torch, AB, dev, stream):
     """Roofline of the headline's tensor-core kernel: the split-TF32 GEMM of the
     FP32 factorization's first trailing update (M = 7936, N = 7680, K = 256;
-    A and B split into TF32 high and low parts, three products = K 768 on the
-    tensor cores), timed with CUDA events on the library's stream over 10 calls
+    A and B each split into a TF32 high and a TF32 low plane, three products
+    hi*hi + lo*hi + hi*lo on the tensor cores), timed with CUDA events on the
+    library's stream over 10 calls
     (each call also runs the operand-split kernel).  Algorithmic work per call:
     2 * M * N * (3 K) TF32 flop.  Beside it, the latency of the FP32 leaf panel
     (one 8192 x 32 panel through atlb_sgetrf_dev) per column."""
@@ -412,6 +413,7 @@ def extra_factorizations(torch, AB, dev, stream):
         Q.copy_(q0)
         AB.atlb_dgeqrf_dev(m, nq, Q, m, tau)
     qr()
+    qr()   # the second call captures the factorization's graph; timed calls replay it
     ms = timed(torch, stream, qr, 2)
     flop = 2.0 * m * nq ** 2 - 2.0 / 3.0 * nq ** 3
     res["dgeqrf_16384x8192"] = {"ms": ms, "gflops": flop / ms / 1e6}
@@ -433,6 +435,7 @@ def extra_kappa(torch, AB, dev, stream, n):
             AB.atlb_dsgesv_ex(n, 1, acol, n, ipiv, b, n, x, n, prec, 0, it)
             if it[0] < 0:
                 acol.copy_(a0)
+        call()
         call()
         ms = timed(torch, stream, call, 2)
         res[name] = {"ms": ms, "iter": int(it[0]), "backward_error": backward_error(torch, a0, x, b)}
@@ -617,6 +620,7 @@ def extra_adjoints(torch, AB, dev, stream):
         AB.atlb_dpotrf_adjoint_dev(n, L, n, Lbar, n, Abar, n)
         AB.atlb_dpotrs_adjoint_dev(n, 1, L, n, x, n, y, n, Bbar, n, Abar, n)
     fwd_bwd()
+    fwd_bwd()   # graphs are captured on the second call and replayed from the third
     ms = timed(torch, stream, fwd_bwd, 3)
     ainv = torch.linalg.inv(a)
     av = ainv @ y
@@ -639,6 +643,7 @@ def extra_adjoints(torch, AB, dev, stream):
         AB.atlb_dgetrs_dev(111, n, 1, LU, n, ipiv, xv, n)
         Abar2.zero_()
         AB.atlb_dgetrs_adjoint_dev(n, 1, LU, n, ipiv, xv, n, cv, n, Bbar, n, Abar2, n)
+    lu_fwd_bwd()
     lu_fwd_bwd()
     ms2 = timed(torch, stream, lu_fwd_bwd, 3)
     closed2 = -torch.outer(torch.linalg.solve(ag.T, cv), torch.linalg.solve(ag, bv))
@@ -670,6 +675,7 @@ def extra_adjoints(torch, AB, dev, stream):
         Lb.diagonal(dim1=1, dim2=2).copy_(2.0 / Lw.diagonal(dim1=1, dim2=2))
         AB.atlb_dpotrf_adjoint_batched_dev(cnt, nv, pL, nv, pLb, nv, pAb, nv)
         AB.atlb_dpotrs_adjoint_batched_dev(cnt, nv, ones, pL, nv, pX, nv, pY, nv, pBb, nv, pAb, nv)
+    batched_fwd_bwd()
     batched_fwd_bwd()
     ms3 = timed(torch, stream, batched_fwd_bwd, 3)
     ainv = torch.linalg.inv(A0)
