@@ -39,8 +39,8 @@ void sgemm_tf32_dev(int ta, int tb, int M, int N, int K, float alpha, const floa
 void sgemm_bf16_dev(int ta, int tb, int M, int N, int K, float alpha, const float *A, long lda,
                     const float *B, long ldb, float beta, float *C, long ldc, cudaStream_t st,
                     int tri);
-// FP32-accurate GEMM on the TF32 tensor cores (operands split into TF32 high
-// and low parts, three products summed in one K-concatenated GEMM).
+// Near-FP32 GEMM on the TF32 tensor cores (operands split into TF32 high and
+// low planes, three products per k-step into one accumulator).
 void sgemm_tf32x3_dev(int ta, int tb, int M, int N, int K, float alpha, const float *A, long lda,
                       const float *B, long ldb, float beta, float *C, long ldc, cudaStream_t st,
                       int tri);

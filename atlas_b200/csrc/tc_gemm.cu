@@ -439,8 +439,10 @@ __global__ void to_kmajor_kernel(int rows, int K, const float *__restrict__ X, l
 
 // 3xTF32: op(X) -> rows of two K-planes, each ldk wide: the TF32-rounded
 // high part hi(x) at [0, ldk) and the TF32-rounded remainder x - hi(x) at
-// [ldk, 2 ldk).  The split GEMM sums hi*hi + lo*hi + hi*lo, the FP32-accurate
-// product (the lo*lo term is below FP32 rounding).
+// [ldk, 2 ldk).  The split GEMM sums hi*hi + lo*hi + hi*lo (the lo*lo term is
+// below FP32 rounding); the tensor cores' FP32 accumulation then bounds the
+// accuracy: measured against FP64, 2.3e-6 at K = 256 and 5.5e-5 at K = 8192,
+// where FP32 FMA gives 4.2e-6.
 struct SplitOperand {
   int rows, K;
   const float *X;

@@ -351,6 +351,52 @@ def extra_sharded(torch, AB, dev, stream, rank, world):
     return out
 
 
+def extra_sgemm(torch, AB, dev, stream, M):
+    """FP32 GEMM M^3: cblas_sgemm (the reference's entry point; FP32 FMA on the
+    SIMT pipes, device pointers), cuBLAS FP32 with TF32 off in the same run,
+    and the split-TF32 tensor-core product (atlb_sgemm_tc_dev precision 3).
+    Errors: max |C - C_fp64| / max |C_fp64| on 256 rows of C."""
+    f32 = torch.float32
+    g = torch.Generator(device=dev)
+    g.manual_seed(21)
+    sa = torch.rand(M, M, dtype=f32, device=dev, generator=g) * 2 - 1   # column-major storage
+    sb = torch.rand(M, M, dtype=f32, device=dev, generator=g) * 2 - 1
+    sc = torch.zeros(M, M, dtype=f32, device=dev)
+    rows = torch.arange(0, M, M // 256, device=dev)[:256]
+    # column-major storage: logical A = sa^T, B = sb^T, C = sc^T; the sample is C[rows, :]
+    ref = sa.T[rows].double() @ sb.T.double()
+    flop = 2.0 * M ** 3
+
+    def err():
+        c_rows = sc.T[rows].double()
+        return ((c_rows - ref).abs().max() / ref.abs().max()).item()
+
+    out = {}
+    simt = lambda: AB.cblas_sgemm(102, 111, 111, M, M, M, 1.0, sa, M, sb, M, 0.0, sc, M)
+    for _ in range(2):
+        simt()
+    ms = timed(torch, stream, simt, 3)
+    out["cblas_sgemm"] = {"ms": ms, "tflops": flop / ms / 1e9, "rel_err_vs_fp64": err(),
+                          "path": "FP32 FMA on the SIMT pipes"}
+    tc3 = lambda: AB.atlb_sgemm_tc_dev(3, 111, 111, M, M, M, 1.0, sa, M, sb, M, 0.0, sc, M)
+    for _ in range(2):
+        tc3()
+    ms = timed(torch, stream, tc3, 3)
+    out["split_tf32"] = {"ms": ms, "tflops": flop / ms / 1e9, "rel_err_vs_fp64": err(),
+                         "path": "atlb_sgemm_tc_dev precision 3: hi*hi + lo*hi + hi*lo on tcgen05"}
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    # the storage of C = A B is sb @ sa (row-major), all contiguous
+    for _ in range(2):
+        torch.matmul(sb, sa, out=sc)
+    ms = timed(torch, stream, lambda: torch.matmul(sb, sa, out=sc), 3)
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    out["cublas_fp32"] = {"ms": ms, "tflops": flop / ms / 1e9, "rel_err_vs_fp64": err()}
+    out["cblas_sgemm"]["frac_of_cublas_fp32"] = out["cblas_sgemm"]["tflops"] / out["cublas_fp32"]["tflops"]
+    del sa, sb, sc
+    return out
+
+
 def extra_factorizations(torch, AB, dev, stream):
     """The FP64 factorization configurations: dgetrf+dgetrs N=8192 with 16
     right-hand sides on A = G/sqrt(N) + 4I, dpotrf+dpotrs N=8192 on
@@ -938,6 +984,7 @@ def main():
                              "frac_of_cublas": dgemm_tf / cublas_tf,
                              "dram_bytes_per_launch": measured_traffic("dgemm_dmma_kernel 8192^3")}
         del ga, gb
+        out["sgemm_8192"] = extra_sgemm(torch, AB, dev, stream, M)
         out["roofline"] = headline_roofline(torch, AB, dev, stream)
 
         # ---- split-integer (Ozaki) DGEMM 8192^3 on the INT8 tensor cores

@@ -199,8 +199,9 @@ int atlb_dgemm_dev(int TransA, int TransB, int M, int N, int K, double alpha, co
 int atlb_sgemm_dev(int TransA, int TransB, int M, int N, int K, float alpha, const float *A,
                    int lda, const float *B, int ldb, float beta, float *C, int ldc);
 /* FP32 GEMM on the tensor cores: operands rounded to TF32 (prec 1) or BF16
- * (prec 2), or split into TF32 high/low parts for an FP32-accurate product
- * (prec 3); FP32 accumulation (tcgen05, TMEM accumulators). */
+ * (prec 2), or split into TF32 high/low parts whose three products come close
+ * to FP32 accuracy (prec 3; the FP32 accumulation of the tensor cores limits
+ * it at long K); FP32 accumulation (tcgen05, TMEM accumulators). */
 int atlb_sgemm_tc_dev(int prec, int TransA, int TransB, int M, int N, int K, float alpha,
                       const float *A, int lda, const float *B, int ldb, float beta, float *C,
                       int ldc);
@@ -256,7 +257,7 @@ int atlb_dormqr_dev(int Side, int Trans, int M, int N, int K, const double *A, i
 /* Mixed-precision solvers (no counterpart in the reference; LAPACK's
  * dsgesv/dsposv contract).  Factor an FP32 copy of A on the GPU -- trailing
  * updates in FP32 (prec 0), on the tensor cores in TF32 (1), BF16 with FP32
- * accumulation (2), or FP32-accurate split TF32 (3) -- then refine in FP64 until every column reaches a
+ * accumulation (2), or near-FP32 split TF32 (3) -- then refine in FP64 until every column reaches a
  * normwise backward error ||b-Ax||_inf/(||A||_inf ||x||_inf + ||b||_inf) <=
  * N*2^-53.  A and B are unchanged and *iter >= 0 (refinement steps) on
  * success; otherwise the FP64 solver runs, A/ipiv hold its factors and *iter
