@@ -41,6 +41,10 @@ void *pinned(int slot, size_t bytes);
 // enqueued on the two streams never shares a workspace.
 cudaStream_t side_stream();
 cudaEvent_t side_event(int i);  // eight reusable events per thread (i < 8)
+// A third stream per host thread for host-to-device copies that overlap the
+// factorization (streamed inputs), and a growable set of events for them.
+cudaStream_t copy_stream();
+cudaEvent_t chunk_event(int i);
 struct SideScope {
   SideScope();
   ~SideScope();
@@ -68,7 +72,7 @@ enum ScratchSlot {
   kSlotBatch3, kSlotAdj0, kSlotAdj1, kSlotAdj2, kSlotTc0, kSlotTc1, kSlotTrsmW, kSlotTrsvCtl, kSlotLaswp,
   kSlotMixedWL, kSlotMixedWU, kSlotMixedPerm, kSlotGemmSplit, kSlotPermPlan,
   kSlotQrApply, kSlotExt0, kSlotExt1, kSlotExt2, kSlotExt3, kSlotAdjProbs, kSlotKrylov, kSlotKrylovH,
-  kNumSlots
+  kSlotStreamPerm, kSlotStreamTmp, kNumSlots
 };
 
 inline int cdiv(long a, long b) { return (int)((a + b - 1) / b); }

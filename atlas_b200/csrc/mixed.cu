@@ -82,11 +82,11 @@ abs_rowsum_partial_kernel(int N, const double *__restrict__ A, long lda, double 
 // i converts its row's elements and sums their magnitudes in column order,
 // the order of abs_rowsum_partial_kernel, eight loads in flight.
 __global__ void __launch_bounds__(GV_ROWS)
-d2s_rowsum_kernel(int N, const double *__restrict__ A, long lda, float *__restrict__ S, long lds,
+d2s_rowsum_kernel(int N, int ncols, const double *__restrict__ A, long lda, float *__restrict__ S, long lds,
                   double *__restrict__ part) {
   const int i = blockIdx.x * GV_ROWS + threadIdx.x, c0 = blockIdx.y * GV_COLS;
   if (i >= N) return;
-  const int c1 = min(N, c0 + GV_COLS);
+  const int c1 = min(ncols, c0 + GV_COLS);
   const double *a = A + i + (long)c0 * lda;
   float *o = S + i + (long)c0 * lds;
   double s = 0.0;
@@ -328,8 +328,125 @@ void d2s_norm_dev(int N, const double *A, long lda, float *S, long lds, double *
                   cudaStream_t st) {
   const int nch = cdiv(N, GV_COLS);
   ATLB_CUDA_CHECK(cudaMemsetAsync(out, 0, sizeof(unsigned long long), st));
-  d2s_rowsum_kernel<<<dim3(cdiv(N, GV_ROWS), nch), GV_ROWS, 0, st>>>(N, A, lda, S, lds, part);
+  d2s_rowsum_kernel<<<dim3(cdiv(N, GV_ROWS), nch), GV_ROWS, 0, st>>>(N, N, A, lda, S, lds, part);
   rowsum_finish_kernel<<<std::min(cdiv(N, 256), 148), 256, 0, st>>>(N, nch, part, out);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
+
+// d2s_rowsum_kernel with the rows gathered: row i of S takes row perm[i] of
+// A, whose row-sum partial goes to part[.. + perm[i]] (the partial belongs to
+// the source row, so the norm does not depend on the order).
+__global__ void __launch_bounds__(GV_ROWS)
+d2s_rowsum_perm_kernel(int N, int ncols, const double *__restrict__ A, long lda, const int *__restrict__ perm,
+                       float *__restrict__ S, long lds, double *__restrict__ part) {
+  const int i = blockIdx.x * GV_ROWS + threadIdx.x, c0 = blockIdx.y * GV_COLS;
+  if (i >= N) return;
+  const int c1 = min(ncols, c0 + GV_COLS), src = perm[i];
+  const double *a = A + src + (long)c0 * lda;
+  float *o = S + i + (long)c0 * lds;
+  double s = 0.0;
+  int c = c0;
+  for (; c + 8 <= c1; c += 8, a += 8 * lda, o += 8 * lds) {
+    double v[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) v[q] = a[(long)q * lda];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      o[(long)q * lds] = (float)v[q];
+      s += fabs(v[q]);
+    }
+  }
+  for (; c < c1; c++, a += lda, o += lds) {
+    const double v = *a;
+    *o = (float)v;
+    s += fabs(v);
+  }
+  part[(long)blockIdx.y * N + src] = s;
+}
+
+// out[i] = ipiv[i] for i < h, i (no interchange) for h <= i < n
+__global__ void head_ipiv_kernel(int n, int h, const int *__restrict__ ipiv, int *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = i < h ? ipiv[i] : i;
+}
+
+// Y (M x ncols) = rows perm[0..M) of X
+__global__ void gather_rows_kernel(int M, int ncols, const float *__restrict__ X, long ldx,
+                                   const int *__restrict__ perm, float *__restrict__ Y, long ldy) {
+  const long total = (long)M * ncols;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total; idx += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(idx % M), j = (int)(idx / M);
+    Y[i + (long)j * ldy] = X[perm[i] + (long)j * ldx];
+  }
+}
+
+// Pivot numbers of the trailing factorization made absolute (ipiv[h..n) +=
+// h), and its info (dinfo2: 0 or its first zero pivot, counted from row h)
+// folded into *dinfo when the leading part had none.
+__global__ void split_fixup_kernel(int n, int h, int *ipiv, int *dinfo, const int *dinfo2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h + i < n) ipiv[h + i] += h;
+  if (i == 0 && *dinfo == 0 && *dinfo2 > 0) *dinfo = h + *dinfo2;
+}
+
+// The FP32 factorization of a host matrix overlapped with its copy, split
+// at h = about N/2 as the first level of src/lapack/ATL_getrfC.c's
+// recursion.  The copy stream brings the block columns (GV_COLS wide) over
+// back to back; the main stream converts the left half's as they land (S and
+// the row-sum partials) and factors the left N x h panel (getrf_dev) while
+// the right half is still being copied.  The right half is then converted
+// with the panel's row interchanges applied (one gather through their net
+// permutation), brought up to date in two large operations (the unit-lower
+// solve of its top h rows, the product with the panel's L below), and its
+// trailing (N-h) x (N-h) block factored; the trailing interchanges reach the
+// panel's L by one gather of its rows.  ||A||_inf is summed from the
+// partials at the end, as in d2s_norm_dev.  The copies start after the work
+// already on st (a previous call may still read dA).
+void streamed_factor_dev(int N, const double *hA, long hlda, double *dA, long dlda, float *S, long lds,
+                         int *ipiv, int *dinfo, double *part, unsigned long long *nrm, SgemmFn gemm,
+                         cudaStream_t st) {
+  const int nblk = cdiv(N, GV_COLS), hb = nblk / 2, h = hb * GV_COLS, nt = N - h;
+  int *pw = (int *)scratch(kSlotStreamPerm, sizeof(int) * 3 * (size_t)N);
+  int *head = pw, *perm = pw + N, *perm3 = pw + 2 * N;
+  float *tmp = (float *)scratch(kSlotStreamTmp, sizeof(float) * (size_t)nt * h);
+  cudaStream_t cs = copy_stream();
+  ATLB_CUDA_CHECK(cudaMemsetAsync(nrm, 0, sizeof(unsigned long long), st));
+  ATLB_CUDA_CHECK(cudaEventRecord(chunk_event(0), st));
+  ATLB_CUDA_CHECK(cudaStreamWaitEvent(cs, chunk_event(0), 0));
+  for (int c = 0; c < nblk; c++) {
+    const int c0 = c * GV_COLS, w = std::min(GV_COLS, N - c0);
+    ATLB_CUDA_CHECK(cudaMemcpy2DAsync(dA + (long)c0 * dlda, dlda * sizeof(double), hA + (long)c0 * hlda,
+                                      hlda * sizeof(double), (size_t)N * sizeof(double), w,
+                                      cudaMemcpyHostToDevice, cs));
+    if (c < hb || c == nblk - 1) ATLB_CUDA_CHECK(cudaEventRecord(chunk_event(1 + c), cs));
+  }
+  // the left half, converted as it lands, then factored
+  for (int c = 0; c < hb; c++) {
+    const int c0 = c * GV_COLS;
+    ATLB_CUDA_CHECK(cudaStreamWaitEvent(st, chunk_event(1 + c), 0));
+    d2s_rowsum_kernel<<<dim3(cdiv(N, GV_ROWS), 1), GV_ROWS, 0, st>>>(N, GV_COLS, dA + (long)c0 * dlda, dlda,
+                                                                      S + (long)c0 * lds, lds, part + (long)c * N);
+  }
+  ATLB_CUDA_CHECK(cudaGetLastError());
+  getrf_dev<float>(N, h, S, lds, ipiv, dinfo, st, gemm);
+  // the right half: converted through the panel's net row permutation
+  head_ipiv_kernel<<<cdiv(N, 256), 256, 0, st>>>(N, h, ipiv, head);
+  ipiv_to_perm_dev(N, head, perm, st);
+  ATLB_CUDA_CHECK(cudaStreamWaitEvent(st, chunk_event(nblk), 0));  // the last copy (they run in order)
+  float *Sr = S + (long)h * lds;
+  d2s_rowsum_perm_kernel<<<dim3(cdiv(N, GV_ROWS), nblk - hb), GV_ROWS, 0, st>>>(
+      N, nt, dA + (long)h * dlda, dlda, perm, Sr, lds, part + (long)hb * N);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+  trsm_dev<float>(kLeft, kLower, kNoTrans, kUnit, h, nt, 1.f, S, lds, Sr, lds, st, gemm);
+  (gemm ? gemm : sgemm_dev)(kNoTrans, kNoTrans, nt, nt, h, -1.f, S + h, lds, Sr, lds, 1.f, Sr + h, lds, st, 0);
+  // the trailing block, then its interchanges on the panel's L (one gather)
+  getrf_dev<float>(nt, nt, Sr + h, lds, ipiv + h, dinfo + 1, st, gemm);
+  ipiv_to_perm_dev(nt, ipiv + h, perm3, st);
+  gather_rows_kernel<<<grid_for((long)nt * h), 256, 0, st>>>(nt, h, S + h, lds, perm3, tmp, nt);
+  ATLB_CUDA_CHECK(cudaMemcpy2DAsync(S + h, lds * sizeof(float), tmp, nt * sizeof(float), nt * sizeof(float), h,
+                                    cudaMemcpyDeviceToDevice, st));
+  split_fixup_kernel<<<cdiv(nt, 256), 256, 0, st>>>(N, h, ipiv, dinfo, dinfo + 1);
+  rowsum_finish_kernel<<<std::min(cdiv(N, 256), 148), 256, 0, st>>>(N, nblk, part, nrm);
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
 
@@ -590,12 +707,16 @@ int atlb_dsgesv_ex(int N, int NRHS, double *A, int lda, int *ipiv, double *B, in
   *iter = 0;
   if (N == 0 || NRHS == 0) return 0;
   cudaStream_t st = stream();
-  DMat<double> dA = stage_in(kSlotA, (const double *)A, N, N, lda, true, st);
+  // a host A at a size where the copy is long is factored while its second
+  // half arrives
+  const bool streamed = !pivoting && N >= 2048 && !is_dev(A);
+  DMat<double> dA = stage_in(kSlotA, (const double *)A, N, N, lda, !streamed, st);
   DMat<double> dB = stage_in(kSlotB, (const double *)B, N, NRHS, ldb, true, st);
   DMat<double> dX = stage_in(kSlotC, (const double *)X, N, NRHS, ldx, false, st);
   int *dip = stage_vec_in<int>(kSlotIpiv, ipiv, N, false, st);
   int *dinfo = (int *)scratch(kSlotInfo, 64);
   SgemmFn g = factor_gemm(prec);
+  bool copied = !streamed;  // the FP64 A is on the device
   const int n4 = rbt_order(N);
   const long lds = pivoting ? n4 : N;
   float *S = (float *)scratch(kSlotMixedA, sizeof(float) * (size_t)lds * lds);
@@ -614,6 +735,10 @@ int atlb_dsgesv_ex(int N, int NRHS, double *A, int lda, int *ipiv, double *B, in
       rbt_init_dev(n4, rd, st);
       rbt_matrix_dev(N, dA.d, dA.ld, rd, S, st);
       getrf_nopiv_dev<float>(n4, S, lds, dinfo, st, g);
+    } else if (!copied) {
+      streamed_factor_dev(N, (const double *)A, lda, dA.d, dA.ld, S, lds, dip, dinfo, part, nrm, g, st);
+      copied = true;
+      if (few) ipiv_to_perm_dev(N, dip, perm, st);
     } else {
       d2s_norm_dev(N, dA.d, dA.ld, S, lds, part, nrm, st);
       getrf_dev<float>(N, N, S, lds, dip, dinfo, st, g);

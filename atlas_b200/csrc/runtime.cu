@@ -22,7 +22,9 @@ struct ThreadState {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   cudaStream_t side = nullptr;
+  cudaStream_t copy = nullptr;
   cudaEvent_t events[8] = {};
+  std::vector<cudaEvent_t> chunk_events;
   Buf dev[2 * kNumSlots];   // second half: buffers of work on the side stream
   Buf host[2 * kNumSlots];
   ~ThreadState() {
@@ -87,6 +89,21 @@ cudaStream_t side_stream() {
     ATLB_CUDA_CHECK(cudaStreamCreateWithPriority(&tl.side, cudaStreamNonBlocking, greatest));
   }
   return tl.side;
+}
+
+cudaStream_t copy_stream() {
+  ensure_device();
+  if (!tl.copy) ATLB_CUDA_CHECK(cudaStreamCreateWithFlags(&tl.copy, cudaStreamNonBlocking));
+  return tl.copy;
+}
+
+cudaEvent_t chunk_event(int i) {
+  while ((int)tl.chunk_events.size() <= i) {
+    cudaEvent_t e;
+    ATLB_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    tl.chunk_events.push_back(e);
+  }
+  return tl.chunk_events[i];
 }
 
 cudaEvent_t side_event(int i) {

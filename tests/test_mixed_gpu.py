@@ -197,3 +197,40 @@ def test_dsposv_bf16_gmres_ir(gpu):
     assert AB.atlb_dsposv(AB.CblasLower, n, 2, a0.copy(order="F"), n, b0.copy(order="F"), n, x, n, 2, it) == 0
     assert it[0] >= 0, f"no convergence (iter={it[0]})"
     assert np.all(bwd_err(a0, x, b0) <= n * 2.0 ** -53)
+
+
+@pytest.mark.parametrize("n,nrhs,pinned", [(2148, 1, False), (4096, 2, True)])
+def test_dsgesv_host_input_factored_while_copied(gpu, n, nrhs, pinned):
+    """A host A of order >= 2048 is factored while its block columns are
+    copied (each one catches up with the blocks factored before it falls
+    due): the solution meets the same bound as with A on the device, in about
+    the same number of steps, and A is left unchanged.  2148 leaves a ragged
+    last block column; the pinned case is the asynchronous copy."""
+    import torch
+    a0 = kappa_matrix(n, 1e2, n)
+    b0 = np.asfortranarray(np.random.default_rng(9).uniform(-1, 1, (n, nrhs)))
+    ipiv = np.zeros(n, dtype=np.int32)
+    it = np.zeros(1, dtype=np.int32)
+    # host input (column-major storage)
+    if pinned:
+        a = torch.empty((n, n), dtype=torch.float64).pin_memory()
+        a.copy_(torch.from_numpy(np.ascontiguousarray(a0.T)))
+    else:
+        a = a0.copy(order="F")
+    b = b0.copy(order="F")
+    x = np.zeros((n, nrhs), order="F")
+    assert AB.atlb_dsgesv_ex(n, nrhs, a, n, ipiv, b, n, x, n, 3, 0, it) == 0
+    it_host = int(it[0])
+    assert it_host >= 0
+    assert np.all(bwd_err(a0, x, b0) <= n * 2.0 ** -53)
+    a_after = a.numpy().T if pinned else a
+    assert np.array_equal(a_after, a0)
+    # the same system with A on the device (factored after one whole copy)
+    da = torch.from_numpy(np.ascontiguousarray(a0.T)).cuda()
+    db = torch.from_numpy(np.ascontiguousarray(b0.T)).cuda()
+    dx = torch.zeros((nrhs, n), dtype=torch.float64, device="cuda")
+    dpiv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    assert AB.atlb_dsgesv_ex(n, nrhs, da, n, dpiv, db, n, dx, n, 3, 0, it) == 0
+    assert it[0] >= 0 and abs(it_host - int(it[0])) <= 1
+    xd = dx.cpu().numpy().T
+    assert np.all(bwd_err(a0, xd, b0) <= n * 2.0 ** -53)
