@@ -389,26 +389,44 @@ __global__ void split_fixup_kernel(int n, int h, int *ipiv, int *dinfo, const in
   if (i == 0 && *dinfo == 0 && *dinfo2 > 0) *dinfo = h + *dinfo2;
 }
 
-// The FP32 factorization of a host matrix overlapped with its copy, split
-// at h = about N/2 as the first level of src/lapack/ATL_getrfC.c's
-// recursion.  The copy stream brings the block columns (GV_COLS wide) over
-// back to back; the main stream converts the left half's as they land (S and
-// the row-sum partials) and factors the left N x h panel (getrf_dev) while
-// the right half is still being copied.  The right half is then converted
-// with the panel's row interchanges applied (one gather through their net
-// permutation), brought up to date in two large operations (the unit-lower
-// solve of its top h rows, the product with the panel's L below), and its
-// trailing (N-h) x (N-h) block factored; the trailing interchanges reach the
-// panel's L by one gather of its rows.  ||A||_inf is summed from the
-// partials at the end, as in d2s_norm_dev.  The copies start after the work
-// already on st (a previous call may still read dA).
+// B = L^-1 B for L unit lower triangular (n x n) and B n x m, n a multiple
+// of 256 (or at most 256): halves at multiples of 256 down to 256-row
+// leaves, each solved in one trsm_llu_small_dev launch, the halves coupled by
+// one GEMM per level (K >= 256, so every product runs at the tensor cores'
+// long-K rate; trsm_dev's 64-row leaves suit narrow right-hand sides).
+void llu_solve(int n, int m, const float *L, long ldl, float *B, long ldb, SgemmFn gemm, cudaStream_t st) {
+  if (n <= 256) {
+    trsm_llu_small_dev<float>(n, m, L, ldl, B, ldb, st);
+    return;
+  }
+  const int n1 = (n / 2 + 255) / 256 * 256;
+  llu_solve(n1, m, L, ldl, B, ldb, gemm, st);
+  (gemm ? gemm : sgemm_dev)(kNoTrans, kNoTrans, n - n1, m, n1, -1.f, L + n1, ldl, B, ldb, 1.f, B + n1, ldb, st, 0);
+  llu_solve(n - n1, m, L + n1 + (long)n1 * ldl, ldl, B + n1, ldb, gemm, st);
+}
+
+// The FP32 factorization of a host matrix overlapped with its copy, as the
+// outer levels of src/lapack/ATL_getrfC.c's recursion taken left to right
+// over column segments [0, N/4), [N/4, N/2), [N/2, N) (multiples of GV_COLS).
+// The copy stream brings the block columns over back to back.  The first
+// segment is converted as its columns land (S and the row-sum partials) and
+// factored (getrf_dev on its N-row panel) while the rest is still being
+// copied.  Each later segment, once its columns have landed, is converted
+// with the row interchanges of everything to its left applied (one gather
+// through their net permutation), brought up to date with the factored
+// columns in two large operations (the unit-lower solve of its top rows, the
+// product with the L below), and its panel factored; its interchanges reach
+// the L to its left by one gather of those rows.  ||A||_inf is summed from
+// the partials at the end, as in d2s_norm_dev.  The copies start after the
+// work already on st (a previous call may still read dA).
 void streamed_factor_dev(int N, const double *hA, long hlda, double *dA, long dlda, float *S, long lds,
                          int *ipiv, int *dinfo, double *part, unsigned long long *nrm, SgemmFn gemm,
                          cudaStream_t st) {
-  const int nblk = cdiv(N, GV_COLS), hb = nblk / 2, h = hb * GV_COLS, nt = N - h;
-  int *pw = (int *)scratch(kSlotStreamPerm, sizeof(int) * 3 * (size_t)N);
-  int *head = pw, *perm = pw + N, *perm3 = pw + 2 * N;
-  float *tmp = (float *)scratch(kSlotStreamTmp, sizeof(float) * (size_t)nt * h);
+  const int nblk = cdiv(N, GV_COLS);
+  const int segs[4] = {0, std::max(1, nblk / 4) * GV_COLS, std::max(2, nblk / 2) * GV_COLS, N};
+  int *pw = (int *)scratch(kSlotStreamPerm, sizeof(int) * 2 * (size_t)N);
+  int *head = pw, *perm = pw + N;
+  float *tmp = (float *)scratch(kSlotStreamTmp, sizeof(float) * (size_t)(N / 2 + GV_COLS) * (N / 2 + GV_COLS));
   cudaStream_t cs = copy_stream();
   ATLB_CUDA_CHECK(cudaMemsetAsync(nrm, 0, sizeof(unsigned long long), st));
   ATLB_CUDA_CHECK(cudaEventRecord(chunk_event(0), st));
@@ -418,34 +436,41 @@ void streamed_factor_dev(int N, const double *hA, long hlda, double *dA, long dl
     ATLB_CUDA_CHECK(cudaMemcpy2DAsync(dA + (long)c0 * dlda, dlda * sizeof(double), hA + (long)c0 * hlda,
                                       hlda * sizeof(double), (size_t)N * sizeof(double), w,
                                       cudaMemcpyHostToDevice, cs));
-    if (c < hb || c == nblk - 1) ATLB_CUDA_CHECK(cudaEventRecord(chunk_event(1 + c), cs));
+    ATLB_CUDA_CHECK(cudaEventRecord(chunk_event(1 + c), cs));
   }
-  // the left half, converted as it lands, then factored
-  for (int c = 0; c < hb; c++) {
-    const int c0 = c * GV_COLS;
-    ATLB_CUDA_CHECK(cudaStreamWaitEvent(st, chunk_event(1 + c), 0));
-    d2s_rowsum_kernel<<<dim3(cdiv(N, GV_ROWS), 1), GV_ROWS, 0, st>>>(N, GV_COLS, dA + (long)c0 * dlda, dlda,
-                                                                      S + (long)c0 * lds, lds, part + (long)c * N);
+  for (int si = 0; si < 3; si++) {
+    const int a = segs[si], b = segs[si + 1], w = b - a;
+    if (w <= 0) continue;
+    float *Sa = S + (long)a * lds;
+    if (a == 0) {  // converted chunk by chunk as the columns land
+      for (int c = 0; c < cdiv(b, GV_COLS); c++) {
+        const int c0 = c * GV_COLS;
+        ATLB_CUDA_CHECK(cudaStreamWaitEvent(st, chunk_event(1 + c), 0));
+        d2s_rowsum_kernel<<<dim3(cdiv(N, GV_ROWS), 1), GV_ROWS, 0, st>>>(
+            N, std::min(GV_COLS, b - c0), dA + (long)c0 * dlda, dlda, S + (long)c0 * lds, lds, part + (long)c * N);
+      }
+      ATLB_CUDA_CHECK(cudaGetLastError());
+      getrf_dev<float>(N, w, S, lds, ipiv, dinfo, st, gemm);
+      continue;
+    }
+    // converted through the net permutation of ipiv[0..a), then updated
+    head_ipiv_kernel<<<cdiv(N, 256), 256, 0, st>>>(N, a, ipiv, head);
+    ipiv_to_perm_dev(N, head, perm, st);
+    ATLB_CUDA_CHECK(cudaStreamWaitEvent(st, chunk_event(cdiv(b, GV_COLS)), 0));  // copies land in order
+    d2s_rowsum_perm_kernel<<<dim3(cdiv(N, GV_ROWS), cdiv(w, GV_COLS)), GV_ROWS, 0, st>>>(
+        N, w, dA + (long)a * dlda, dlda, perm, Sa, lds, part + (long)(a / GV_COLS) * N);
+    ATLB_CUDA_CHECK(cudaGetLastError());
+    llu_solve(a, w, S, lds, Sa, lds, gemm, st);
+    (gemm ? gemm : sgemm_dev)(kNoTrans, kNoTrans, N - a, w, a, -1.f, S + a, lds, Sa, lds, 1.f, Sa + a, lds, st, 0);
+    // its panel, then its interchanges on the L to its left (one gather)
+    getrf_dev<float>(N - a, w, Sa + a, lds, ipiv + a, dinfo + 1, st, gemm);
+    head_ipiv_kernel<<<cdiv(N - a, 256), 256, 0, st>>>(N - a, w, ipiv + a, head);  // its w pivots only
+    ipiv_to_perm_dev(N - a, head, perm, st);
+    gather_rows_kernel<<<grid_for((long)(N - a) * a), 256, 0, st>>>(N - a, a, S + a, lds, perm, tmp, N - a);
+    ATLB_CUDA_CHECK(cudaMemcpy2DAsync(S + a, lds * sizeof(float), tmp, (N - a) * sizeof(float),
+                                      (N - a) * sizeof(float), a, cudaMemcpyDeviceToDevice, st));
+    split_fixup_kernel<<<cdiv(w, 256), 256, 0, st>>>(b, a, ipiv, dinfo, dinfo + 1);
   }
-  ATLB_CUDA_CHECK(cudaGetLastError());
-  getrf_dev<float>(N, h, S, lds, ipiv, dinfo, st, gemm);
-  // the right half: converted through the panel's net row permutation
-  head_ipiv_kernel<<<cdiv(N, 256), 256, 0, st>>>(N, h, ipiv, head);
-  ipiv_to_perm_dev(N, head, perm, st);
-  ATLB_CUDA_CHECK(cudaStreamWaitEvent(st, chunk_event(nblk), 0));  // the last copy (they run in order)
-  float *Sr = S + (long)h * lds;
-  d2s_rowsum_perm_kernel<<<dim3(cdiv(N, GV_ROWS), nblk - hb), GV_ROWS, 0, st>>>(
-      N, nt, dA + (long)h * dlda, dlda, perm, Sr, lds, part + (long)hb * N);
-  ATLB_CUDA_CHECK(cudaGetLastError());
-  trsm_dev<float>(kLeft, kLower, kNoTrans, kUnit, h, nt, 1.f, S, lds, Sr, lds, st, gemm);
-  (gemm ? gemm : sgemm_dev)(kNoTrans, kNoTrans, nt, nt, h, -1.f, S + h, lds, Sr, lds, 1.f, Sr + h, lds, st, 0);
-  // the trailing block, then its interchanges on the panel's L (one gather)
-  getrf_dev<float>(nt, nt, Sr + h, lds, ipiv + h, dinfo + 1, st, gemm);
-  ipiv_to_perm_dev(nt, ipiv + h, perm3, st);
-  gather_rows_kernel<<<grid_for((long)nt * h), 256, 0, st>>>(nt, h, S + h, lds, perm3, tmp, nt);
-  ATLB_CUDA_CHECK(cudaMemcpy2DAsync(S + h, lds * sizeof(float), tmp, nt * sizeof(float), nt * sizeof(float), h,
-                                    cudaMemcpyDeviceToDevice, st));
-  split_fixup_kernel<<<cdiv(nt, 256), 256, 0, st>>>(N, h, ipiv, dinfo, dinfo + 1);
   rowsum_finish_kernel<<<std::min(cdiv(N, 256), 148), 256, 0, st>>>(N, nblk, part, nrm);
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
