@@ -407,7 +407,8 @@ void llu_solve(int n, int m, const float *L, long ldl, float *B, long ldb, Sgemm
 
 // The FP32 factorization of a host matrix overlapped with its copy, as the
 // outer levels of src/lapack/ATL_getrfC.c's recursion taken left to right
-// over column segments [0, N/4), [N/4, N/2), [N/2, N) (multiples of GV_COLS).
+// over column segments [0, N/8), [N/8, N/4), [N/4, N/2), [N/2, N) (block
+// columns of GV_COLS).
 // The copy stream brings the block columns over back to back.  The first
 // segment is converted as its columns land (S and the row-sum partials) and
 // factored (getrf_dev on its N-row panel) while the rest is still being
@@ -423,7 +424,10 @@ void streamed_factor_dev(int N, const double *hA, long hlda, double *dA, long dl
                          int *ipiv, int *dinfo, double *part, unsigned long long *nrm, SgemmFn gemm,
                          cudaStream_t st) {
   const int nblk = cdiv(N, GV_COLS);
-  const int segs[4] = {0, std::max(1, nblk / 4) * GV_COLS, std::max(2, nblk / 2) * GV_COLS, N};
+  std::vector<int> segs = {0};
+  for (int d : {8, 4, 2})
+    if (nblk / d * GV_COLS > segs.back()) segs.push_back(nblk / d * GV_COLS);
+  segs.push_back(N);
   int *pw = (int *)scratch(kSlotStreamPerm, sizeof(int) * 2 * (size_t)N);
   int *head = pw, *perm = pw + N;
   float *tmp = (float *)scratch(kSlotStreamTmp, sizeof(float) * (size_t)(N / 2 + GV_COLS) * (N / 2 + GV_COLS));
@@ -438,7 +442,7 @@ void streamed_factor_dev(int N, const double *hA, long hlda, double *dA, long dl
                                       cudaMemcpyHostToDevice, cs));
     ATLB_CUDA_CHECK(cudaEventRecord(chunk_event(1 + c), cs));
   }
-  for (int si = 0; si < 3; si++) {
+  for (size_t si = 0; si + 1 < segs.size(); si++) {
     const int a = segs[si], b = segs[si + 1], w = b - a;
     if (w <= 0) continue;
     float *Sa = S + (long)a * lds;
