@@ -199,31 +199,34 @@ def test_dsposv_bf16_gmres_ir(gpu):
     assert np.all(bwd_err(a0, x, b0) <= n * 2.0 ** -53)
 
 
-@pytest.mark.parametrize("n,nrhs,pinned", [(2148, 1, False), (4096, 2, True)])
-def test_dsgesv_host_input_factored_while_copied(gpu, n, nrhs, pinned):
-    """A host A of order >= 2048 is factored while its block columns are
-    copied (each one catches up with the blocks factored before it falls
-    due): the solution meets the same bound as with A on the device, in about
-    the same number of steps, and A is left unchanged.  2148 leaves a ragged
-    last block column; the pinned case is the asynchronous copy."""
+@pytest.mark.parametrize("n,nrhs,pinned,lda", [(2148, 1, False, 2151), (4096, 2, True, 4096)])
+def test_dsgesv_host_input_factored_while_copied(gpu, n, nrhs, pinned, lda):
+    """A host A of order >= 2048 is factored while it is copied (column
+    segments N/8, N/4, N/2, N: each later segment is converted through the
+    interchanges to its left and updated in two large operations): the
+    solution meets the same bound as with A on the device, in about the same
+    number of steps, and A is left unchanged.  2148 leaves a ragged last
+    block column (with a leading dimension above the order); the pinned case
+    is the asynchronous copy."""
     import torch
     a0 = kappa_matrix(n, 1e2, n)
     b0 = np.asfortranarray(np.random.default_rng(9).uniform(-1, 1, (n, nrhs)))
     ipiv = np.zeros(n, dtype=np.int32)
     it = np.zeros(1, dtype=np.int32)
-    # host input (column-major storage)
+    # host input (column-major storage, leading dimension lda)
     if pinned:
         a = torch.empty((n, n), dtype=torch.float64).pin_memory()
         a.copy_(torch.from_numpy(np.ascontiguousarray(a0.T)))
     else:
-        a = a0.copy(order="F")
+        a = np.zeros((lda, n), order="F")
+        a[:n, :] = a0
     b = b0.copy(order="F")
     x = np.zeros((n, nrhs), order="F")
-    assert AB.atlb_dsgesv_ex(n, nrhs, a, n, ipiv, b, n, x, n, 3, 0, it) == 0
+    assert AB.atlb_dsgesv_ex(n, nrhs, a, lda, ipiv, b, n, x, n, 3, 0, it) == 0
     it_host = int(it[0])
     assert it_host >= 0
     assert np.all(bwd_err(a0, x, b0) <= n * 2.0 ** -53)
-    a_after = a.numpy().T if pinned else a
+    a_after = a.numpy().T if pinned else a[:n, :]
     assert np.array_equal(a_after, a0)
     # the same system with A on the device (factored after one whole copy)
     da = torch.from_numpy(np.ascontiguousarray(a0.T)).cuda()
@@ -234,3 +237,20 @@ def test_dsgesv_host_input_factored_while_copied(gpu, n, nrhs, pinned):
     assert it[0] >= 0 and abs(it_host - int(it[0])) <= 1
     xd = dx.cpu().numpy().T
     assert np.all(bwd_err(a0, xd, b0) <= n * 2.0 ** -53)
+
+
+@pytest.mark.parametrize("zero_col", [100, 400, 700, 2100])
+def test_dsgesv_host_input_singular_in_each_segment(gpu, zero_col):
+    """A zero column in any segment of the streamed factorization (2148:
+    [0, 256), [256, 512), [512, 1024), [1024, 2148)) reports its position
+    through the segments' info and pivot offsets: the FP32 factorization
+    fails, the FP64 one finds the same column, info = column + 1."""
+    n = 2148
+    a0 = np.asfortranarray(np.random.default_rng(3).uniform(-1, 1, (n, n)))
+    a0[:, zero_col] = 0.0
+    x = np.zeros((n, 1), order="F")
+    b = np.ones((n, 1), order="F")
+    it = np.zeros(1, dtype=np.int32)
+    ipiv = np.zeros(n, dtype=np.int32)
+    assert AB.atlb_dsgesv_ex(n, 1, a0.copy(order="F"), n, ipiv, b, n, x, n, 3, 0, it) == zero_col + 1
+    assert it[0] == -3
