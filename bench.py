@@ -27,6 +27,7 @@ threads) solving the same N = 8192 system, whole solves, no extrapolation.
 import argparse
 import json
 import os
+import re
 import subprocess
 import sys
 import threading
@@ -132,7 +133,10 @@ def count_kernels(torch, fn):
             torch.cuda.synchronize()
         names = [e.name for e in prof.events() if e.device_type == DeviceType.CUDA
                  and not e.name.startswith(("Memcpy", "Memset", "cudaMem"))]
-        return len(names), sorted(set(n.split("(")[0][:60] for n in names))
+        def short(n):  # "void ns::(anonymous namespace)::k<T, 32>(args)" -> "ns::k<T, 32>"
+            n = n.replace("(anonymous namespace)::", "").replace("void ", "")
+            return re.split(r"\((?!\d)", n)[0][:70]
+        return len(names), sorted(set(short(n) for n in names))
     except Exception as exc:  # profiler unavailable on this box
         return None, repr(exc)[:120]
 
@@ -994,6 +998,19 @@ def main():
         out["dgemm_8192"] = {"ms": dgemm_ms, "tflops": dgemm_tf, "cublas_fp64_tflops": cublas_tf,
                              "frac_of_cublas": dgemm_tf / cublas_tf,
                              "dram_bytes_per_launch": measured_traffic("dgemm_dmma_kernel 8192^3")}
+        # the factorizations' trailing-update shape: C (8192 x 8192) -= A (8192 x K) B (K x 8192)
+        short = {}
+        for kk in (128, 192, 256):
+            # column-major A (M x K, lda M) is a (K, M) tensor, B (K x N, ldb K) an (N, K) one
+            sa, sb = ga[:kk, :].contiguous(), gb[:, :kk].contiguous()
+            f_ours = lambda: AB.atlb_dgemm_dev(111, 111, M, M, kk, -1.0, sa, M, sb, kk, 1.0, gc, M)
+            f_cub = lambda: torch.addmm(gc, sb, sa, alpha=-1.0, out=gc)
+            for f in (f_ours, f_cub):
+                f()
+            t_ours, t_cub = timed(torch, stream, f_ours, 5), timed(torch, stream, f_cub, 5)
+            fl = 2.0 * M * M * kk
+            short[f"k{kk}"] = {"tflops": fl / t_ours / 1e9, "cublas_fp64_tflops": fl / t_cub / 1e9}
+        out["dgemm_8192_short_k"] = short
         del ga, gb
         out["sgemm_8192"] = extra_sgemm(torch, AB, dev, stream, M)
         out["roofline"] = headline_roofline(torch, AB, dev, stream)
