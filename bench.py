@@ -493,6 +493,46 @@ def extra_kappa(torch, AB, dev, stream, n):
     return res
 
 
+def extra_dsposv(torch, AB, dev, stream, n):
+    """Mixed dsposv (split-TF32 Cholesky, FP64 refinement) on an SPD system
+    A = Q diag(s) Q^T, s from 1 to 1/kappa (kappa = 1e2), b ~ U[-1, 1], device
+    pointers; beside it the FP64 dpotrf + dpotrs on the same system."""
+    g = torch.Generator(device=dev)
+    g.manual_seed(777)
+    q, _ = torch.linalg.qr(torch.randn(n, n, dtype=torch.float64, device=dev, generator=g))
+    sv = torch.logspace(0, -2, n, dtype=torch.float64, device=dev)
+    a = (q * sv) @ q.T
+    a = 0.5 * (a + a.T)                       # symmetric: its storage is its column-major form
+    del q
+    b = torch.rand(n, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+    x = torch.empty_like(b)
+    it = np.zeros(1, dtype=np.int32)
+
+    def mixed():
+        AB.atlb_dsposv(AB.CblasLower, n, 1, a, n, b, n, x, n, 3, it)
+    mixed()
+    mixed()
+    ms = timed(torch, stream, mixed, 3)
+    res = {"ms": ms, "iter": int(it[0]), "backward_error": backward_error(torch, a, x, b)}
+    L = torch.empty_like(a)
+    xf = torch.empty_like(b)
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def fp64():
+        L.copy_(a)
+        xf.copy_(b)
+        AB.atlb_dpotrf_dev(122, n, L, n, info)
+        AB.atlb_dpotrs_dev(122, n, 1, L, n, xf, n)
+    fp64()
+    fp64()
+    res["fp64_dpotrf_dpotrs_ms"] = timed(torch, stream, fp64, 3)
+    res["fp64_backward_error"] = backward_error(torch, a, xf, b)
+    res["speedup_mixed_vs_fp64"] = res["fp64_dpotrf_dpotrs_ms"] / ms
+    res["system"] = "SPD Q diag(s) Q^T, kappa 1e2, 1 RHS, split-TF32 factors"
+    del a, L
+    return res
+
+
 def extra_batched(torch, AB, dev, stream):
     """10,000 SPD systems (n in [8,256], 4 RHS), 10,000 LU solves, 50,000 uneven
     DGEMMs (M,N,K in [16,512]): one launch per batch, against a per-instance
@@ -1049,6 +1089,7 @@ def main():
         torch.cuda.empty_cache()
         out["fp64_factorizations"] = extra_factorizations(torch, AB, dev, stream)
         out["mixed_kappa_1e6"] = extra_kappa(torch, AB, dev, stream, n)
+        out["mixed_dsposv_8192"] = extra_dsposv(torch, AB, dev, stream, n)
         out["batched"] = extra_batched(torch, AB, dev, stream)
         out["adjoints"] = extra_adjoints(torch, AB, dev, stream)
 
