@@ -199,15 +199,17 @@ def test_dsposv_bf16_gmres_ir(gpu):
     assert np.all(bwd_err(a0, x, b0) <= n * 2.0 ** -53)
 
 
-@pytest.mark.parametrize("n,nrhs,pinned,lda", [(2148, 1, False, 2151), (4096, 2, True, 4096)])
-def test_dsgesv_host_input_factored_while_copied(gpu, n, nrhs, pinned, lda):
+@pytest.mark.parametrize("n,nrhs,pinned,lda,prec", [(2148, 1, False, 2151, 3), (4096, 2, True, 4096, 3),
+                                                    (2304, 12, False, 2304, 0)])
+def test_dsgesv_host_input_factored_while_copied(gpu, n, nrhs, pinned, lda, prec):
     """A host A of order >= 2048 is factored while it is copied (column
     segments N/8, N/4, N/2, N: each later segment is converted through the
     interchanges to its left and updated in two large operations): the
     solution meets the same bound as with A on the device, in about the same
     number of steps, and A is left unchanged.  2148 leaves a ragged last
     block column (with a leading dimension above the order); the pinned case
-    is the asynchronous copy."""
+    is the asynchronous copy; FP32 factors with 12 right-hand sides take the
+    SIMT products and the blocked solves."""
     import torch
     a0 = kappa_matrix(n, 1e2, n)
     b0 = np.asfortranarray(np.random.default_rng(9).uniform(-1, 1, (n, nrhs)))
@@ -222,7 +224,7 @@ def test_dsgesv_host_input_factored_while_copied(gpu, n, nrhs, pinned, lda):
         a[:n, :] = a0
     b = b0.copy(order="F")
     x = np.zeros((n, nrhs), order="F")
-    assert AB.atlb_dsgesv_ex(n, nrhs, a, lda, ipiv, b, n, x, n, 3, 0, it) == 0
+    assert AB.atlb_dsgesv_ex(n, nrhs, a, lda, ipiv, b, n, x, n, prec, 0, it) == 0
     it_host = int(it[0])
     assert it_host >= 0
     assert np.all(bwd_err(a0, x, b0) <= n * 2.0 ** -53)
@@ -233,7 +235,7 @@ def test_dsgesv_host_input_factored_while_copied(gpu, n, nrhs, pinned, lda):
     db = torch.from_numpy(np.ascontiguousarray(b0.T)).cuda()
     dx = torch.zeros((nrhs, n), dtype=torch.float64, device="cuda")
     dpiv = torch.zeros(n, dtype=torch.int32, device="cuda")
-    assert AB.atlb_dsgesv_ex(n, nrhs, da, n, dpiv, db, n, dx, n, 3, 0, it) == 0
+    assert AB.atlb_dsgesv_ex(n, nrhs, da, n, dpiv, db, n, dx, n, prec, 0, it) == 0
     assert it[0] >= 0 and abs(it_host - int(it[0])) <= 1
     xd = dx.cpu().numpy().T
     assert np.all(bwd_err(a0, xd, b0) <= n * 2.0 ** -53)
