@@ -2,7 +2,10 @@
 // mode of the mixed-precision solvers).  128x128x8 CTA tile, 256 threads,
 // 8x8 outputs per thread; op(A) and op(B) tiles are staged in shared memory
 // k-major (m / n contiguous) by a 3-stage cp.async pipeline, whatever their
-// global layout, so the inner loop reads 128-bit vectors.
+// global layout, so the inner loop reads 128-bit vectors.  An output of few
+// tiles with a long K (the Cholesky's diagonal-block updates) is split along
+// K over gridDim.y: each slice writes its partial product to a workspace and
+// one pass sums the slices into C.
 // Reference semantics: src/blas/reference/level3/ATL_srefgemm.c.
 #include <cstdint>
 #include "common.cuh"
@@ -33,7 +36,17 @@ template <bool TA, bool TB>
 __global__ void __launch_bounds__(THREADS, 2)
 sgemm_simt_kernel(int M, int N, int K, float alpha, const float *__restrict__ A, long lda,
                   const float *__restrict__ B, long ldb, float beta, float *__restrict__ C,
-                  long ldc, int tri) {
+                  long ldc, int tri, int kc, float *__restrict__ W) {
+  if (gridDim.y > 1) {  // K slice blockIdx.y: its partial product, unscaled, into W's slice (ld M)
+    const int k0 = blockIdx.y * kc;
+    A += TA ? (long)k0 : (long)k0 * lda;
+    B += TB ? (long)k0 * ldb : (long)k0;
+    K = min(kc, K - k0);
+    C = W + (long)blockIdx.y * M * N;
+    ldc = M;
+    alpha = 1.f;
+    beta = 0.f;
+  }
   __shared__ __align__(16) float sA[STAGES][BK * LDS];
   __shared__ __align__(16) float sB[STAGES][BK * LDS];
   const int tiles_m = (M + BM - 1) / BM, tiles_n = (N + BN - 1) / BN;
@@ -150,6 +163,21 @@ sgemm_simt_kernel(int M, int N, int K, float alpha, const float *__restrict__ A,
   }
 }
 
+// C = beta C + alpha (sum of the S partial products in W, ld M), in C's triangle
+__global__ void splitk_sum_kernel(int M, int N, int S, const float *__restrict__ W, float alpha, float beta,
+                                  float *__restrict__ C, long ldc, int tri) {
+  const long total = (long)M * N;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total; idx += (long)gridDim.x * blockDim.x) {
+    const int r = (int)(idx % M), c = (int)(idx / M);
+    if (tri == 1 && r < c) continue;
+    if (tri == 2 && r > c) continue;
+    float v = 0.f;
+    for (int s = 0; s < S; s++) v += W[idx + (long)s * total];
+    float *p = C + r + (long)c * ldc;
+    *p = beta == 0.f ? alpha * v : fmaf(beta, *p, alpha * v);
+  }
+}
+
 __global__ void sscale_kernel(int M, int N, float beta, float *C, long ldc, int tri) {
   long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
   long total = (long)M * N;
@@ -178,11 +206,28 @@ void sgemm_dev(int ta, int tb, int M, int N, int K, float alpha, const float *A,
   }
   int tiles = cdiv(M, BM) * cdiv(N, BN);
   const bool tA = ta != kNoTrans, tB = tb != kNoTrans;
-  if (!tA && !tB) sgemm_simt_kernel<false, false><<<tiles, THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, tri);
-  else if (!tA && tB) sgemm_simt_kernel<false, true><<<tiles, THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, tri);
-  else if (tA && !tB) sgemm_simt_kernel<true, false><<<tiles, THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, tri);
-  else sgemm_simt_kernel<true, true><<<tiles, THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, tri);
+  // few output tiles and a long K: split K so that about two CTAs per SM run
+  int S = 1, kc = K;
+  float *W = nullptr;
+  if (tiles < num_sms() / 2 && K >= 1024 && !no_alloc_active()) {
+    S = std::min(cdiv(K, 256), std::max(1, 2 * num_sms() / tiles));
+    kc = cdiv(cdiv(K, S), BK) * BK;
+    S = cdiv(K, kc);
+    if (S > 1) W = (float *)scratch(kSlotGemmSplit, sizeof(float) * (size_t)S * M * N);
+    else kc = K;
+  }
+  const dim3 grid(tiles, S);
+  if (!tA && !tB) sgemm_simt_kernel<false, false><<<grid, THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, tri, kc, W);
+  else if (!tA && tB) sgemm_simt_kernel<false, true><<<grid, THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, tri, kc, W);
+  else if (tA && !tB) sgemm_simt_kernel<true, false><<<grid, THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, tri, kc, W);
+  else sgemm_simt_kernel<true, true><<<grid, THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, tri, kc, W);
   ATLB_CUDA_CHECK(cudaGetLastError());
+  if (S > 1) {
+    const long total = (long)M * N;
+    splitk_sum_kernel<<<(int)std::min<long>((total + 255) / 256, 148L * 8), 256, 0, st>>>(M, N, S, W, alpha, beta, C,
+                                                                                      ldc, tri);
+    ATLB_CUDA_CHECK(cudaGetLastError());
+  }
 }
 
 }  // namespace atlb

@@ -479,6 +479,30 @@ void streamed_factor_dev(int N, const double *hA, long hlda, double *dA, long dl
   ATLB_CUDA_CHECK(cudaGetLastError());
 }
 
+// The referenced triangle of S (uplo) copied, transposed, into the other
+// one (the diagonal stays): after a Cholesky factorization S then holds L and
+// L^T (or U^T and U), so both triangular solves read their factor with
+// coalesced column accesses.  32 x 32 tiles through shared memory; a CTA
+// takes the tile pair (bi, bj), bi > bj, of the lower grid.
+__global__ void mirror_tri_kernel(int uplo, int N, float *__restrict__ S, long lds) {
+  __shared__ float t[32][33];
+  const int bi = blockIdx.y, bj = blockIdx.x;
+  if (bj > bi) return;
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  // source tile: rows of block bi, columns of block bj (lower) or its transpose position (upper)
+  const int sr0 = uplo == kLower ? bi * 32 : bj * 32, sc0 = uplo == kLower ? bj * 32 : bi * 32;
+  for (int q = ty; q < 32; q += 8) {
+    const int r = sr0 + tx, c = sc0 + q;
+    t[q][tx] = (r < N && c < N) ? S[r + (long)c * lds] : 0.f;
+  }
+  __syncthreads();
+  for (int q = ty; q < 32; q += 8) {
+    const int r = sc0 + tx, c = sr0 + q;  // destination: the transposed position
+    const bool strict = uplo == kLower ? r < c : r > c;
+    if (r < N && c < N && strict) S[r + (long)c * lds] = t[tx][q];
+  }
+}
+
 void d2s_dev(int M, int N, const double *A, long lda, float *S, long lds, cudaStream_t st) {
   d2s_kernel<<<grid_for((long)M * N), 256, 0, st>>>(M, N, A, lda, S, lds);
   ATLB_CUDA_CHECK(cudaGetLastError());
@@ -861,22 +885,26 @@ int atlb_dsposv(int Uplo, int N, int NRHS, double *A, int lda, double *B, int ld
   const bool few = NRHS <= 8;
   float *W1 = few ? (float *)scratch(kSlotMixedWL, sizeof(float) * trsv_w_elems(N)) : nullptr;
   float *W2 = few ? (float *)scratch(kSlotMixedWU, sizeof(float) * trsv_w_elems(N)) : nullptr;
-  // A = U^T U: solve with U^T then U; A = L L^T: with L then L^T
-  const int t1 = Uplo == kUpper ? kTrans : kNoTrans, t2 = Uplo == kUpper ? kNoTrans : kTrans;
+  // A = L L^T (or U^T U): the factor mirrored into the other triangle of S,
+  // then a lower solve with L (or U^T) and an upper one with L^T (or U), both
+  // reading S column by column
   auto factor = [&](double *part, unsigned long long *nrm) {
     d2s_norm_dev(N, Af, N, S, N, part, nrm, st);
     potrf_dev<float>(Uplo, N, S, N, dinfo, st, g);
     if (few) {
-      trsv_inverse_dev<float>(Uplo, t1, kNonUnit, N, S, N, W1, st);
-      trsv_inverse_dev<float>(Uplo, t2, kNonUnit, N, S, N, W2, st);
+      const dim3 tiles(cdiv(N, 32), cdiv(N, 32));
+      mirror_tri_kernel<<<tiles, dim3(32, 8), 0, st>>>(Uplo, N, S, N);
+      ATLB_CUDA_CHECK(cudaGetLastError());
+      trsv_inverse_dev<float>(kLower, kNoTrans, kNonUnit, N, S, N, W1, st);
+      trsv_inverse_dev<float>(kUpper, kNoTrans, kNonUnit, N, S, N, W2, st);
     }
     return read_info(dinfo, st);
   };
   auto correct = [&](const double *R, long ldr, double *Xc, long ldxc) {
     d2s_dev(N, NRHS, R, ldr, Rs, N, st);
     if (few) {
-      trsv_w_dev<float>(Uplo, t1, N, NRHS, S, N, W1, Rs, N, st);
-      trsv_w_dev<float>(Uplo, t2, N, NRHS, S, N, W2, Rs, N, st);
+      trsv_w_dev<float>(kLower, kNoTrans, N, NRHS, S, N, W1, Rs, N, st);
+      trsv_w_dev<float>(kUpper, kNoTrans, N, NRHS, S, N, W2, Rs, N, st);
     } else {
       potrs_dev<float>(Uplo, N, NRHS, S, N, Rs, N, st, g);
     }

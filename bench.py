@@ -829,6 +829,16 @@ def run_probe(torch, AB, what, n, acol0, b0, x, ipiv, it, hprec, hpiv, dev, trac
         def call():
             A.copy_(G0)
             AB.atlb_dgeqrf_dev(2 * n, n, A, 2 * n, tau)
+    elif what == "mixed_posv":   # mixed dsposv on an SPD system (split-TF32 Cholesky), device pointers
+        g = torch.Generator(device=dev)
+        g.manual_seed(5)
+        gm = torch.randn(n, n, dtype=f64, device=dev, generator=g)
+        S = gm @ gm.T / n + torch.eye(n, dtype=f64, device=dev)
+        del gm
+        sx = torch.empty_like(b0)
+
+        def call():
+            AB.atlb_dsposv(AB.CblasLower, n, 1, S, n, b0, n, sx, n, hprec, it)
     elif what == "mixed_host":   # the e2e call: pinned host A, b, x (A copied while it is factored)
         ha = torch.empty((n, n), dtype=f64).pin_memory()
         ha.copy_(acol0.cpu())
@@ -906,8 +916,8 @@ def main():
     ap.add_argument("--n", type=int, default=N_DEFAULT, help="matrix order (default 8192; smaller for profiling)")
     ap.add_argument("--skip-e2e", action="store_true", help="omit the host-buffer leg (profiling)")
     ap.add_argument("--skip-extras", action="store_true", help="only the headline and FP64 solves (profiling)")
-    ap.add_argument("--probe", choices=["dgemm", "getrf", "potrf", "geqrf", "mixed", "mixed_host", "ozaki",
-                                        "tcgemm"],
+    ap.add_argument("--probe", choices=["dgemm", "getrf", "potrf", "geqrf", "mixed", "mixed_host", "mixed_posv",
+                                        "ozaki", "tcgemm"],
                     help="profiling aid: warm up, then run ONE call of the named path at order --n between "
                          "cudaProfilerStart/Stop (ncu --profile-from-start off) and exit")
     ap.add_argument("--trace", action="store_true",

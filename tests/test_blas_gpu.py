@@ -109,6 +109,27 @@ def test_sgemm_vs_oracle(gpu, orc, ta, tb):
     assert np.max(np.abs(c - cr)) <= tol
 
 
+@pytest.mark.parametrize("ta,tb", [(111, 111), (112, 112), (111, 112)])
+@pytest.mark.parametrize("m,n,k", [(200, 150, 5000), (128, 128, 4096)])
+def test_sgemm_split_k_vs_fp64(gpu, ta, tb, m, n, k):
+    """A few output tiles with a long K: the SIMT FP32 GEMM splits K over the
+    grid (partial products summed by a second pass) -- alpha, beta and the
+    transposes still apply, to FP32 accuracy against an FP64 product."""
+    rng = np.random.default_rng(m + n + k + ta + tb)
+    ma, na = (m, k) if ta == 111 else (k, m)
+    mb, nb = (k, n) if tb == 111 else (n, k)
+    a = np.asfortranarray(rng.uniform(-1, 1, (ma, na)), dtype=np.float32)
+    b = np.asfortranarray(rng.uniform(-1, 1, (mb, nb)), dtype=np.float32)
+    c0 = np.asfortranarray(rng.uniform(-1, 1, (m, n)), dtype=np.float32)
+    c = c0.copy(order="F")
+    AB.cblas_sgemm(CM, ta, tb, m, n, k, -0.75, a, ma, b, mb, 0.5, c, m)
+    opa = a.astype(np.float64) if ta == 111 else a.astype(np.float64).T
+    opb = b.astype(np.float64) if tb == 111 else b.astype(np.float64).T
+    ref = -0.75 * (opa @ opb) + 0.5 * c0.astype(np.float64)
+    tol = 4 * k * np.finfo(np.float32).eps * (np.abs(opa) @ np.abs(opb)).max()
+    assert np.max(np.abs(c - ref)) <= tol
+
+
 def test_trsm_trmm_golden_cases(gpu, orc, gold):
     for i in range(int(gold["counts"][1])):
         m, n, side, uplo, ta, diag, alpha = gold[f"trsm{i}"]
