@@ -244,6 +244,92 @@ void gemm_call<float>(SgemmFn fn, int ta, int tb, int M, int N, int K, float alp
   (fn ? fn : sgemm_dev)(ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, st, 0);
 }
 
+// C (M x N) -= op(A) (M x K) op(B) (K x N) for K <= 64: the product that
+// couples the two halves of a TRSM of order <= 128 (the Cholesky's block
+// columns).  The general GEMMs pay their K-loop pipeline, or a split-K pass
+// with its reduction, for what is one 64-deep step; here a CTA takes a
+// 64 x 64 tile of C, copies its slices of op(A) and op(B) into shared memory
+// (cp.async, all in flight at once) while its threads load their old C
+// values, and each thread computes 4 rows (16 apart) x 4 columns (16 apart).
+constexpr int SK_T = 64, SK_K = 64;
+template <typename T, bool TA, bool TB>
+__global__ void __launch_bounds__(256, 2)
+gemm_smallk_kernel(int M, int N, int K, const T *__restrict__ A, long lda, const T *__restrict__ B, long ldb,
+                   T *__restrict__ C, long ldc) {
+  extern __shared__ __align__(16) unsigned char sk_smem[];
+  T(*sA)[SK_T + 1] = reinterpret_cast<T(*)[SK_T + 1]>(sk_smem);  // sA[k][m]
+  T(*sB)[SK_T + 1] = sA + SK_K;                                   // sB[k][n]
+  const int tid = threadIdx.x, m0 = blockIdx.x * SK_T, n0 = blockIdx.y * SK_T;
+  const int tr = tid % 16, tc = tid / 16;
+  for (int e = tid; e < SK_K * SK_T; e += 256) {
+    // op(A)(m, k) = TA ? A[k + m lda] : A[m + k lda]; the faster index runs along memory
+    const int i = TA ? e % SK_K : e / SK_T, r = TA ? e / SK_K : e % SK_T;  // (k, m)
+    const bool okA = i < K && m0 + r < M;
+    const T *ga = TA ? A + i + (long)(m0 + r) * lda : A + (m0 + r) + (long)i * lda;
+    if (sizeof(T) == 8) cp_async8(&sA[i][r], okA ? ga : A, okA);
+    else cp_async4(&sA[i][r], okA ? ga : A, okA);
+    // op(B)(k, n) = TB ? B[n + k ldb] : B[k + n ldb]
+    const int kb = TB ? e / SK_T : e % SK_K, c = TB ? e % SK_T : e / SK_K;
+    const bool okB = kb < K && n0 + c < N;
+    const T *gb = TB ? B + (n0 + c) + (long)kb * ldb : B + kb + (long)(n0 + c) * ldb;
+    if (sizeof(T) == 8) cp_async8(&sB[kb][c], okB ? gb : B, okB);
+    else cp_async4(&sB[kb][c], okB ? gb : B, okB);
+  }
+  cp_async_commit();
+  T old[4][4], acc[4][4];
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+      const int r = m0 + tr + 16 * a, c = n0 + tc + 16 * q;
+      old[a][q] = (r < M && c < N) ? C[r + (long)c * ldc] : T(0);
+      acc[a][q] = T(0);
+    }
+  cp_async_wait<0>();
+  __syncthreads();
+  for (int i = 0; i < K; i++) {
+    T av[4], bv[4];
+#pragma unroll
+    for (int a = 0; a < 4; a++) av[a] = sA[i][tr + 16 * a];
+#pragma unroll
+    for (int q = 0; q < 4; q++) bv[q] = sB[i][tc + 16 * q];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[a][q] = fma(av[a], bv[q], acc[a][q]);
+  }
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+      const int r = m0 + tr + 16 * a, c = n0 + tc + 16 * q;
+      if (r < M && c < N) C[r + (long)c * ldc] = old[a][q] - acc[a][q];
+    }
+}
+
+template <typename T, bool TA, bool TB>
+void smallk_launch(int M, int N, int K, const T *A, long lda, const T *B, long ldb, T *C, long ldc, cudaStream_t st) {
+  constexpr int smem = 2 * SK_K * (SK_T + 1) * (int)sizeof(T);
+  static bool configured = false;
+  if (!configured) {
+    ATLB_CUDA_CHECK(cudaFuncSetAttribute(gemm_smallk_kernel<T, TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         smem));
+    configured = true;
+  }
+  gemm_smallk_kernel<T, TA, TB><<<dim3(cdiv(M, SK_T), cdiv(N, SK_T)), 256, smem, st>>>(M, N, K, A, lda, B, ldb, C,
+                                                                                      ldc);
+  ATLB_CUDA_CHECK(cudaGetLastError());
+}
+
+template <typename T>
+void gemm_smallk(int ta, int tb, int M, int N, int K, const T *A, long lda, const T *B, long ldb, T *C, long ldc,
+                 cudaStream_t st) {
+  if (ta == kNoTrans && tb == kNoTrans) smallk_launch<T, false, false>(M, N, K, A, lda, B, ldb, C, ldc, st);
+  else if (ta == kNoTrans) smallk_launch<T, false, true>(M, N, K, A, lda, B, ldb, C, ldc, st);
+  else if (tb == kNoTrans) smallk_launch<T, true, false>(M, N, K, A, lda, B, ldb, C, ldc, st);
+  else smallk_launch<T, true, true>(M, N, K, A, lda, B, ldb, C, ldc, st);
+}
+
 // B2 (n2 x m) -= T21 (n2 x n1) * X1 (n1 x m), everything in effective strides.
 template <typename T>
 void eff_update(const Eff<T> &e, int r2, int n2, int r1, int n1, int m, SgemmFn fn,
@@ -251,14 +337,17 @@ void eff_update(const Eff<T> &e, int r2, int n2, int r1, int n1, int m, SgemmFn 
   const T *T21 = e.Tp + r2 * e.tr + r1 * e.tc;
   T *B2 = e.Bp + r2 * e.br;
   const T *X1 = e.Bp + r1 * e.br;
+  const bool small = n1 <= SK_K && n2 <= 2 * SK_T;  // the coupling product of an order <= 128 solve
   if (e.br == 1) {  // B column-major (ld = bc)
     int ta = (e.tr == 1) ? kNoTrans : kTrans;
     long ldt = (e.tr == 1) ? e.tc : e.tr;
-    gemm_call<T>(fn, ta, kNoTrans, n2, m, n1, T(-1), T21, ldt, X1, e.bc, T(1), B2, e.bc, st);
+    if (small) gemm_smallk<T>(ta, kNoTrans, n2, m, n1, T21, ldt, X1, e.bc, B2, e.bc, st);
+    else gemm_call<T>(fn, ta, kNoTrans, n2, m, n1, T(-1), T21, ldt, X1, e.bc, T(1), B2, e.bc, st);
   } else {  // B^T column-major (m x n) with ld = br: B2^T -= X1^T * T21^T
     int tb = (e.tc == 1) ? kNoTrans : kTrans;
     long ldt = (e.tc == 1) ? e.tr : e.tc;
-    gemm_call<T>(fn, kNoTrans, tb, m, n2, n1, T(-1), X1, e.br, T21, ldt, T(1), B2, e.br, st);
+    if (small) gemm_smallk<T>(kNoTrans, tb, m, n2, n1, X1, e.br, T21, ldt, B2, e.br, st);
+    else gemm_call<T>(fn, kNoTrans, tb, m, n2, n1, T(-1), X1, e.br, T21, ldt, T(1), B2, e.br, st);
   }
 }
 
