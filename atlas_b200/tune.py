@@ -107,8 +107,8 @@ def main():
         ("potrf_nb", [128, 256, 384, 512], potrf, 3),
         ("dgemm_group", [4, 8, 16], dgemm_big, 3),
         ("dgemm_splitk", [0, 1], dgemm_small, 5),
-        ("sgetrf_nb", [192, 256], mixed, 7),
-        ("mixed_tc_min_work_log2", [24, 26, 28, 31], mixed, 7),
+        ("sgetrf_nb", [192, 224, 256], mixed, 7),
+        ("mixed_tc_min_work_log2", [20, 22, 24, 26, 28, 31], mixed, 7),
     ]
     lines = [f"# atlas_b200 tuning, {time.strftime('%Y-%m-%d %H:%M:%S')}, "
              f"{torch.cuda.get_device_name(0)}, factorization order {n}"]
