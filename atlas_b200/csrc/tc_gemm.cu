@@ -6,7 +6,7 @@
 // FP32 accumulation; kind::i8 (signed INT8 operands, exact INT32
 // accumulation).  One CTA computes a 128 x BN tile: warp 0 streams 128-byte
 // K-slabs of A and B into a STAGES-deep ring of 128B-swizzled shared-memory
-// tiles with TMA (no multicast), one thread of warp 1 issues tcgen05.mma into
+// tiles with TMA (each CTA loads its own tiles), one thread of warp 1 issues tcgen05.mma into
 // a TMEM accumulator and releases each stage with tcgen05.commit, and all
 // four warps drain TMEM (tcgen05.ld 32x32b) into the epilogue.  Every
 // mbarrier wait is bounded: on timeout the kernel records an error code in

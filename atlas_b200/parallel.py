@@ -18,8 +18,9 @@ the same decomposition needs no exchange on the data path:
   chain is sequential): `bench.py --gpus N` runs N independent replicas.
 
 Timing across ranks is device time, reduced with MAX (the slowest rank
-sets the job's time).  No TMA or bulk load with cluster multicast is issued
-by any kernel these paths run, so they may run on several GPUs.
+sets the job's time).  Every TMA load of the kernels these paths run reads
+this GPU's own memory into the issuing CTA alone, so they may run on several
+GPUs.
 """
 import numpy as np
 
