@@ -407,8 +407,8 @@ void llu_solve(int n, int m, const float *L, long ldl, float *B, long ldb, Sgemm
 
 // The FP32 factorization of a host matrix overlapped with its copy, as the
 // outer levels of src/lapack/ATL_getrfC.c's recursion taken left to right
-// over column segments [0, N/8), [N/8, N/4), [N/4, N/2), [N/2, N) (block
-// columns of GV_COLS).
+// over column segments [0, N/16), [N/16, N/8), [N/8, N/4), [N/4, N/2),
+// [N/2, N) (block columns of GV_COLS).
 // The copy stream brings the block columns over back to back.  The first
 // segment is converted as its columns land (S and the row-sum partials) and
 // factored (getrf_dev on its N-row panel) while the rest is still being
@@ -425,7 +425,7 @@ void streamed_factor_dev(int N, const double *hA, long hlda, double *dA, long dl
                          cudaStream_t st) {
   const int nblk = cdiv(N, GV_COLS);
   std::vector<int> segs = {0};
-  for (int d : {8, 4, 2})
+  for (int d : {16, 8, 4, 2})
     if (nblk / d * GV_COLS > segs.back()) segs.push_back(nblk / d * GV_COLS);
   segs.push_back(N);
   int *pw = (int *)scratch(kSlotStreamPerm, sizeof(int) * 2 * (size_t)N);

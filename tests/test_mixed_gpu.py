@@ -203,7 +203,7 @@ def test_dsposv_bf16_gmres_ir(gpu):
                                                     (2304, 12, False, 2304, 0)])
 def test_dsgesv_host_input_factored_while_copied(gpu, n, nrhs, pinned, lda, prec):
     """A host A of order >= 2048 is factored while it is copied (column
-    segments N/8, N/4, N/2, N: each later segment is converted through the
+    segments N/16, N/8, N/4, N/2, N: each later segment is converted through the
     interchanges to its left and updated in two large operations): the
     solution meets the same bound as with A on the device, in about the same
     number of steps, and A is left unchanged.  2148 leaves a ragged last
